@@ -1,0 +1,1647 @@
+// Host driver of the B200 numerical phase: pastix_data_t, the pastix_task_* /
+// pastix_subtask_* entry points, device residency of the factor, and the
+// level-by-level launch sequence of the factorization and of the solve.
+//
+// Entry points follow the reference's control flow and argument checks:
+//   pastixInitParam / pastixInit / pastixFinalize   common/api.c:420,905,928
+//   pastix_task_analyze                             blend/pastix_task_analyze.c:53
+//   pastix_subtask_spm2bcsc/bcsc2ctab/sopalin       sopalin/pastix_task_sopalin.c:93,213,412
+//   pastix_task_numfact                             sopalin/pastix_task_sopalin.c:654
+//   pastix_subtask_applyorder/trsm/diag/solve(_adv) sopalin/pastix_task_solve.c:169,296,422,512,713
+//   pastix_task_solve                               sopalin/pastix_task_solve.c:758
+//   pastix_subtask_refine / pastix_task_refine      refinement/pastix_task_refine.c:106,236
+//   pastix()                                        sopalin/pastix.c:103
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/pastix_b200.h"
+#include "device.cuh"
+#include "symbol.hpp"
+
+namespace pgpu {
+// factor.cu
+template <typename T>
+void launch_fill_coef(int64_t, const double *, const int64_t *, const int64_t *, T *, T *, cudaStream_t);
+template <typename T, int F>
+void launch_panel_small(const DevStruct &, const int *, int, size_t, T *, T *, const FactParams &, cudaStream_t);
+template <typename T, int F>
+void launch_diag_large(const DevStruct &, const int *, int, size_t, T *, T *, const FactParams &, cudaStream_t);
+template <typename T, int F>
+void launch_trsm(const DevStruct &, const RowTile *, int, int, size_t, T *, T *, cudaStream_t);
+template <typename T, int F>
+void launch_update(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);
+template <typename T, int F>
+cudaError_t set_smem_attrs(size_t, size_t, size_t);
+// solve.cu
+template <typename T>
+void launch_fwd_diag(const DevStruct &, const int *, int, int, const T *, int, T *, int, int, cudaStream_t);
+template <typename T>
+void launch_fwd_update(const DevStruct &, const RowTile *, int, int, const T *, T *, int, int, cudaStream_t);
+template <typename T>
+void launch_bwd_update(const DevStruct &, const RowTile *, int, const T *, T *, int, int, cudaStream_t);
+template <typename T>
+void launch_bwd_diag(const DevStruct &, const int *, int, int, const T *, int, T *, int, int, cudaStream_t);
+template <typename T>
+void launch_diag_scale(const DevStruct &, int, const T *, T *, int, int, cudaStream_t);
+int solve_rows_per_tile();
+// vec.cu
+void launch_spmv(int, int64_t, const int *, const int *, const double *, double, const double *, double, double *,
+                 cudaStream_t);
+int reduce_partials();
+void launch_dot(int64_t, const double *, const double *, double *, int, double *, cudaStream_t);
+void launch_axpy(int64_t, double, const double *, double *, cudaStream_t);
+void launch_xpby(int64_t, const double *, double, double *, cudaStream_t);
+void launch_scal(int64_t, double, double *, cudaStream_t);
+void launch_gemv(int64_t, int, const double *, const double *, double *, cudaStream_t);
+template <typename TS, typename TD>
+void launch_permute(int, int, const int64_t *, int, const TS *, int64_t, TD *, int64_t, cudaStream_t);
+template <typename TS, typename TD>
+void launch_cast(int64_t, const TS *, TD *, cudaStream_t);
+void launch_sampled(int64_t, const int *, const int *, double, const double *, const double *, double *,
+                    cudaStream_t);
+}  // namespace pgpu
+
+using pgpu::idx_t;
+
+// ---------------------------------------------------------------------------
+// internal state
+// ---------------------------------------------------------------------------
+enum : int {
+    STEP_INIT = 1 << 0, STEP_ORDERING = 1 << 1, STEP_SYMBFACT = 1 << 2, STEP_ANALYSE = 1 << 3,
+    STEP_CSC2BCSC = 1 << 4, STEP_BCSC2CTAB = 1 << 5, STEP_NUMFACT = 1 << 6, STEP_SOLVE = 1 << 7,
+    STEP_REFINE = 1 << 8
+};
+
+namespace {
+
+constexpr idx_t SMALL_PANEL_ELEMS = 4096;  // st*nc below which a cblk is factored in one CTA's smem
+
+template <typename X>
+struct DBuf {  // owning device buffer
+    X *p = nullptr;
+    size_t n = 0;
+    ~DBuf() { reset(); }
+    void reset() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t cnt) {
+        if (cnt == n && p) return cudaSuccess;
+        reset();
+        if (cnt == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&p, cnt * sizeof(X));
+        if (e == cudaSuccess) n = cnt;
+        return e;
+    }
+    cudaError_t upload(const std::vector<X> &v, cudaStream_t st) {
+        cudaError_t e = alloc(v.size());
+        if (e != cudaSuccess || v.empty()) return e;
+        return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice, st);
+    }
+};
+
+// Launch lists of one level, as offsets into the flat device arrays.
+struct LevelLists {
+    int small0, small1;     // k_panel_small cblks
+    int large0, large1;     // k_diag_large cblks
+    int trsm0, trsm1;       // k_trsm row tiles
+    int upd0, upd1;         // k_update tiles
+    int cb0, cb1;           // all cblks of the level (solve diag)
+    int st0, st1;           // solve row tiles
+    int maxnc;
+    size_t small_smem_elems, diag_smem_elems, trsm_smem_elems;
+};
+
+struct Device {
+    bool ready = false;
+    int dev = -1;
+    cudaStream_t stream = nullptr;
+    // structure
+    DBuf<int> cb_fcol, cb_lcol, cb_stride, cb_fblok, bk_frow, bk_lrow, bk_rowoff, bk_fcblk, rowidx;
+    DBuf<int64_t> cb_coef, cb_rowidx;
+    DBuf<pgpu::TaskDev> tasks;
+    DBuf<int> small_list, large_list, level_cblks;
+    DBuf<pgpu::RowTile> trsm_tiles, solve_tiles;
+    DBuf<pgpu::UpdTile> upd_tiles;
+    // matrix
+    DBuf<double> vals, csr_val;
+    DBuf<int64_t> lmap, umap, csr_src, perm;
+    DBuf<int> csr_rowptr, csr_col, e_row, e_col;
+    // factor
+    DBuf<unsigned char> Lc, Uc;
+    int fltsize = 0;
+    // work
+    DBuf<int> counters;      // [0] nbpivots, [1] status
+    DBuf<double> part, scal; // reduction partials, scalars
+    DBuf<double> w1, w2;     // permuted double work vectors
+    DBuf<float> wf;          // float work for mixed precision
+    pgpu::DevStruct ds{};
+};
+
+}  // namespace
+
+struct pastix_rhs_s {
+    int8_t allocated;
+    int flttype;           // SpmDouble or SpmFloat
+    pastix_int_t m, n, ld;
+    void *b;               // device memory, permuted numbering
+};
+
+struct pastix_data_s {
+    pastix_int_t *iparm = nullptr;
+    double *dparm = nullptr;
+    int steps = 0;
+    // analysed pattern
+    idx_t n = 0, nnz = 0;
+    int mtxtype = SpmGeneral;
+    std::vector<idx_t> colptr, rowind;  // 0-based copy of the pattern
+    pgpu::Graph graph;
+    pgpu::Order order;
+    bool user_order = false;
+    pgpu::Symbol symbol;
+    pgpu::Solver solver;
+    // value maps (host, structure only)
+    std::vector<int64_t> lmap, umap, csr_src;
+    std::vector<int> csr_rowptr, csr_col, e_row, e_col;
+    idx_t csr_nnz = 0;
+    std::vector<LevelLists> levels;
+    // host copies of the launch lists
+    std::vector<int> small_list, large_list, level_cblks;
+    std::vector<pgpu::RowTile> trsm_tiles, solve_tiles;
+    std::vector<pgpu::UpdTile> upd_tiles;
+    std::vector<pgpu::TaskDev> tasks;
+    int factotype = PastixFactPOTRF;
+    int mixed = 0;
+    double anorm = 0.0;
+    Device dev;
+};
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+static void perr(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    fprintf(stderr, "pastix_b200: ");
+    vfprintf(stderr, fmt, ap);
+    fprintf(stderr, "\n");
+    va_end(ap);
+}
+
+#define CUDA_TRY(call)                                                                    \
+    do {                                                                                  \
+        cudaError_t _e = (call);                                                          \
+        if (_e != cudaSuccess) {                                                          \
+            perr("%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, __LINE__); \
+            return PASTIX_ERR_INTERNAL;                                                   \
+        }                                                                                 \
+    } while (0)
+
+static double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+static int fact_kind(const pastix_data_t *pd) {
+    int f = pd->factotype;
+    if (f == PastixFactLLT || f == PastixFactPOTRF) return pgpu::FACT_POTRF;
+    if (f == PastixFactLDLT || f == PastixFactHETRF) return pgpu::FACT_SYTRF;
+    return pgpu::FACT_GETRF;
+}
+
+// ---------------------------------------------------------------------------
+// parameters (common/api.c:420-571)
+// ---------------------------------------------------------------------------
+extern "C" void pastixInitParam(pastix_int_t *iparm, double *dparm) {
+    if (!iparm || !dparm) return;
+    for (int i = 0; i < IPARM_SIZE; i++) iparm[i] = 0;
+    for (int i = 0; i < DPARM_SIZE; i++) dparm[i] = 0.0;
+    iparm[IPARM_VERBOSE] = PastixVerboseNo;
+    iparm[IPARM_ORDERING] = PastixOrderScotch;
+    iparm[IPARM_ORDERING_DEFAULT] = 1;
+    iparm[IPARM_SCOTCH_MT] = 1;
+    iparm[IPARM_SCOTCH_SWITCH_LEVEL] = 120;
+    iparm[IPARM_SCOTCH_CMAX] = 100000;
+    iparm[IPARM_SCOTCH_FRAT] = 8;
+    iparm[IPARM_METIS_CTYPE] = -1;
+    iparm[IPARM_METIS_RTYPE] = -1;
+    iparm[IPARM_METIS_NSEPS] = 1;
+    iparm[IPARM_METIS_NITER] = 10;
+    iparm[IPARM_METIS_UFACTOR] = 200;
+    iparm[IPARM_METIS_COMPRESS] = 1;
+    iparm[IPARM_METIS_SEED] = 3452;
+    iparm[IPARM_AMALGAMATION_LVLCBLK] = 5;
+    iparm[IPARM_AMALGAMATION_LVLBLAS] = 5;
+    iparm[IPARM_REORDERING_STOP] = INT64_MAX;
+    iparm[IPARM_SPLITTING_STRATEGY] = 1;  // PastixSplitKway
+    iparm[IPARM_SPLITTING_LEVELS_KWAY] = INT64_MAX;
+    iparm[IPARM_SPLITTING_PROJECTIONS_DEPTH] = 3;
+    iparm[IPARM_SPLITTING_PROJECTIONS_DISTANCE] = 3;
+    iparm[IPARM_SPLITTING_PROJECTIONS_WIDTH] = 1;
+    iparm[IPARM_MIN_BLOCKSIZE] = 160;
+    iparm[IPARM_MAX_BLOCKSIZE] = 320;
+    iparm[IPARM_TASKS2D_LEVEL] = -1;
+    iparm[IPARM_TASKS2D_WIDTH] = 160;
+    iparm[IPARM_FACTORIZATION] = PastixFactLU;
+    iparm[IPARM_FACTO_LOOK_SIDE] = 1;  // PastixFactRightLooking
+    iparm[IPARM_TRANSPOSE_SOLVE] = PastixNoTrans;
+    iparm[IPARM_APPLYPERM_WS] = 1;
+    iparm[IPARM_REFINEMENT] = PastixRefineGMRES;
+    iparm[IPARM_ITERMAX] = 250;
+    iparm[IPARM_GMRES_IM] = 25;
+    iparm[IPARM_SCHEDULER] = PastixSchedDynamic;
+    iparm[IPARM_THREAD_NBR] = -1;
+    iparm[IPARM_SOCKET_NBR] = -1;
+    iparm[IPARM_GPU_NBR] = 1;
+    iparm[IPARM_GPU_MEMORY_PERCENTAGE] = 95;
+    iparm[IPARM_GPU_MEMORY_BLOCK_SIZE] = 32 * 1024;
+    iparm[IPARM_COMPRESS_MIN_WIDTH] = 128;
+    iparm[IPARM_COMPRESS_MIN_HEIGHT] = 20;
+    iparm[IPARM_COMPRESS_METHOD] = 1;  // PQRCP
+    iparm[IPARM_COMPRESS_PRESELECT] = 1;
+    iparm[IPARM_COMPRESS_ILUK] = -2;
+    iparm[IPARM_MODIFY_PARAMETER] = 1;
+    iparm[IPARM_START_TASK] = PastixTaskOrdering;
+    iparm[IPARM_END_TASK] = PastixTaskClean;
+    iparm[IPARM_FLOAT] = -1;
+    iparm[IPARM_MTX_TYPE] = -1;
+    iparm[IPARM_DOF_NBR] = 1;
+    dparm[DPARM_EPSILON_REFINEMENT] = -1.;
+    dparm[DPARM_RELATIVE_ERROR] = -1.;
+    dparm[DPARM_EPSILON_MAGN_CTRL] = 0.;
+    dparm[DPARM_COMPRESS_TOLERANCE] = 0.01;
+    dparm[DPARM_COMPRESS_MIN_RATIO] = 1.0;
+}
+
+extern "C" void pastixInit(pastix_data_t **pd, PASTIX_Comm, pastix_int_t *iparm, double *dparm) {
+    if (!pd) return;
+    *pd = nullptr;
+    if (!iparm || !dparm) {
+        perr("pastixInit: iparm and dparm must be given (call pastixInitParam first)");
+        return;
+    }
+    pastix_data_t *p = new pastix_data_t();
+    p->iparm = iparm;
+    p->dparm = dparm;
+    p->steps = STEP_INIT;
+    *pd = p;
+}
+
+extern "C" void pastixInitWithAffinity(pastix_data_t **pd, PASTIX_Comm c, pastix_int_t *iparm, double *dparm,
+                                       const int *) {
+    pastixInit(pd, c, iparm, dparm);
+}
+
+extern "C" void pastixFinalize(pastix_data_t **pd) {
+    if (!pd || !*pd) return;
+    pastix_data_t *p = *pd;
+    if (p->dev.ready) {
+        cudaSetDevice(p->dev.dev);
+        cudaStreamSynchronize(p->dev.stream);
+    }
+    cudaStream_t st = p->dev.stream;
+    delete p;  // DBuf destructors free device memory
+    if (st) cudaStreamDestroy(st);
+    *pd = nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// ordering
+// ---------------------------------------------------------------------------
+extern "C" int pastixOrderGrid(pastix_order_t **myorder, pastix_int_t nx, pastix_int_t ny, pastix_int_t nz) {
+    if (!myorder || !*myorder || nx < 1 || ny < 1 || nz < 1) return PASTIX_ERR_BADPARAMETER;
+    pgpu::Order o;
+    try {
+        pgpu::order_grid(o, nx, ny, nz);
+    } catch (const std::exception &e) {
+        perr("pastixOrderGrid: %s", e.what());
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    pastix_order_t *ord = *myorder;
+    memset(ord, 0, sizeof(*ord));
+    ord->baseval = 0;
+    ord->vertnbr = o.n;
+    ord->cblknbr = o.cblknbr;
+    auto dup = [](const std::vector<idx_t> &v) {
+        pastix_int_t *p = (pastix_int_t *)malloc(std::max<size_t>(1, v.size()) * sizeof(pastix_int_t));
+        if (!v.empty()) memcpy(p, v.data(), v.size() * sizeof(pastix_int_t));
+        return p;
+    };
+    ord->permtab = dup(o.permtab);
+    ord->peritab = dup(o.peritab);
+    ord->rangtab = dup(o.rangtab);
+    ord->treetab = dup(o.treetab);
+    return PASTIX_SUCCESS;
+}
+
+extern "C" void pastixOrderExit(pastix_order_t *o) {
+    if (!o) return;
+    free(o->permtab);
+    free(o->peritab);
+    free(o->rangtab);
+    free(o->treetab);
+    free(o->selevtx);
+    free(o->sndetab);
+    free(o->peritab_exp);
+    memset(o, 0, sizeof(*o));
+}
+
+static int check_spm(const spmatrix_t *spm) {
+    if (!spm) { perr("spm is NULL"); return PASTIX_ERR_BADPARAMETER; }
+    if (spm->fmttype != SpmCSC) { perr("only CSC input is supported"); return PASTIX_ERR_BADPARAMETER; }
+    if (spm->mtxtype != SpmGeneral && spm->mtxtype != SpmSymmetric) {
+        perr("mtxtype must be SpmGeneral or SpmSymmetric (real arithmetic)");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    if (spm->dof != 1 && spm->dof != 0) { perr("give dof>1 matrices expanded (dof = 1)"); return PASTIX_ERR_BADPARAMETER; }
+    if (spm->n <= 0 || !spm->colptr || (spm->nnz > 0 && !spm->rowptr)) return PASTIX_ERR_BADPARAMETER;
+    if (spm->baseval != 0 && spm->baseval != 1) return PASTIX_ERR_BADPARAMETER;
+    return PASTIX_SUCCESS;
+}
+
+// pastix_subtask_order (order/pastix_subtask_order.c:100): build the graph and
+// the ordering.  PastixOrderPersonal uses the given order (grid or user
+// permutation); any other value uses the built-in nested dissection of the
+// graph, since Scotch and Metis are not part of this library.
+extern "C" int pastix_subtask_order(pastix_data_t *pd, const spmatrix_t *spm, pastix_order_t *myorder) {
+    if (!pd) return PASTIX_ERR_BADPARAMETER;
+    int rc = check_spm(spm);
+    if (rc) return rc;
+    const idx_t n = spm->n, b = spm->baseval, nnz = spm->colptr[n] - b;
+    pd->n = n;
+    pd->nnz = nnz;
+    pd->mtxtype = spm->mtxtype;
+    pd->colptr.assign(n + 1, 0);
+    pd->rowind.assign(nnz, 0);
+    for (idx_t j = 0; j <= n; j++) pd->colptr[j] = spm->colptr[j] - b;
+    for (idx_t e = 0; e < nnz; e++) {
+        idx_t r = spm->rowptr[e] - b;
+        if (r < 0 || r >= n) { perr("row index out of range"); return PASTIX_ERR_BADPARAMETER; }
+        pd->rowind[e] = r;
+    }
+    for (idx_t j = 0; j < n; j++)
+        if (pd->colptr[j + 1] < pd->colptr[j]) return PASTIX_ERR_BADPARAMETER;
+    // symmetric graph without the diagonal
+    {
+        std::vector<idx_t> deg(n + 1, 0);
+        for (idx_t j = 0; j < n; j++)
+            for (idx_t e = pd->colptr[j]; e < pd->colptr[j + 1]; e++) {
+                idx_t i = pd->rowind[e];
+                if (i != j) { deg[i + 1]++; deg[j + 1]++; }
+            }
+        for (idx_t i = 0; i < n; i++) deg[i + 1] += deg[i];
+        std::vector<idx_t> adj(deg[n]);
+        std::vector<idx_t> pos(deg.begin(), deg.end() - 1);
+        for (idx_t j = 0; j < n; j++)
+            for (idx_t e = pd->colptr[j]; e < pd->colptr[j + 1]; e++) {
+                idx_t i = pd->rowind[e];
+                if (i != j) { adj[pos[i]++] = j; adj[pos[j]++] = i; }
+            }
+        pd->graph.n = n;
+        pd->graph.colptr.assign(n + 1, 0);
+        pd->graph.rowind.clear();
+        pd->graph.rowind.reserve(adj.size());
+        for (idx_t i = 0; i < n; i++) {
+            auto b0 = adj.begin() + deg[i], b1 = adj.begin() + deg[i + 1];
+            std::sort(b0, b1);
+            auto e1 = std::unique(b0, b1);
+            pd->graph.rowind.insert(pd->graph.rowind.end(), b0, e1);
+            pd->graph.colptr[i + 1] = (idx_t)pd->graph.rowind.size();
+        }
+    }
+    pgpu::Order &o = pd->order;
+    o = pgpu::Order{};
+    if (pd->iparm[IPARM_ORDERING] == PastixOrderPersonal && myorder && myorder->permtab) {
+        idx_t vn = myorder->vertnbr, ob = myorder->baseval;
+        if (vn <= 0 || n % vn != 0) { perr("personal order size mismatch"); return PASTIX_ERR_BADPARAMETER; }
+        o.n = vn;
+        o.permtab.resize(vn);
+        o.peritab.resize(vn);
+        for (idx_t i = 0; i < vn; i++) o.permtab[i] = myorder->permtab[i] - ob;
+        if (myorder->peritab)
+            for (idx_t i = 0; i < vn; i++) o.peritab[i] = myorder->peritab[i] - ob;
+        else
+            for (idx_t i = 0; i < vn; i++) o.peritab[o.permtab[i]] = i;
+        if (myorder->rangtab && myorder->treetab && myorder->cblknbr > 0) {
+            o.cblknbr = myorder->cblknbr;
+            o.rangtab.resize(o.cblknbr + 1);
+            o.treetab.resize(o.cblknbr);
+            for (idx_t k = 0; k <= o.cblknbr; k++) o.rangtab[k] = myorder->rangtab[k] - ob;
+            for (idx_t k = 0; k < o.cblknbr; k++) o.treetab[k] = myorder->treetab[k] < 0 ? -1 : myorder->treetab[k] - ob;
+        }
+        if (vn != n) pgpu::order_expand_dof(o, n / vn);  // node ordering of a dof>1 matrix
+        pd->user_order = true;
+    } else {
+        // identity start; nested dissection of the graph is applied below
+        o.n = n;
+        o.permtab.resize(n);
+        o.peritab.resize(n);
+        pgpu::order_nd_graph(o, pd->graph);
+        pd->user_order = false;
+    }
+    if (o.rangtab.empty()) pgpu::order_find_supernodes(o, pd->graph);
+    std::string err = pgpu::order_check(o);
+    if (!err.empty()) { perr("ordering check failed: %s", err.c_str()); return PASTIX_ERR_BADPARAMETER; }
+    pd->steps = STEP_INIT | STEP_ORDERING;
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pastix_subtask_symbfact(pastix_data_t *pd) {
+    if (!pd || !(pd->steps & STEP_ORDERING)) {
+        perr("pastix_subtask_symbfact: pastix_subtask_order() has to be called first");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    double t0 = now_s();
+    pgpu::symbol_fax(pd->symbol, pd->graph, pd->order);
+    pd->dparm[DPARM_SYMBFACT_TIME] = now_s() - t0;
+    pd->steps |= STEP_SYMBFACT;
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pastix_subtask_reordering(pastix_data_t *pd) {
+    if (!pd || !(pd->steps & STEP_SYMBFACT)) return PASTIX_ERR_BADPARAMETER;
+    pd->dparm[DPARM_REORDER_TIME] = 0.0;
+    return PASTIX_SUCCESS;
+}
+
+// Host-side construction of the value maps and of the launch lists.
+static int build_maps_and_lists(pastix_data_t *pd) {
+    const pgpu::Solver &sv = pd->solver;
+    const idx_t n = pd->n, nnz = pd->nnz;
+    const auto &perm = pd->order.permtab;
+    const int fk = fact_kind(pd);
+    const bool sym = pd->mtxtype == SpmSymmetric;
+    // column -> cblk
+    std::vector<int> col2cb(n);
+    for (idx_t k = 0; k < sv.cblknbr; k++)
+        for (idx_t c = sv.cb_fcol[k]; c <= sv.cb_lcol[k]; c++) col2cb[c] = (int)k;
+    auto rowpos = [&](idx_t k, idx_t r) -> idx_t {
+        idx_t lo = sv.cb_fblok[k], hi = sv.cb_fblok[k + 1] - 1;
+        while (lo < hi) {
+            idx_t mid = (lo + hi + 1) / 2;
+            if (sv.bk_frow[mid] <= r) lo = mid; else hi = mid - 1;
+        }
+        if (r < sv.bk_frow[lo] || r > sv.bk_lrow[lo]) return -1;
+        return sv.bk_rowoff[lo] + (r - sv.bk_frow[lo]);
+    };
+    auto coefpos = [&](idx_t r, idx_t c) -> int64_t {  // lower position (r >= c) in the L-shaped panel
+        idx_t k = col2cb[c];
+        idx_t rp = rowpos(k, r);
+        if (rp < 0) return -2;
+        return sv.cb_coef[k] + rp + (c - sv.cb_fcol[k]) * sv.cb_stride[k];
+    };
+    pd->lmap.assign(nnz, -1);
+    pd->umap.clear();
+    if (fk == pgpu::FACT_GETRF) pd->umap.assign(nnz, -1);
+    pd->e_row.resize(nnz);
+    pd->e_col.resize(nnz);
+    std::vector<std::pair<idx_t, idx_t>> ent;  // (permuted row, permuted col) of the full matrix, with source
+    std::vector<int64_t> src;
+    ent.reserve(sym ? 2 * nnz : nnz);
+    src.reserve(sym ? 2 * nnz : nnz);
+    for (idx_t j = 0; j < n; j++) {
+        for (idx_t e = pd->colptr[j]; e < pd->colptr[j + 1]; e++) {
+            idx_t i = pd->rowind[e];
+            pd->e_row[e] = (int)i;
+            pd->e_col[e] = (int)j;
+            idx_t pi = perm[i], pj = perm[j];
+            ent.emplace_back(pi, pj);
+            src.push_back(e);
+            if (sym && pi != pj) { ent.emplace_back(pj, pi); src.push_back(e); }
+            idx_t r = std::max(pi, pj), c = std::min(pi, pj);
+            if (sym) {
+                int64_t p = coefpos(r, c);
+                if (p == -2) { perr("entry outside the symbolic structure"); return PASTIX_ERR_INTERNAL; }
+                pd->lmap[e] = p;
+                if (fk == pgpu::FACT_GETRF && pi != pj) pd->umap[e] = p;
+            } else if (pi >= pj) {
+                int64_t p = coefpos(pi, pj);
+                if (p == -2) { perr("entry outside the symbolic structure"); return PASTIX_ERR_INTERNAL; }
+                pd->lmap[e] = p;
+            } else if (fk == pgpu::FACT_GETRF) {
+                int64_t p = coefpos(pj, pi);
+                if (p == -2) { perr("entry outside the symbolic structure"); return PASTIX_ERR_INTERNAL; }
+                pd->umap[e] = p;
+            }
+        }
+    }
+    // CSR of the permuted full matrix (counting sort by row, then by column)
+    idx_t fn = (idx_t)ent.size();
+    pd->csr_nnz = fn;
+    if (fn >= (idx_t)INT32_MAX) { perr("matrix too large for 32-bit CSR"); return PASTIX_ERR_INTEGER_TYPE; }
+    std::vector<idx_t> order(fn);
+    {
+        std::vector<idx_t> cnt(n + 1, 0), tmp(fn);
+        for (idx_t p = 0; p < fn; p++) cnt[ent[p].second + 1]++;
+        for (idx_t i = 0; i < n; i++) cnt[i + 1] += cnt[i];
+        for (idx_t p = 0; p < fn; p++) tmp[cnt[ent[p].second]++] = p;
+        std::fill(cnt.begin(), cnt.end(), 0);
+        for (idx_t p = 0; p < fn; p++) cnt[ent[p].first + 1]++;
+        for (idx_t i = 0; i < n; i++) cnt[i + 1] += cnt[i];
+        pd->csr_rowptr.assign(n + 1, 0);
+        for (idx_t i = 0; i <= n; i++) pd->csr_rowptr[i] = (int)cnt[i];
+        for (idx_t q = 0; q < fn; q++) {
+            idx_t p = tmp[q];
+            order[cnt[ent[p].first]++] = p;
+        }
+    }
+    pd->csr_col.resize(fn);
+    pd->csr_src.resize(fn);
+    for (idx_t q = 0; q < fn; q++) {
+        pd->csr_col[q] = (int)ent[order[q]].second;
+        pd->csr_src[q] = src[order[q]];
+        if (q > 0 && pd->csr_col[q] == pd->csr_col[q - 1]) {
+            idx_t row = std::upper_bound(pd->csr_rowptr.begin(), pd->csr_rowptr.end(), (int)q) - pd->csr_rowptr.begin() - 1;
+            if (pd->csr_rowptr[row] != (int)q) {
+                perr("duplicate entry in the matrix (symmetric matrices store one triangle)");
+                return PASTIX_ERR_BADPARAMETER;
+            }
+        }
+    }
+
+    // ---- launch lists per level ----
+    pd->levels.assign(sv.nlevels, LevelLists{});
+    pd->small_list.clear(); pd->large_list.clear(); pd->level_cblks.clear();
+    pd->trsm_tiles.clear(); pd->solve_tiles.clear(); pd->upd_tiles.clear();
+    // exclusive tasks: dst targeted by a single source in the level
+    pd->tasks.resize(sv.tasks.size());
+    {
+        std::vector<int> last_src(sv.cblknbr, -1), nsrc(sv.cblknbr, 0);
+        for (idx_t l = 0; l < sv.nlevels; l++) {
+            for (idx_t t = sv.lvl_task_ptr[l]; t < sv.lvl_task_ptr[l + 1]; t++) {
+                const auto &tk = sv.tasks[t];
+                if (last_src[tk.dst] != (int)tk.src) {
+                    if (last_src[tk.dst] == -1 || nsrc[tk.dst] == 0) nsrc[tk.dst] = 0;
+                    nsrc[tk.dst]++;
+                    last_src[tk.dst] = (int)tk.src;
+                }
+            }
+            for (idx_t t = sv.lvl_task_ptr[l]; t < sv.lvl_task_ptr[l + 1]; t++) {
+                const auto &tk = sv.tasks[t];
+                pgpu::TaskDev d;
+                d.src = (int)tk.src; d.dst = (int)tk.dst; d.row0 = (int)tk.row0; d.n = (int)tk.n; d.m = (int)tk.m;
+                d.excl = nsrc[tk.dst] == 1 ? 1 : 0;
+                pd->tasks[t] = d;
+            }
+            for (idx_t t = sv.lvl_task_ptr[l]; t < sv.lvl_task_ptr[l + 1]; t++) {
+                last_src[sv.tasks[t].dst] = -1;
+                nsrc[sv.tasks[t].dst] = 0;
+            }
+        }
+    }
+    const int SR = pgpu::solve_rows_per_tile();
+    for (idx_t l = 0; l < sv.nlevels; l++) {
+        LevelLists &L = pd->levels[l];
+        L.small0 = (int)pd->small_list.size();
+        L.large0 = (int)pd->large_list.size();
+        L.trsm0 = (int)pd->trsm_tiles.size();
+        L.cb0 = (int)pd->level_cblks.size();
+        L.st0 = (int)pd->solve_tiles.size();
+        L.maxnc = 1;
+        L.small_smem_elems = L.diag_smem_elems = L.trsm_smem_elems = 0;
+        for (idx_t p = sv.lvl_ptr[l]; p < sv.lvl_ptr[l + 1]; p++) {
+            idx_t k = sv.lvl_cblk[p];
+            idx_t nc = sv.cb_lcol[k] - sv.cb_fcol[k] + 1, st = sv.cb_stride[k];
+            L.maxnc = std::max<int>(L.maxnc, (int)nc);
+            pd->level_cblks.push_back((int)k);
+            if (st * nc <= SMALL_PANEL_ELEMS) {
+                pd->small_list.push_back((int)k);
+                L.small_smem_elems = std::max<size_t>(L.small_smem_elems, (size_t)(st * nc) * (fk == pgpu::FACT_GETRF ? 2 : 1));
+            } else {
+                pd->large_list.push_back((int)k);
+                L.diag_smem_elems = std::max<size_t>(L.diag_smem_elems, (size_t)32 * nc * (fk == pgpu::FACT_GETRF ? 2 : 1));
+                int bm = nc <= 160 ? 64 : 32;
+                for (idx_t r = nc; r < st; r += bm) pd->trsm_tiles.push_back(pgpu::RowTile{(int)k, (int)r});
+                if (st > nc) L.trsm_smem_elems = std::max<size_t>(L.trsm_smem_elems, (size_t)bm * nc);
+            }
+            for (idx_t r = nc; r < st; r += SR) pd->solve_tiles.push_back(pgpu::RowTile{(int)k, (int)r});
+        }
+        L.small1 = (int)pd->small_list.size();
+        L.large1 = (int)pd->large_list.size();
+        L.trsm1 = (int)pd->trsm_tiles.size();
+        L.cb1 = (int)pd->level_cblks.size();
+        L.st1 = (int)pd->solve_tiles.size();
+        L.upd0 = (int)pd->upd_tiles.size();
+        for (idx_t t = sv.lvl_task_ptr[l]; t < sv.lvl_task_ptr[l + 1]; t++) {
+            const auto &tk = sv.tasks[t];
+            const int B = 64;
+            for (int side = 0; side < (fk == pgpu::FACT_GETRF ? 2 : 1); side++) {
+                idx_t M = tk.m - (side ? tk.n : 0);
+                if (M <= 0) continue;
+                idx_t mt = (M + B - 1) / B, ntl = (tk.n + B - 1) / B;
+                for (idx_t a = 0; a < mt; a++)
+                    for (idx_t c = 0; c < ntl; c++) {
+                        // symmetric kinds: skip tiles strictly above the diagonal of the square part
+                        if (fk != pgpu::FACT_GETRF && (a + 1) * B <= c * B) continue;
+                        pd->upd_tiles.push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
+                    }
+            }
+        }
+        L.upd1 = (int)pd->upd_tiles.size();
+    }
+    return PASTIX_SUCCESS;
+}
+
+// pastix_subtask_blend (blend/pastix_subtask_blend.c:121): split, solver
+// structure, schedule.
+extern "C" int pastix_subtask_blend(pastix_data_t *pd) {
+    if (!pd || !(pd->steps & STEP_SYMBFACT)) {
+        perr("pastix_subtask_blend: pastix_subtask_symbfact() has to be called first");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    double t0 = now_s();
+    idx_t bmin = pd->iparm[IPARM_MIN_BLOCKSIZE], bmax = pd->iparm[IPARM_MAX_BLOCKSIZE];
+    if (bmin > bmax || bmin < 1) { perr("IPARM_MIN_BLOCKSIZE > IPARM_MAX_BLOCKSIZE"); return PASTIX_ERR_BADPARAMETER; }
+    pgpu::symbol_split(pd->symbol, bmin, bmax);
+    std::string err = pgpu::symbol_check(pd->symbol);
+    if (!err.empty()) { perr("symbol check failed: %s", err.c_str()); return PASTIX_ERR_INTERNAL; }
+    pd->factotype = (int)pd->iparm[IPARM_FACTORIZATION];
+    int fk = fact_kind(pd);
+    pgpu::solver_build(pd->solver, pd->symbol, fk);
+    int rc = build_maps_and_lists(pd);
+    if (rc) return rc;
+    pd->dparm[DPARM_FACT_THFLOPS] = pd->solver.thflops;
+    pd->iparm[IPARM_NNZEROS] = pd->solver.nnzl * (fk == pgpu::FACT_GETRF ? 2 : 1);
+    pd->dparm[DPARM_BLEND_TIME] = now_s() - t0;
+    pd->steps |= STEP_ANALYSE;
+    pd->dev.ready = false;  // structure changed: device copy must be rebuilt
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pastix_task_analyze(pastix_data_t *pd, const spmatrix_t *spm) {
+    if (!pd) return PASTIX_ERR_BADPARAMETER;
+    double t0 = now_s();
+    int rc = pastix_subtask_order(pd, spm, nullptr);
+    if (rc) return rc;
+    rc = pastix_subtask_symbfact(pd);
+    if (rc) return rc;
+    rc = pastix_subtask_reordering(pd);
+    if (rc) return rc;
+    rc = pastix_subtask_blend(pd);
+    pd->dparm[DPARM_ANALYZE_TIME] = now_s() - t0;
+    return rc;
+}
+
+extern "C" int pgpu_solver_info(const pastix_data_t *pd, pgpu_solver_info_t *info) {
+    if (!pd || !info || !(pd->steps & STEP_ANALYSE)) return PASTIX_ERR_BADPARAMETER;
+    const pgpu::Solver &sv = pd->solver;
+    info->n = sv.n;
+    info->cblknbr = sv.cblknbr;
+    info->bloknbr = sv.bloknbr;
+    info->coefnbr = sv.coefnbr;
+    info->nlevels = sv.nlevels;
+    info->ntasks = (pastix_int_t)sv.tasks.size();
+    info->cb_fcol = sv.cb_fcol.data();
+    info->cb_lcol = sv.cb_lcol.data();
+    info->cb_fblok = sv.cb_fblok.data();
+    info->cb_stride = sv.cb_stride.data();
+    info->cb_coef = sv.cb_coef.data();
+    info->cb_level = sv.cb_level.data();
+    info->bk_frow = sv.bk_frow.data();
+    info->bk_lrow = sv.bk_lrow.data();
+    info->bk_fcblk = sv.bk_fcblk.data();
+    info->bk_lcblk = sv.bk_lcblk.data();
+    info->bk_rowoff = sv.bk_rowoff.data();
+    info->permtab = pd->order.permtab.data();
+    info->peritab = pd->order.peritab.data();
+    info->thflops = sv.thflops;
+    return PASTIX_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// device residency
+// ---------------------------------------------------------------------------
+template <typename X>
+static std::vector<int> to_i32(const std::vector<X> &v) {
+    std::vector<int> r(v.size());
+    for (size_t i = 0; i < v.size(); i++) r[i] = (int)v[i];
+    return r;
+}
+
+static int device_setup(pastix_data_t *pd) {
+    Device &d = pd->dev;
+    if (d.ready) { CUDA_TRY(cudaSetDevice(d.dev)); return PASTIX_SUCCESS; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        perr("no CUDA device available: the numerical phase runs on the GPU only");
+        return PASTIX_ERR_INTERNAL;
+    }
+    if (d.dev < 0) CUDA_TRY(cudaGetDevice(&d.dev));
+    CUDA_TRY(cudaSetDevice(d.dev));
+    if (!d.stream) CUDA_TRY(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
+    cudaStream_t st = d.stream;
+    const pgpu::Solver &sv = pd->solver;
+    if (sv.n >= INT32_MAX || (idx_t)sv.rowidx.size() >= INT32_MAX) { perr("problem too large"); return PASTIX_ERR_INTEGER_TYPE; }
+    CUDA_TRY(d.cb_fcol.upload(to_i32(sv.cb_fcol), st));
+    CUDA_TRY(d.cb_lcol.upload(to_i32(sv.cb_lcol), st));
+    CUDA_TRY(d.cb_stride.upload(to_i32(sv.cb_stride), st));
+    CUDA_TRY(d.cb_fblok.upload(to_i32(sv.cb_fblok), st));
+    CUDA_TRY(d.bk_frow.upload(to_i32(sv.bk_frow), st));
+    CUDA_TRY(d.bk_lrow.upload(to_i32(sv.bk_lrow), st));
+    CUDA_TRY(d.bk_rowoff.upload(to_i32(sv.bk_rowoff), st));
+    CUDA_TRY(d.bk_fcblk.upload(to_i32(sv.bk_fcblk), st));
+    CUDA_TRY(d.rowidx.upload(to_i32(sv.rowidx), st));
+    std::vector<int64_t> coef(sv.cb_coef.begin(), sv.cb_coef.end()), ridx(sv.cb_rowidx.begin(), sv.cb_rowidx.end());
+    CUDA_TRY(d.cb_coef.upload(coef, st));
+    CUDA_TRY(d.cb_rowidx.upload(ridx, st));
+    CUDA_TRY(d.tasks.upload(pd->tasks, st));
+    CUDA_TRY(d.small_list.upload(pd->small_list, st));
+    CUDA_TRY(d.large_list.upload(pd->large_list, st));
+    CUDA_TRY(d.level_cblks.upload(pd->level_cblks, st));
+    CUDA_TRY(d.trsm_tiles.upload(pd->trsm_tiles, st));
+    CUDA_TRY(d.solve_tiles.upload(pd->solve_tiles, st));
+    CUDA_TRY(d.upd_tiles.upload(pd->upd_tiles, st));
+    CUDA_TRY(d.lmap.upload(pd->lmap, st));
+    if (!pd->umap.empty()) CUDA_TRY(d.umap.upload(pd->umap, st));
+    else d.umap.reset();
+    CUDA_TRY(d.csr_src.upload(pd->csr_src, st));
+    CUDA_TRY(d.csr_rowptr.upload(pd->csr_rowptr, st));
+    CUDA_TRY(d.csr_col.upload(pd->csr_col, st));
+    CUDA_TRY(d.e_row.upload(pd->e_row, st));
+    CUDA_TRY(d.e_col.upload(pd->e_col, st));
+    std::vector<int64_t> perm(pd->order.permtab.begin(), pd->order.permtab.end());
+    CUDA_TRY(d.perm.upload(perm, st));
+    CUDA_TRY(d.vals.alloc(std::max<idx_t>(1, pd->nnz)));
+    CUDA_TRY(d.csr_val.alloc(std::max<idx_t>(1, pd->csr_nnz)));
+    CUDA_TRY(d.counters.alloc(4));
+    CUDA_TRY(cudaMemsetAsync(d.counters.p, 0, 4 * sizeof(int), st));
+    CUDA_TRY(d.part.alloc(pgpu::reduce_partials()));
+    CUDA_TRY(d.scal.alloc(64));
+    pgpu::DevStruct &s = d.ds;
+    s.n = (int)sv.n;
+    s.cblknbr = (int)sv.cblknbr;
+    s.cb_fcol = d.cb_fcol.p; s.cb_lcol = d.cb_lcol.p; s.cb_stride = d.cb_stride.p; s.cb_fblok = d.cb_fblok.p;
+    s.cb_coef = d.cb_coef.p; s.cb_rowidx = d.cb_rowidx.p;
+    s.bk_frow = d.bk_frow.p; s.bk_lrow = d.bk_lrow.p; s.bk_rowoff = d.bk_rowoff.p; s.bk_fcblk = d.bk_fcblk.p;
+    s.rowidx = d.rowidx.p;
+    s.tasks = d.tasks.p;
+    static bool attrs = false;
+    if (!attrs) {
+        const size_t mx = 220 * 1024;
+        CUDA_TRY((pgpu::set_smem_attrs<double, pgpu::FACT_POTRF>(mx, mx, mx)));
+        CUDA_TRY((pgpu::set_smem_attrs<double, pgpu::FACT_SYTRF>(mx, mx, mx)));
+        CUDA_TRY((pgpu::set_smem_attrs<double, pgpu::FACT_GETRF>(mx, mx, mx)));
+        CUDA_TRY((pgpu::set_smem_attrs<float, pgpu::FACT_POTRF>(mx, mx, mx)));
+        CUDA_TRY((pgpu::set_smem_attrs<float, pgpu::FACT_SYTRF>(mx, mx, mx)));
+        CUDA_TRY((pgpu::set_smem_attrs<float, pgpu::FACT_GETRF>(mx, mx, mx)));
+        attrs = true;
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    d.ready = true;
+    return PASTIX_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// numerical factorization
+// ---------------------------------------------------------------------------
+template <typename T, int F>
+static int run_factor(pastix_data_t *pd, double criterion) {
+    Device &d = pd->dev;
+    cudaStream_t st = d.stream;
+    T *L = reinterpret_cast<T *>(d.Lc.p);
+    T *U = reinterpret_cast<T *>(d.Uc.p);
+    pgpu::FactParams fp{criterion, d.counters.p, d.counters.p + 1};
+    for (size_t l = 0; l < pd->levels.size(); l++) {
+        const LevelLists &lv = pd->levels[l];
+        pgpu::launch_panel_small<T, F>(d.ds, d.small_list.p + lv.small0, lv.small1 - lv.small0,
+                                       lv.small_smem_elems * sizeof(T), L, U, fp, st);
+        pgpu::launch_diag_large<T, F>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0,
+                                      lv.diag_smem_elems * sizeof(T), L, U, fp, st);
+        pgpu::launch_trsm<T, F>(d.ds, d.trsm_tiles.p + lv.trsm0, lv.trsm1 - lv.trsm0, 0,
+                                lv.trsm_smem_elems * sizeof(T), L, U, st);
+        pgpu::launch_update<T, F>(d.ds, d.upd_tiles.p + lv.upd0, lv.upd1 - lv.upd0, L, U, st);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return PASTIX_SUCCESS;
+}
+
+// spm values (host or device) -> device values
+static int upload_values(pastix_data_t *pd, const void *values, bool on_device, int flttype) {
+    Device &d = pd->dev;
+    if (flttype == SpmDouble) {
+        CUDA_TRY(cudaMemcpyAsync(d.vals.p, values, pd->nnz * sizeof(double),
+                                 on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, d.stream));
+    } else if (flttype == SpmFloat && !on_device) {
+        std::vector<double> tmp(pd->nnz);
+        const float *f = (const float *)values;
+        for (idx_t i = 0; i < pd->nnz; i++) tmp[i] = f[i];
+        CUDA_TRY(cudaMemcpyAsync(d.vals.p, tmp.data(), pd->nnz * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+        CUDA_TRY(cudaStreamSynchronize(d.stream));
+    } else {
+        perr("unsupported value type");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    return PASTIX_SUCCESS;
+}
+
+__global__ void k_gather_csr(int64_t nnz, const int64_t *__restrict__ src, const double *__restrict__ vals,
+                             double *__restrict__ out) {
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nnz; q += (int64_t)gridDim.x * blockDim.x)
+        out[q] = vals[src[q]];
+}
+
+// bcsc analogue: permuted CSR values + ||A||_F (sopalin/pastix_task_sopalin.c:93-160)
+static int values_to_csr(pastix_data_t *pd) {
+    Device &d = pd->dev;
+    int blocks = (int)std::min<int64_t>((pd->csr_nnz + 255) / 256, 148 * 16);
+    k_gather_csr<<<std::max(blocks, 1), 256, 0, d.stream>>>(pd->csr_nnz, d.csr_src.p, d.vals.p, d.csr_val.p);
+    pgpu::launch_dot(pd->csr_nnz, d.csr_val.p, d.csr_val.p, d.part.p, 1, d.scal.p, d.stream);
+    double nrm = 0;
+    CUDA_TRY(cudaMemcpyAsync(&nrm, d.scal.p, sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+    CUDA_TRY(cudaStreamSynchronize(d.stream));
+    pd->anorm = nrm;
+    pd->dparm[DPARM_A_NORM] = nrm;
+    return PASTIX_SUCCESS;
+}
+
+static int spm2bcsc_common(pastix_data_t *pd, const void *values, bool on_device, int flttype) {
+    if (!(pd->steps & STEP_ANALYSE)) {
+        perr("pastix_subtask_spm2bcsc: pastix_task_analyze() has to be called first");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    int rc = device_setup(pd);
+    if (rc) return rc;
+    rc = upload_values(pd, values, on_device, flttype);
+    if (rc) return rc;
+    rc = values_to_csr(pd);
+    if (rc) return rc;
+    pd->steps |= STEP_CSC2BCSC;
+    pd->steps &= ~(STEP_BCSC2CTAB | STEP_NUMFACT);
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pastix_subtask_spm2bcsc(pastix_data_t *pd, spmatrix_t *spm) {
+    if (!pd) return PASTIX_ERR_BADPARAMETER;
+    int rc = check_spm(spm);
+    if (rc) return rc;
+    if (spm->n != pd->n || spm->colptr[spm->n] - spm->baseval != pd->nnz) {
+        perr("pastix_subtask_spm2bcsc: the matrix does not match the analysed pattern");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    if (!spm->values) return PASTIX_ERR_BADPARAMETER;
+    return spm2bcsc_common(pd, spm->values, false, spm->flttype);
+}
+
+// coeftabInit (sopalin/coeftab.c:205): allocate and fill the panels
+extern "C" int pastix_subtask_bcsc2ctab(pastix_data_t *pd) {
+    if (!pd || !(pd->steps & STEP_CSC2BCSC)) {
+        perr("pastix_subtask_bcsc2ctab: pastix_subtask_spm2bcsc() has to be called first");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    Device &d = pd->dev;
+    CUDA_TRY(cudaSetDevice(d.dev));
+    pd->mixed = pd->iparm[IPARM_MIXED] ? 1 : 0;
+    const int fs = pd->mixed ? 4 : 8;
+    const int fk = fact_kind(pd);
+    const size_t bytes = (size_t)std::max<idx_t>(1, pd->solver.coefnbr) * fs;
+    if (d.Lc.n != bytes) CUDA_TRY(d.Lc.alloc(bytes));
+    if (fk == pgpu::FACT_GETRF) { if (d.Uc.n != bytes) CUDA_TRY(d.Uc.alloc(bytes)); }
+    else d.Uc.reset();
+    d.fltsize = fs;
+    CUDA_TRY(cudaMemsetAsync(d.Lc.p, 0, bytes, d.stream));
+    if (d.Uc.p) CUDA_TRY(cudaMemsetAsync(d.Uc.p, 0, bytes, d.stream));
+    const int64_t *um = d.Uc.p ? d.umap.p : nullptr;
+    if (pd->mixed)
+        pgpu::launch_fill_coef<float>(pd->nnz, d.vals.p, d.lmap.p, um, (float *)d.Lc.p, (float *)d.Uc.p, d.stream);
+    else
+        pgpu::launch_fill_coef<double>(pd->nnz, d.vals.p, d.lmap.p, um, (double *)d.Lc.p, (double *)d.Uc.p, d.stream);
+    CUDA_TRY(cudaGetLastError());
+    pd->dparm[DPARM_MEM_FR] = (double)bytes * (d.Uc.p ? 2 : 1);
+    pd->steps |= STEP_BCSC2CTAB;
+    return PASTIX_SUCCESS;
+}
+
+// pastix_subtask_sopalin (sopalin/pastix_task_sopalin.c:412-560)
+extern "C" int pastix_subtask_sopalin(pastix_data_t *pd) {
+    if (!pd || !(pd->steps & STEP_BCSC2CTAB)) {
+        perr("pastix_subtask_sopalin: pastix_subtask_bcsc2ctab() has to be called first");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    Device &d = pd->dev;
+    CUDA_TRY(cudaSetDevice(d.dev));
+    double *dparm = pd->dparm;
+    double threshold;
+    if (dparm[DPARM_EPSILON_MAGN_CTRL] < 0.) threshold = -dparm[DPARM_EPSILON_MAGN_CTRL];
+    else if (dparm[DPARM_EPSILON_MAGN_CTRL] == 0.) threshold = ldexp(1.0, -53) * pd->anorm;  // dlamch('e') * ||A||
+    else threshold = dparm[DPARM_EPSILON_MAGN_CTRL] * pd->anorm;
+    CUDA_TRY(cudaMemsetAsync(d.counters.p, 0, 2 * sizeof(int), d.stream));
+    CUDA_TRY(cudaStreamSynchronize(d.stream));
+    double t0 = now_s();
+    int fk = fact_kind(pd), rc;
+    if (pd->mixed) {
+        if (fk == pgpu::FACT_POTRF) rc = run_factor<float, pgpu::FACT_POTRF>(pd, threshold);
+        else if (fk == pgpu::FACT_SYTRF) rc = run_factor<float, pgpu::FACT_SYTRF>(pd, threshold);
+        else rc = run_factor<float, pgpu::FACT_GETRF>(pd, threshold);
+    } else {
+        if (fk == pgpu::FACT_POTRF) rc = run_factor<double, pgpu::FACT_POTRF>(pd, threshold);
+        else if (fk == pgpu::FACT_SYTRF) rc = run_factor<double, pgpu::FACT_SYTRF>(pd, threshold);
+        else rc = run_factor<double, pgpu::FACT_GETRF>(pd, threshold);
+    }
+    if (rc) return rc;
+    int cnt[2] = {0, 0};
+    CUDA_TRY(cudaMemcpyAsync(cnt, d.counters.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, d.stream));
+    CUDA_TRY(cudaStreamSynchronize(d.stream));
+    double t = now_s() - t0;
+    if (cnt[1] != 0) { perr("device status %d after factorization", cnt[1]); return PASTIX_ERR_INTERNAL; }
+    dparm[DPARM_FACT_TIME] = t;
+    dparm[DPARM_FACT_FLOPS] = t > 0 ? dparm[DPARM_FACT_THFLOPS] / t : 0.0;
+    dparm[DPARM_FACT_RLFLOPS] = dparm[DPARM_FACT_THFLOPS];
+    pd->iparm[IPARM_STATIC_PIVOTING] = cnt[0];
+    pd->steps |= STEP_NUMFACT;
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pastix_task_numfact(pastix_data_t *pd, spmatrix_t *spm) {
+    if (!pd) return PASTIX_ERR_BADPARAMETER;
+    int rc = pastix_subtask_spm2bcsc(pd, spm);
+    if (rc) return rc;
+    rc = pastix_subtask_bcsc2ctab(pd);
+    if (rc) return rc;
+    return pastix_subtask_sopalin(pd);
+}
+
+extern "C" int pgpu_numfact_device(pastix_data_t *pd, const double *values_dev) {
+    if (!pd || !values_dev) return PASTIX_ERR_BADPARAMETER;
+    int rc = spm2bcsc_common(pd, values_dev, true, SpmDouble);
+    if (rc) return rc;
+    rc = pastix_subtask_bcsc2ctab(pd);
+    if (rc) return rc;
+    return pastix_subtask_sopalin(pd);
+}
+
+extern "C" int pgpu_get_coeftab(const pastix_data_t *pd, void *L, void *U) {
+    if (!pd || !(pd->steps & STEP_NUMFACT) || !L) return PASTIX_ERR_BADPARAMETER;
+    const Device &d = pd->dev;
+    CUDA_TRY(cudaSetDevice(d.dev));
+    size_t bytes = (size_t)pd->solver.coefnbr * d.fltsize;
+    CUDA_TRY(cudaMemcpyAsync(L, d.Lc.p, bytes, cudaMemcpyDeviceToHost, d.stream));
+    if (U && d.Uc.p) CUDA_TRY(cudaMemcpyAsync(U, d.Uc.p, bytes, cudaMemcpyDeviceToHost, d.stream));
+    CUDA_TRY(cudaStreamSynchronize(d.stream));
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pgpu_device_status(const pastix_data_t *pd) {
+    if (!pd || !pd->dev.ready) return 0;
+    int cnt[2] = {0, 0};
+    if (cudaMemcpy(cnt, pd->dev.counters.p, 2 * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return cnt[1];
+}
+
+// ---------------------------------------------------------------------------
+// solve on permuted device vectors
+// ---------------------------------------------------------------------------
+// forward with panel P (lower), unit or not
+template <typename T>
+static void sweep_forward(pastix_data_t *pd, const T *P, int unit, T *Y, int ldy, int nrhs) {
+    Device &d = pd->dev;
+    for (size_t l = 0; l < pd->levels.size(); l++) {
+        const LevelLists &lv = pd->levels[l];
+        pgpu::launch_fwd_diag<T>(d.ds, d.level_cblks.p + lv.cb0, lv.cb1 - lv.cb0, lv.maxnc, P, unit, Y, ldy, nrhs,
+                                 d.stream);
+        pgpu::launch_fwd_update<T>(d.ds, d.solve_tiles.p + lv.st0, lv.st1 - lv.st0, lv.maxnc, P, Y, ldy, nrhs,
+                                   d.stream);
+    }
+}
+// backward: solve P^T x = y with P lower
+template <typename T>
+static void sweep_backward(pastix_data_t *pd, const T *P, int unit, T *Y, int ldy, int nrhs) {
+    Device &d = pd->dev;
+    for (size_t l = pd->levels.size(); l-- > 0;) {
+        const LevelLists &lv = pd->levels[l];
+        pgpu::launch_bwd_update<T>(d.ds, d.solve_tiles.p + lv.st0, lv.st1 - lv.st0, P, Y, ldy, nrhs, d.stream);
+        pgpu::launch_bwd_diag<T>(d.ds, d.level_cblks.p + lv.cb0, lv.cb1 - lv.cb0, lv.maxnc, P, unit, Y, ldy, nrhs,
+                                 d.stream);
+    }
+}
+
+// Solve A X = B (trans = 0) or A^T X = B (trans = 1) in place on permuted
+// device vectors of type T (the factor's arithmetic).
+template <typename T>
+static void solve_perm(pastix_data_t *pd, int trans, T *Y, int ldy, int nrhs) {
+    Device &d = pd->dev;
+    const T *L = reinterpret_cast<const T *>(d.Lc.p);
+    const T *U = reinterpret_cast<const T *>(d.Uc.p);
+    int fk = fact_kind(pd);
+    if (fk == pgpu::FACT_POTRF) {
+        sweep_forward<T>(pd, L, 0, Y, ldy, nrhs);
+        sweep_backward<T>(pd, L, 0, Y, ldy, nrhs);
+    } else if (fk == pgpu::FACT_SYTRF) {
+        sweep_forward<T>(pd, L, 1, Y, ldy, nrhs);
+        pgpu::launch_diag_scale<T>(d.ds, (int)pd->solver.cblknbr, L, Y, ldy, nrhs, d.stream);
+        sweep_backward<T>(pd, L, 1, Y, ldy, nrhs);
+    } else if (!trans) {  // L (unit) then U through U^T
+        sweep_forward<T>(pd, L, 1, Y, ldy, nrhs);
+        sweep_backward<T>(pd, U, 0, Y, ldy, nrhs);
+    } else {  // A^T = U^T L^T
+        sweep_forward<T>(pd, U, 0, Y, ldy, nrhs);
+        sweep_backward<T>(pd, L, 1, Y, ldy, nrhs);
+    }
+}
+
+// FP64 permuted vectors in, FP64 out; FP32 factors go through a float copy.
+static int solve_perm_d(pastix_data_t *pd, int trans, double *Y, int ldy, int nrhs) {
+    Device &d = pd->dev;
+    if (!pd->mixed) {
+        solve_perm<double>(pd, trans, Y, ldy, nrhs);
+    } else {
+        size_t need = (size_t)pd->n * nrhs;
+        if (d.wf.n < need) CUDA_TRY(d.wf.alloc(need));
+        for (int j = 0; j < nrhs; j++)
+            pgpu::launch_cast<double, float>(pd->n, Y + (size_t)j * ldy, d.wf.p + (size_t)j * pd->n, d.stream);
+        solve_perm<float>(pd, trans, d.wf.p, (int)pd->n, nrhs);
+        for (int j = 0; j < nrhs; j++)
+            pgpu::launch_cast<float, double>(pd->n, d.wf.p + (size_t)j * pd->n, Y + (size_t)j * ldy, d.stream);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return PASTIX_SUCCESS;
+}
+
+static int check_numfact(const pastix_data_t *pd, const char *who) {
+    if (!pd || !(pd->steps & STEP_NUMFACT)) {
+        perr("%s: pastix_task_numfact() has to be called first", who);
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    return PASTIX_SUCCESS;
+}
+
+// Device solve in the original numbering: B (n x nrhs, ld ldb) overwritten.
+static int solve_device_orig(pastix_data_t *pd, int trans, int nrhs, double *B, idx_t ldb, cudaStream_t user) {
+    Device &d = pd->dev;
+    CUDA_TRY(cudaSetDevice(d.dev));
+    const idx_t n = pd->n;
+    size_t need = (size_t)n * nrhs;
+    if (d.w1.n < need) CUDA_TRY(d.w1.alloc(need));
+    cudaEvent_t ev = nullptr;
+    if (user && user != d.stream) {  // order the library stream after the caller's stream
+        CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventRecord(ev, user));
+        CUDA_TRY(cudaStreamWaitEvent(d.stream, ev, 0));
+    }
+    pgpu::launch_permute<double, double>((int)n, nrhs, d.perm.p, 1, B, ldb, d.w1.p, n, d.stream);
+    int rc = solve_perm_d(pd, trans, d.w1.p, (int)n, nrhs);
+    if (rc) return rc;
+    pgpu::launch_permute<double, double>((int)n, nrhs, d.perm.p, 0, d.w1.p, n, B, ldb, d.stream);
+    if (ev) {
+        CUDA_TRY(cudaEventRecord(ev, d.stream));
+        CUDA_TRY(cudaStreamWaitEvent(user, ev, 0));
+        cudaEventDestroy(ev);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pgpu_solve_device(pastix_data_t *pd, pastix_int_t nrhs, double *B, pastix_int_t ldb, void *stream) {
+    int rc = check_numfact(pd, "pgpu_solve_device");
+    if (rc) return rc;
+    if (nrhs < 1 || ldb < pd->n || !B) return PASTIX_ERR_BADPARAMETER;
+    return solve_device_orig(pd, 0, (int)nrhs, B, ldb, (cudaStream_t)stream);
+}
+
+extern "C" int pgpu_solve_transposed_device(pastix_data_t *pd, pastix_int_t nrhs, double *B, pastix_int_t ldb,
+                                            void *stream) {
+    int rc = check_numfact(pd, "pgpu_solve_transposed_device");
+    if (rc) return rc;
+    if (nrhs < 1 || ldb < pd->n || !B) return PASTIX_ERR_BADPARAMETER;
+    return solve_device_orig(pd, 1, (int)nrhs, B, ldb, (cudaStream_t)stream);
+}
+
+extern "C" int pastix_task_solve(pastix_data_t *pd, pastix_int_t m, pastix_int_t nrhs, void *B, pastix_int_t ldb) {
+    int rc = check_numfact(pd, "pastix_task_solve");
+    if (rc) return rc;
+    if (m != pd->n || nrhs < 1 || ldb < m || !B) return PASTIX_ERR_BADPARAMETER;
+    Device &d = pd->dev;
+    CUDA_TRY(cudaSetDevice(d.dev));
+    double t0 = now_s();
+    DBuf<double> buf;
+    CUDA_TRY(buf.alloc((size_t)m * nrhs));
+    CUDA_TRY(cudaMemcpy2DAsync(buf.p, m * sizeof(double), B, ldb * sizeof(double), m * sizeof(double), nrhs,
+                               cudaMemcpyHostToDevice, d.stream));
+    int trans = pd->iparm[IPARM_TRANSPOSE_SOLVE] == PastixTrans ? 1 : 0;
+    rc = solve_device_orig(pd, trans, (int)nrhs, buf.p, m, d.stream);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpy2DAsync(B, ldb * sizeof(double), buf.p, m * sizeof(double), m * sizeof(double), nrhs,
+                               cudaMemcpyDeviceToHost, d.stream));
+    CUDA_TRY(cudaStreamSynchronize(d.stream));
+    pd->dparm[DPARM_SOLV_TIME] = now_s() - t0;
+    pd->steps |= STEP_SOLVE;
+    return PASTIX_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// subtask-level solve API on pastix_rhs_t (sopalin/pastix_task_solve.c)
+// ---------------------------------------------------------------------------
+extern "C" int pastixRhsInit(pastix_rhs_t *rhs) {
+    if (!rhs) return PASTIX_ERR_BADPARAMETER;
+    *rhs = (pastix_rhs_t)calloc(1, sizeof(struct pastix_rhs_s));
+    (*rhs)->flttype = SpmDouble;
+    return PASTIX_SUCCESS;
+}
+extern "C" int pastixRhsFinalize(pastix_rhs_t rhs) {
+    if (!rhs) return PASTIX_ERR_BADPARAMETER;
+    if (rhs->allocated && rhs->b) cudaFree(rhs->b);
+    free(rhs);
+    return PASTIX_SUCCESS;
+}
+static int rhs_alloc(pastix_rhs_t r, int flt, pastix_int_t m, pastix_int_t n) {
+    size_t es = flt == SpmFloat ? 4 : 8;
+    if (r->allocated && r->b) cudaFree(r->b);
+    r->b = nullptr;
+    CUDA_TRY(cudaMalloc(&r->b, std::max<size_t>(1, (size_t)m * n) * es));
+    r->allocated = 1;
+    r->flttype = flt;
+    r->m = m;
+    r->n = n;
+    r->ld = m;
+    return PASTIX_SUCCESS;
+}
+extern "C" int pastixRhsDoubletoSingle(const pastix_rhs_t dB, pastix_rhs_t sB) {
+    if (!dB || !sB || dB->flttype != SpmDouble) return PASTIX_ERR_BADPARAMETER;
+    int rc = rhs_alloc(sB, SpmFloat, dB->m, dB->n);
+    if (rc) return rc;
+    for (pastix_int_t j = 0; j < dB->n; j++)
+        pgpu::launch_cast<double, float>(dB->m, (const double *)dB->b + j * dB->ld, (float *)sB->b + j * sB->ld, 0);
+    CUDA_TRY(cudaDeviceSynchronize());
+    return PASTIX_SUCCESS;
+}
+extern "C" int pastixRhsSingleToDouble(const pastix_rhs_t sB, pastix_rhs_t dB) {
+    if (!dB || !sB || sB->flttype != SpmFloat || dB->flttype != SpmDouble || !dB->b) return PASTIX_ERR_BADPARAMETER;
+    for (pastix_int_t j = 0; j < sB->n; j++)
+        pgpu::launch_cast<float, double>(sB->m, (const float *)sB->b + j * sB->ld, (double *)dB->b + j * dB->ld, 0);
+    CUDA_TRY(cudaDeviceSynchronize());
+    return PASTIX_SUCCESS;
+}
+
+// Forward: B (host, original numbering) -> Bp (device, permuted, FP64).
+// Backward: Bp -> B.
+extern "C" int pastix_subtask_applyorder(pastix_data_t *pd, pastix_dir_t dir, pastix_int_t m, pastix_int_t n, void *B,
+                                         pastix_int_t ldb, pastix_rhs_t Bp) {
+    if (!pd || !(pd->steps & STEP_ANALYSE) || !Bp || m != pd->n || n < 1 || ldb < m || !B) return PASTIX_ERR_BADPARAMETER;
+    int rc = device_setup(pd);
+    if (rc) return rc;
+    Device &d = pd->dev;
+    DBuf<double> tmp;
+    CUDA_TRY(tmp.alloc((size_t)m * n));
+    if (dir == PastixDirForward) {
+        if (!(Bp->b && Bp->allocated && Bp->m == m && Bp->n == n && Bp->flttype == SpmDouble)) {
+            rc = rhs_alloc(Bp, SpmDouble, m, n);
+            if (rc) return rc;
+        }
+        CUDA_TRY(cudaMemcpy2DAsync(tmp.p, m * 8, B, ldb * 8, m * 8, n, cudaMemcpyHostToDevice, d.stream));
+        pgpu::launch_permute<double, double>((int)m, (int)n, d.perm.p, 1, tmp.p, m, (double *)Bp->b, Bp->ld, d.stream);
+    } else {
+        if (!Bp->b || Bp->flttype != SpmDouble) return PASTIX_ERR_BADPARAMETER;
+        pgpu::launch_permute<double, double>((int)m, (int)n, d.perm.p, 0, (const double *)Bp->b, Bp->ld, tmp.p, m, d.stream);
+        CUDA_TRY(cudaMemcpy2DAsync(B, ldb * 8, tmp.p, m * 8, m * 8, n, cudaMemcpyDeviceToHost, d.stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(d.stream));
+    return PASTIX_SUCCESS;
+}
+
+// pastix_subtask_trsm: one triangular sweep on a permuted device rhs
+// (side = Left only; uplo/trans/diag select the sweep as in the reference's
+// step table, sopalin/pastix_task_solve.c:543-649).
+extern "C" int pastix_subtask_trsm(pastix_data_t *pd, pastix_side_t side, pastix_uplo_t uplo, pastix_trans_t trans,
+                                   pastix_diag_t diag, pastix_rhs_t b) {
+    int rc = check_numfact(pd, "pastix_subtask_trsm");
+    if (rc) return rc;
+    if (side != PastixLeft || !b || !b->b) return PASTIX_ERR_BADPARAMETER;
+    Device &d = pd->dev;
+    int fk = fact_kind(pd);
+    int unit = diag == PastixUnit;
+    int isd = b->flttype == SpmDouble;
+    if ((pd->mixed && isd) || (!pd->mixed && !isd)) {
+        perr("pastix_subtask_trsm: rhs precision must match the factor's");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    // which panel: lower sweeps (uplo Lower, NoTrans) use L; upper sweeps use L^T,
+    // or U through the U^T panel for GETRF.
+    auto run = [&](auto *Y) {
+        using T = std::remove_pointer_t<decltype(Y)>;
+        const T *L = reinterpret_cast<const T *>(d.Lc.p);
+        const T *U = reinterpret_cast<const T *>(d.Uc.p);
+        if (uplo == PastixLower && trans == PastixNoTrans) sweep_forward<T>(pd, L, unit, Y, (int)b->ld, (int)b->n);
+        else if (uplo == PastixLower) sweep_backward<T>(pd, L, unit, Y, (int)b->ld, (int)b->n);
+        else if (uplo == PastixUpper && trans == PastixNoTrans)
+            sweep_backward<T>(pd, fk == pgpu::FACT_GETRF ? U : L, unit, Y, (int)b->ld, (int)b->n);
+        else sweep_forward<T>(pd, fk == pgpu::FACT_GETRF ? U : L, unit, Y, (int)b->ld, (int)b->n);
+    };
+    if (isd) run((double *)b->b);
+    else run((float *)b->b);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(d.stream));
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pastix_subtask_diag(pastix_data_t *pd, pastix_rhs_t b) {
+    int rc = check_numfact(pd, "pastix_subtask_diag");
+    if (rc) return rc;
+    if (!b || !b->b || fact_kind(pd) != pgpu::FACT_SYTRF) return PASTIX_ERR_BADPARAMETER;
+    Device &d = pd->dev;
+    if (b->flttype == SpmDouble && !pd->mixed)
+        pgpu::launch_diag_scale<double>(d.ds, (int)pd->solver.cblknbr, (const double *)d.Lc.p, (double *)b->b, (int)b->ld,
+                                        (int)b->n, d.stream);
+    else if (b->flttype == SpmFloat && pd->mixed)
+        pgpu::launch_diag_scale<float>(d.ds, (int)pd->solver.cblknbr, (const float *)d.Lc.p, (float *)b->b, (int)b->ld,
+                                       (int)b->n, d.stream);
+    else return PASTIX_ERR_BADPARAMETER;
+    CUDA_TRY(cudaStreamSynchronize(d.stream));
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pastix_subtask_solve_adv(pastix_data_t *pd, pastix_trans_t transA, pastix_rhs_t b) {
+    int rc = check_numfact(pd, "pastix_subtask_solve");
+    if (rc) return rc;
+    if (!b || !b->b || b->flttype != SpmDouble) return PASTIX_ERR_BADPARAMETER;
+    rc = solve_perm_d(pd, transA == PastixNoTrans ? 0 : 1, (double *)b->b, (int)b->ld, (int)b->n);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(pd->dev.stream));
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pastix_subtask_solve(pastix_data_t *pd, pastix_rhs_t b) {
+    return pastix_subtask_solve_adv(pd, PastixNoTrans, b);
+}
+
+// ---------------------------------------------------------------------------
+// refinement on the device (refinement/z_refine_*.c), one rhs at a time
+// ---------------------------------------------------------------------------
+namespace {
+struct Refiner {
+    pastix_data_t *pd;
+    Device &d;
+    int64_t n;
+    bool precond;
+    explicit Refiner(pastix_data_t *p) : pd(p), d(p->dev), n(p->n), precond((p->steps & STEP_NUMFACT) != 0) {}
+    double dot(const double *a, const double *b) {
+        pgpu::launch_dot(n, a, b, d.part.p, 0, d.scal.p, d.stream);
+        double v = 0;
+        cudaMemcpyAsync(&v, d.scal.p, sizeof(double), cudaMemcpyDeviceToHost, d.stream);
+        cudaStreamSynchronize(d.stream);
+        return v;
+    }
+    double norm(const double *a) {
+        pgpu::launch_dot(n, a, a, d.part.p, 1, d.scal.p, d.stream);
+        double v = 0;
+        cudaMemcpyAsync(&v, d.scal.p, sizeof(double), cudaMemcpyDeviceToHost, d.stream);
+        cudaStreamSynchronize(d.stream);
+        return v;
+    }
+    void spmv(double alpha, const double *x, double beta, double *y) {
+        pgpu::launch_spmv((int)n, pd->csr_nnz, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha, x, beta, y, d.stream);
+    }
+    void copy(const double *a, double *b) { cudaMemcpyAsync(b, a, n * 8, cudaMemcpyDeviceToDevice, d.stream); }
+    void axpy(double a, const double *x, double *y) { pgpu::launch_axpy(n, a, x, y, d.stream); }
+    void scal(double a, double *x) { pgpu::launch_scal(n, a, x, d.stream); }
+    int spsv(double *x) { return precond ? solve_perm_d(pd, 0, x, (int)n, 1) : 0; }
+};
+
+// GMRES(im), right preconditioned (refinement/z_refine_gmres.c:49-371)
+static int refine_gmres(Refiner &R, double *x, const double *b, double eps, int itermax, int im, int &iters_out) {
+    const int64_t n = R.n;
+    const int im1 = im + 1;
+    DBuf<double> V, W;
+    if (V.alloc((size_t)n * im1) || W.alloc((size_t)n * im)) return PASTIX_ERR_OUTOFMEMORY;
+    std::vector<double> H((size_t)im * im1, 0.0), gcos(im), gsin(im), G(im1);
+    DBuf<double> gdev;
+    if (gdev.alloc(im1)) return PASTIX_ERR_OUTOFMEMORY;
+    double normb = R.norm(b);
+    if (normb == 0.) normb = 1;
+    double normx = R.norm(x);
+    int iters = 0;
+    double resid_b = 0;
+    bool outflag = true;
+    while (outflag) {
+        double *v0 = V.p;
+        R.copy(b, v0);
+        if (normx > 0.) R.spmv(-1., x, 1., v0);
+        double resid = R.norm(v0);
+        resid_b = resid / normb;
+        if (resid_b <= eps) break;
+        R.scal(1.0 / resid, v0);
+        G[0] = resid;
+        int i = -1;
+        bool inflag = true;
+        while (inflag) {
+            i++;
+            double *Hi = H.data() + (size_t)i * im1;
+            double *Vi = V.p + (size_t)i * n;
+            double *Wi = W.p + (size_t)i * n;
+            R.copy(Vi, Wi);
+            if (R.spsv(Wi)) return PASTIX_ERR_INTERNAL;
+            double *Vn = Vi + n;
+            R.spmv(1.0, Wi, 0., Vn);
+            for (int j = 0; j <= i; j++) {
+                Hi[j] = R.dot(Vn, V.p + (size_t)j * n);
+                R.axpy(-Hi[j], V.p + (size_t)j * n, Vn);
+            }
+            double nrm = R.norm(Vn);
+            Hi[i + 1] = nrm;
+            if (nrm > 1e-50) R.scal(1.0 / nrm, Vn);
+            for (int j = 0; j < i; j++) {
+                double t = Hi[j];
+                Hi[j] = gcos[j] * t + gsin[j] * Hi[j + 1];
+                Hi[j + 1] = gcos[j] * Hi[j + 1] - gsin[j] * t;
+            }
+            double t = std::sqrt(Hi[i] * Hi[i] + Hi[i + 1] * Hi[i + 1]);
+            if (std::fabs(t) <= eps) t = eps;
+            gcos[i] = Hi[i] / t;
+            gsin[i] = Hi[i + 1] / t;
+            G[i + 1] = -gsin[i] * G[i];
+            G[i] = gcos[i] * G[i];
+            Hi[i] = gcos[i] * Hi[i] + gsin[i] * Hi[i + 1];
+            resid = std::fabs(G[i + 1]);
+            resid_b = resid / normb;
+            iters++;
+            if (i + 1 >= im || resid_b <= eps || iters >= itermax) inflag = false;
+        }
+        // y = H^{-1} G (upper triangular, i+1 columns)
+        int m = i + 1;
+        std::vector<double> y(G.begin(), G.begin() + m);
+        for (int r = m - 1; r >= 0; r--) {
+            double s = y[r];
+            for (int c = r + 1; c < m; c++) s -= H[(size_t)c * im1 + r] * y[c];
+            y[r] = s / H[(size_t)r * im1 + r];
+        }
+        cudaMemcpyAsync(gdev.p, y.data(), m * 8, cudaMemcpyHostToDevice, R.d.stream);
+        pgpu::launch_gemv(n, m, R.precond ? W.p : V.p, gdev.p, x, R.d.stream);
+        cudaStreamSynchronize(R.d.stream);
+        normx = 1.0;
+        if (iters >= itermax) outflag = false;
+    }
+    iters_out = iters;
+    return PASTIX_SUCCESS;
+}
+
+// preconditioned CG (refinement/z_refine_grad.c:49-175)
+static int refine_cg(Refiner &R, double *x, const double *b, double eps, int itermax, int &iters_out) {
+    const int64_t n = R.n;
+    DBuf<double> r, p, z, q;
+    if (r.alloc(n) || p.alloc(n) || z.alloc(n) || q.alloc(n)) return PASTIX_ERR_OUTOFMEMORY;
+    double normb = R.norm(b);
+    if (normb == 0.) normb = 1;
+    double normx = R.norm(x);
+    R.copy(b, r.p);
+    if (normx > 0.) R.spmv(-1., x, 1., r.p);
+    double resid_b = R.norm(r.p) / normb;
+    R.copy(r.p, z.p);
+    if (R.spsv(z.p)) return PASTIX_ERR_INTERNAL;
+    R.copy(z.p, p.p);
+    int it = 0;
+    while (resid_b > eps && it < itermax) {
+        it++;
+        R.spmv(1.0, p.p, 0., q.p);
+        double beta = R.dot(r.p, z.p);
+        double alpha = beta / R.dot(q.p, p.p);
+        R.axpy(alpha, p.p, x);
+        R.axpy(-alpha, q.p, r.p);
+        R.copy(r.p, z.p);
+        if (R.spsv(z.p)) return PASTIX_ERR_INTERNAL;
+        double rz = R.dot(r.p, z.p);
+        beta = rz / beta;
+        pgpu::launch_xpby(n, z.p, beta, p.p, R.d.stream);  // p = z + beta p
+        resid_b = R.norm(r.p) / normb;
+    }
+    iters_out = it;
+    return PASTIX_SUCCESS;
+}
+
+// preconditioned BiCGStab (refinement/z_refine_bicgstab.c:49-228)
+static int refine_bicgstab(Refiner &R, double *x, const double *b, double eps, int itermax, int &iters_out) {
+    const int64_t n = R.n;
+    DBuf<double> r, r2, p, y, v, s, z, t, t2;
+    if (r.alloc(n) || r2.alloc(n) || p.alloc(n) || y.alloc(n) || v.alloc(n) || s.alloc(n) || z.alloc(n) ||
+        t.alloc(n) || t2.alloc(n))
+        return PASTIX_ERR_OUTOFMEMORY;
+    double normb = R.norm(b);
+    if (normb == 0.) normb = 1;
+    double normx = R.norm(x);
+    R.copy(b, r.p);
+    if (normx > 0.) R.spmv(-1., x, 1., r.p);
+    double resid_b = R.norm(r.p) / normb;
+    R.copy(r.p, r2.p);
+    R.copy(r.p, p.p);
+    int it = 0;
+    while (resid_b > eps && it < itermax) {
+        it++;
+        R.copy(p.p, y.p);
+        if (R.spsv(y.p)) return PASTIX_ERR_INTERNAL;
+        R.spmv(1.0, y.p, 0., v.p);
+        double alpha = R.dot(v.p, r2.p);
+        double beta = R.dot(r.p, r2.p);
+        alpha = beta / alpha;
+        R.copy(r.p, s.p);
+        R.axpy(-alpha, v.p, s.p);
+        R.copy(s.p, z.p);
+        if (R.spsv(z.p)) return PASTIX_ERR_INTERNAL;
+        R.spmv(1.0, z.p, 0., t.p);
+        R.copy(t.p, t2.p);
+        if (R.spsv(t2.p)) return PASTIX_ERR_INTERNAL;
+        double w = R.dot(t2.p, z.p) / R.dot(t2.p, t2.p);
+        R.axpy(alpha, y.p, x);
+        R.axpy(w, z.p, x);
+        R.copy(s.p, r.p);
+        R.axpy(-w, t.p, r.p);
+        double v1 = R.dot(r.p, r2.p);
+        double bb = (v1 / beta) * (alpha / w);
+        R.axpy(-w, v.p, p.p);
+        R.scal(bb, p.p);
+        R.axpy(1., r.p, p.p);
+        resid_b = R.norm(r.p) / normb;
+    }
+    iters_out = it;
+    return PASTIX_SUCCESS;
+}
+
+// simple iterative refinement (refinement/z_refine_pivot.c:48-157)
+static int refine_sr(Refiner &R, double *x, const double *b, double eps, int itermax, int &iters_out) {
+    const int64_t n = R.n;
+    if (!R.precond) return PASTIX_ERR_BADPARAMETER;
+    DBuf<double> r, dx;
+    if (r.alloc(n) || dx.alloc(n)) return PASTIX_ERR_OUTOFMEMORY;
+    double normb = R.norm(b);
+    if (normb == 0.) normb = 1;
+    int it = 0;
+    double last = 0;
+    while (true) {
+        R.copy(b, r.p);
+        R.spmv(-1., x, 1., r.p);
+        double berr = R.norm(r.p) / normb;
+        if (it == 0) last = 3 * berr;
+        if (it < itermax && berr > eps && berr <= last / 2.) {
+            R.copy(r.p, dx.p);
+            if (R.spsv(dx.p)) return PASTIX_ERR_INTERNAL;
+            R.axpy(1.0, dx.p, x);
+            last = berr;
+            it++;
+        } else break;
+    }
+    iters_out = it;
+    return PASTIX_SUCCESS;
+}
+}  // namespace
+
+// Refinement of permuted device vectors x (in/out) for rhs b (one column each).
+static int refine_perm(pastix_data_t *pd, double *x, const double *b, int &iters) {
+    Refiner R(pd);
+    double eps = pd->dparm[DPARM_EPSILON_REFINEMENT];
+    int itermax = (int)pd->iparm[IPARM_ITERMAX];
+    switch (pd->iparm[IPARM_REFINEMENT]) {
+        case PastixRefineCG: return refine_cg(R, x, b, eps, itermax, iters);
+        case PastixRefineSR: return refine_sr(R, x, b, eps, itermax, iters);
+        case PastixRefineBiCGSTAB: return refine_bicgstab(R, x, b, eps, itermax, iters);
+        default: return refine_gmres(R, x, b, eps, itermax, (int)std::max<pastix_int_t>(1, pd->iparm[IPARM_GMRES_IM]), iters);
+    }
+}
+
+extern "C" int pastix_subtask_refine(pastix_data_t *pd, pastix_rhs_t Bp, pastix_rhs_t Xp) {
+    if (!pd || !(pd->steps & STEP_CSC2BCSC) || !Bp || !Xp || !Bp->b || !Xp->b) return PASTIX_ERR_BADPARAMETER;
+    if (Bp->flttype != SpmDouble || Xp->flttype != SpmDouble) return PASTIX_ERR_BADPARAMETER;
+    if (pd->dparm[DPARM_EPSILON_REFINEMENT] < 0.) pd->dparm[DPARM_EPSILON_REFINEMENT] = 1e-12;  // FP64 input
+    CUDA_TRY(cudaSetDevice(pd->dev.dev));
+    double t0 = now_s();
+    pd->iparm[IPARM_NBITER] = 0;
+    for (pastix_int_t j = 0; j < Bp->n; j++) {
+        int it = 0;
+        int rc = refine_perm(pd, (double *)Xp->b + j * Xp->ld, (const double *)Bp->b + j * Bp->ld, it);
+        if (rc) return rc;
+        pd->iparm[IPARM_NBITER] = std::max<pastix_int_t>(pd->iparm[IPARM_NBITER], it);
+    }
+    CUDA_TRY(cudaStreamSynchronize(pd->dev.stream));
+    pd->dparm[DPARM_REFINE_TIME] = now_s() - t0;
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pastix_task_refine(pastix_data_t *pd, pastix_int_t n, pastix_int_t nrhs, void *B, pastix_int_t ldb,
+                                  void *X, pastix_int_t ldx) {
+    if (!pd || !(pd->steps & STEP_CSC2BCSC)) {
+        perr("pastix_task_refine: the matrix values must be given first (pastix_task_numfact)");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    if (n != pd->n || nrhs < 1 || ldb < n || ldx < n || !B || !X) return PASTIX_ERR_BADPARAMETER;
+    pastix_rhs_t Bp, Xp;
+    pastixRhsInit(&Bp);
+    pastixRhsInit(&Xp);
+    int rc = pastix_subtask_applyorder(pd, PastixDirForward, n, nrhs, B, ldb, Bp);
+    if (!rc) rc = pastix_subtask_applyorder(pd, PastixDirForward, n, nrhs, X, ldx, Xp);
+    if (!rc) rc = pastix_subtask_refine(pd, Bp, Xp);
+    if (!rc) rc = pastix_subtask_applyorder(pd, PastixDirBackward, n, nrhs, X, ldx, Xp);
+    pastixRhsFinalize(Bp);
+    pastixRhsFinalize(Xp);
+    return rc;
+}
+
+extern "C" int pastix_task_solve_and_refine(pastix_data_t *pd, pastix_int_t n, pastix_int_t nrhs, void *B,
+                                            pastix_int_t ldb, void *X, pastix_int_t ldx) {
+    if (!pd || !B || !X || ldx < n || ldb < n) return PASTIX_ERR_BADPARAMETER;
+    for (pastix_int_t j = 0; j < nrhs; j++)
+        memcpy((double *)X + j * ldx, (const double *)B + j * ldb, n * sizeof(double));
+    int rc = pastix_task_solve(pd, n, nrhs, X, ldx);
+    if (rc) return rc;
+    return pastix_task_refine(pd, n, nrhs, B, ldb, X, ldx);
+}
+
+// ---------------------------------------------------------------------------
+// adjoint helpers and device SpMV in the original numbering
+// ---------------------------------------------------------------------------
+extern "C" int pgpu_sampled_outer(pastix_data_t *pd, double alpha, const double *lambda, const double *x, double *G,
+                                  void *stream) {
+    if (!pd || !pd->dev.ready || !lambda || !x || !G) return PASTIX_ERR_BADPARAMETER;
+    CUDA_TRY(cudaSetDevice(pd->dev.dev));
+    cudaStream_t st = stream ? (cudaStream_t)stream : pd->dev.stream;
+    pgpu::launch_sampled(pd->nnz, pd->dev.e_row.p, pd->dev.e_col.p, alpha, lambda, x, G, st);
+    CUDA_TRY(cudaGetLastError());
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pgpu_spmv_device(pastix_data_t *pd, double alpha, const double *x, double beta, double *y,
+                                void *stream) {
+    if (!pd || !(pd->steps & STEP_CSC2BCSC) || !x || !y) return PASTIX_ERR_BADPARAMETER;
+    Device &d = pd->dev;
+    CUDA_TRY(cudaSetDevice(d.dev));
+    if (d.w1.n < (size_t)pd->n) CUDA_TRY(d.w1.alloc(pd->n));
+    if (d.w2.n < (size_t)pd->n) CUDA_TRY(d.w2.alloc(pd->n));
+    cudaStream_t st = stream ? (cudaStream_t)stream : d.stream;
+    pgpu::launch_permute<double, double>((int)pd->n, 1, d.perm.p, 1, x, pd->n, d.w1.p, pd->n, st);
+    pgpu::launch_permute<double, double>((int)pd->n, 1, d.perm.p, 1, y, pd->n, d.w2.p, pd->n, st);
+    pgpu::launch_spmv((int)pd->n, pd->csr_nnz, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha, d.w1.p, beta, d.w2.p, st);
+    pgpu::launch_permute<double, double>((int)pd->n, 1, d.perm.p, 0, d.w2.p, pd->n, y, pd->n, st);
+    CUDA_TRY(cudaGetLastError());
+    return PASTIX_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// legacy one-call interface (sopalin/pastix.c:103-541), tasks START..END
+// ---------------------------------------------------------------------------
+extern "C" int pastix(pastix_data_t **pdp, PASTIX_Comm comm, pastix_int_t n, pastix_int_t *colptr, pastix_int_t *rowptr,
+                      void *values, pastix_int_t *perm, pastix_int_t *invp, void *B, pastix_int_t nrhs,
+                      pastix_int_t *iparm, double *dparm) {
+    if (!pdp || !iparm || !dparm) return PASTIX_ERR_BADPARAMETER;
+    if (iparm[IPARM_MODIFY_PARAMETER] == 0) {
+        pastixInitParam(iparm, dparm);
+        iparm[IPARM_MODIFY_PARAMETER] = 1;
+        return PASTIX_SUCCESS;
+    }
+    if (!*pdp) {
+        pastixInit(pdp, comm, iparm, dparm);
+        if (!*pdp) return PASTIX_ERR_ALLOC;
+    }
+    pastix_data_t *pd = *pdp;
+    spmatrix_t spm;
+    memset(&spm, 0, sizeof(spm));
+    spm.mtxtype = (iparm[IPARM_MTX_TYPE] == SpmSymmetric ||
+                   (iparm[IPARM_MTX_TYPE] == -1 && iparm[IPARM_FACTORIZATION] != PastixFactLU))
+                      ? SpmSymmetric : SpmGeneral;
+    spm.flttype = SpmDouble;
+    spm.fmttype = SpmCSC;
+    spm.baseval = colptr ? colptr[0] : 0;
+    spm.n = spm.gN = n;
+    spm.nnz = spm.gnnz = colptr ? colptr[n] - spm.baseval : 0;
+    spm.dof = 1;
+    spm.colptr = colptr;
+    spm.rowptr = rowptr;
+    spm.values = values;
+    int start = (int)iparm[IPARM_START_TASK], end = (int)iparm[IPARM_END_TASK];
+    int rc = PASTIX_SUCCESS;
+    if (start <= PastixTaskOrdering && end >= PastixTaskOrdering) {
+        pastix_order_t ord;
+        memset(&ord, 0, sizeof(ord));
+        pastix_order_t *po = nullptr;
+        if (iparm[IPARM_ORDERING] == PastixOrderPersonal && perm) {
+            ord.vertnbr = n;
+            ord.baseval = 0;
+            ord.permtab = perm;
+            ord.peritab = invp;
+            po = &ord;
+        }
+        rc = pastix_subtask_order(pd, &spm, po);
+        if (!rc && perm && iparm[IPARM_ORDERING] != PastixOrderPersonal)
+            for (pastix_int_t i = 0; i < n; i++) {
+                perm[i] = pd->order.permtab[i];
+                if (invp) invp[i] = pd->order.peritab[i];
+            }
+    }
+    if (!rc && start <= PastixTaskSymbfact && end >= PastixTaskSymbfact) rc = pastix_subtask_symbfact(pd);
+    if (!rc && start <= PastixTaskAnalyze && end >= PastixTaskAnalyze) rc = pastix_subtask_blend(pd);
+    if (!rc && start <= PastixTaskNumfact && end >= PastixTaskNumfact) rc = pastix_task_numfact(pd, &spm);
+    if (!rc && start <= PastixTaskSolve && end >= PastixTaskSolve && B && nrhs > 0) {
+        std::vector<double> b0((size_t)n * nrhs);
+        memcpy(b0.data(), B, b0.size() * sizeof(double));
+        rc = pastix_task_solve(pd, n, nrhs, B, n);
+        if (!rc && start <= PastixTaskRefine && end >= PastixTaskRefine)
+            rc = pastix_task_refine(pd, n, nrhs, b0.data(), n, B, n);
+    }
+    if (!rc && end >= PastixTaskClean) pastixFinalize(pdp);
+    return rc;
+}

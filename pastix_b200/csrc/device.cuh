@@ -1,0 +1,54 @@
+// Device-side view of the solver structure and the launch lists of the B200
+// numerical phase.  Everything here is plain device pointers; the host driver
+// (api.cu) owns the allocations.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace pgpu {
+
+// Factorization kinds (pastix_factotype_t of include/pastix/api.h).
+enum FactKind : int { FACT_POTRF = 0, FACT_SYTRF = 1, FACT_GETRF = 2 };
+
+// One update task: C_dst -= A(rows [row0 + a_shift, stride_src)) * B(rows [row0, row0+n))^T,
+// scattered into the panel of dst.  a_shift is 0 for the L side and n for the
+// U side of an LU update (core_zgemmsp_2d2d shift, kernels/core_zgemmsp.c:433).
+struct TaskDev {
+    int src, dst;
+    int row0, n;      // the blok facing dst: panel row offset and height
+    int m;            // rows of src from row0 to the end of its panel
+    int excl;         // 1: no other source of the same level writes dst
+};
+
+// One output tile of an update task.
+struct UpdTile {
+    int task;
+    int mt, nt;       // tile coordinates inside the task's (m x n) product
+    int side;         // 0: L side, 1: U side (LU only)
+};
+
+// One row tile of a cblk's off-diagonal panel (TRSM and solve updates).
+struct RowTile {
+    int cblk;
+    int r0;           // first panel row of the tile (>= width: below the diagonal block)
+};
+
+struct DevStruct {
+    int n;
+    int cblknbr;
+    const int *cb_fcol, *cb_lcol, *cb_stride, *cb_fblok;
+    const int64_t *cb_coef;     // panel offset (elements) of each cblk
+    const int64_t *cb_rowidx;   // offset of each cblk in rowidx
+    const int *bk_frow, *bk_lrow, *bk_rowoff, *bk_fcblk;
+    const int *rowidx;          // global row of every panel row
+    const TaskDev *tasks;
+};
+
+// Per-call scalars for the factorization kernels.
+struct FactParams {
+    double criterion;           // static pivoting threshold (eps * ||A||_F)
+    int *nbpivots;              // device counter
+    int *status;                // device status word (0 = fine)
+};
+
+}  // namespace pgpu

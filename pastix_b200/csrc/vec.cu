@@ -1,0 +1,181 @@
+// Vector kernels for the solve glue and the refinement (sm_100a).
+//
+//   k_spmv        y = alpha*A*x + beta*y on the permuted matrix in CSR, FP64
+//                 (bcsc_zspmv, bcsc/bcsc_zspmv.c:629; the bcsc stores A by
+//                 columns, its NoTrans product on the transposed values is
+//                 the row product computed here)
+//   k_dot_part    deterministic two-pass reductions for dot and nrm2
+//                 (bvec_zdotc / bvec_znrm2, bcsc/bvec_zcompute.c:71,561)
+//   k_axpy/scal   bvec_zaxpy / bvec_zscal (bcsc/bvec_zcompute.c:398,259)
+//   k_gemv        x += W y with a small dense y (bvec_zgemv, :1112)
+//   k_permute     b_perm[perm[i]] = b[i] and back (bvec_zlapmr, bcsc/bvec_zlapmr.c:668)
+//   k_cast        FP64 <-> FP32 copies (pastixRhsDoubletoSingle, sopalin/pastix_rhs.c:162)
+//   k_sampled     G[e] = alpha * l[row(e)] * x[col(e)] over the matrix pattern
+//                 (adjoint of the values, no counterpart in the reference)
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace pgpu {
+
+// SpMV with a group of G lanes per row.
+template <int G>
+__global__ void k_spmv(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
+                       const double *__restrict__ val, double alpha, const double *__restrict__ x, double beta,
+                       double *__restrict__ y) {
+    const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int lane = threadIdx.x % G;
+    double acc = 0.0;
+    if (gid < n) {
+        const int b = rowptr[gid], e = rowptr[gid + 1];
+        for (int p = b + lane; p < e; p += G) acc += val[p] * x[col[p]];
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, G);
+    if (lane == 0 && gid < n) y[gid] = alpha * acc + (beta == 0.0 ? 0.0 : beta * y[gid]);
+}
+
+constexpr int RED_THREADS = 256;
+constexpr int RED_BLOCKS = 296;  // 2 x 148 SMs
+
+// per-block partial sums of a[i]*b[i] (b == a gives a squared norm)
+__global__ void k_dot_part(int64_t n, const double *__restrict__ a, const double *__restrict__ b,
+                           double *__restrict__ part) {
+    __shared__ double sh[RED_THREADS / 32];
+    double acc = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc += a[i] * b[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = (threadIdx.x < RED_THREADS / 32) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) part[blockIdx.x] = v;
+    }
+}
+
+// final reduction of the partials in a fixed order; out = sum (or sqrt(sum))
+__global__ void k_dot_final(const double *__restrict__ part, int np, int do_sqrt, double *out) {
+    __shared__ double sh[RED_THREADS / 32];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) acc += part[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = (threadIdx.x < RED_THREADS / 32) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) *out = do_sqrt ? sqrt(v) : v;
+    }
+}
+
+__global__ void k_axpy(int64_t n, double alpha, const double *__restrict__ x, double *__restrict__ y) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] += alpha * x[i];
+}
+// y = x + beta * y
+__global__ void k_xpby(int64_t n, const double *__restrict__ x, double beta, double *__restrict__ y) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = x[i] + beta * y[i];
+}
+__global__ void k_scal(int64_t n, double alpha, double *__restrict__ x) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] *= alpha;
+}
+// x += W[:, 0:m] * yv  (W column major, ld = n, yv in device memory)
+__global__ void k_gemv(int64_t n, int m, const double *__restrict__ W, const double *__restrict__ yv,
+                       double *__restrict__ x) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int j = 0; j < m; j++) acc += W[i + (int64_t)j * n] * yv[j];
+        x[i] += acc;
+    }
+}
+
+// dst[perm[i] + j*ldd] = src[i + j*lds] (forward) or dst[i] = src[perm[i]] (backward)
+template <typename TS, typename TD>
+__global__ void k_permute(int n, int nrhs, const int64_t *__restrict__ perm, int forward, const TS *__restrict__ src,
+                          int64_t lds, TD *__restrict__ dst, int64_t ldd) {
+    int64_t tot = (int64_t)n * nrhs;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        int i = (int)(e % n);
+        int64_t j = e / n;
+        if (forward) dst[perm[i] + j * ldd] = (TD)src[i + j * lds];
+        else dst[i + j * ldd] = (TD)src[perm[i] + j * lds];
+    }
+}
+
+template <typename TS, typename TD>
+__global__ void k_cast(int64_t n, const TS *__restrict__ src, TD *__restrict__ dst) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = (TD)src[i];
+}
+
+// G[e] = alpha * l[row[e]] * x[col[e]] for the stored entries e of the matrix
+__global__ void k_sampled(int64_t nnz, const int *__restrict__ erow, const int *__restrict__ ecol, double alpha,
+                          const double *__restrict__ l, const double *__restrict__ x, double *__restrict__ G) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x)
+        G[e] = alpha * l[erow[e]] * x[ecol[e]];
+}
+
+// ------------------------------ launchers ---------------------------------
+static inline int nblk(int64_t n, int t = 256) {
+    int64_t b = (n + t - 1) / t;
+    return (int)(b < 148 * 32 ? (b < 1 ? 1 : b) : 148 * 32);
+}
+
+void launch_spmv(int n, int64_t nnz, const int *rowptr, const int *col, const double *val, double alpha,
+                 const double *x, double beta, double *y, cudaStream_t st) {
+    if (n <= 0) return;
+    double avg = n ? (double)nnz / n : 0;
+    if (avg <= 12) {
+        constexpr int G = 4;
+        int64_t thr = (int64_t)n * G;
+        k_spmv<G><<<(unsigned)((thr + 255) / 256), 256, 0, st>>>(n, rowptr, col, val, alpha, x, beta, y);
+    } else {
+        constexpr int G = 16;
+        int64_t thr = (int64_t)n * G;
+        k_spmv<G><<<(unsigned)((thr + 255) / 256), 256, 0, st>>>(n, rowptr, col, val, alpha, x, beta, y);
+    }
+}
+int reduce_partials() { return RED_BLOCKS; }
+void launch_dot(int64_t n, const double *a, const double *b, double *part, int do_sqrt, double *out,
+                cudaStream_t st) {
+    k_dot_part<<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, a, b, part);
+    k_dot_final<<<1, RED_THREADS, 0, st>>>(part, RED_BLOCKS, do_sqrt, out);
+}
+void launch_axpy(int64_t n, double alpha, const double *x, double *y, cudaStream_t st) {
+    k_axpy<<<nblk(n), 256, 0, st>>>(n, alpha, x, y);
+}
+void launch_xpby(int64_t n, const double *x, double beta, double *y, cudaStream_t st) {
+    k_xpby<<<nblk(n), 256, 0, st>>>(n, x, beta, y);
+}
+void launch_scal(int64_t n, double alpha, double *x, cudaStream_t st) { k_scal<<<nblk(n), 256, 0, st>>>(n, alpha, x); }
+void launch_gemv(int64_t n, int m, const double *W, const double *yv, double *x, cudaStream_t st) {
+    k_gemv<<<nblk(n), 256, 0, st>>>(n, m, W, yv, x);
+}
+template <typename TS, typename TD>
+void launch_permute(int n, int nrhs, const int64_t *perm, int forward, const TS *src, int64_t lds, TD *dst,
+                    int64_t ldd, cudaStream_t st) {
+    k_permute<TS, TD><<<nblk((int64_t)n * nrhs), 256, 0, st>>>(n, nrhs, perm, forward, src, lds, dst, ldd);
+}
+template <typename TS, typename TD>
+void launch_cast(int64_t n, const TS *src, TD *dst, cudaStream_t st) {
+    k_cast<TS, TD><<<nblk(n), 256, 0, st>>>(n, src, dst);
+}
+void launch_sampled(int64_t nnz, const int *erow, const int *ecol, double alpha, const double *l, const double *x,
+                    double *G, cudaStream_t st) {
+    if (nnz <= 0) return;
+    k_sampled<<<nblk(nnz), 256, 0, st>>>(nnz, erow, ecol, alpha, l, x, G);
+}
+
+template void launch_permute<double, double>(int, int, const int64_t *, int, const double *, int64_t, double *,
+                                             int64_t, cudaStream_t);
+template void launch_permute<double, float>(int, int, const int64_t *, int, const double *, int64_t, float *, int64_t,
+                                            cudaStream_t);
+template void launch_permute<float, double>(int, int, const int64_t *, int, const float *, int64_t, double *, int64_t,
+                                            cudaStream_t);
+template void launch_cast<double, float>(int64_t, const double *, float *, cudaStream_t);
+template void launch_cast<float, double>(int64_t, const float *, double *, cudaStream_t);
+
+}  // namespace pgpu

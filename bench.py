@@ -1,0 +1,375 @@
+"""Benchmark: time-to-solution of the 100^3 7-point Laplacian (n = 10^6) to
+backward error 1e-12 on one B200, FP32 factorization + FP64 GPU CG refinement
+against the plain FP64 factorization + solve (+ refinement check).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = numerical factorization + solve + refinement of one system (the
+hot path; the analysis is done once, outside the timed region).  `value` is
+the device-timed seconds per step with the matrix values and the right-hand
+side already in HBM; `e2e` is the same step through the C ABI with host
+buffers (pastix_task_numfact + pastix_task_solve + pastix_task_refine), the
+host<->device copies inside the timed region.  Multi-GPU runs are independent
+replicas (one system per GPU, no collective on the data path); the time is the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # name: (grid, factorization, refinement, rhs seed)
+    "lap100": ((100, 100, 100), "POTRF", "CG", 1),
+}
+BERR_TARGET = 1e-12
+
+
+def backward_error(A, x, b) -> float:
+    import scipy.sparse.linalg as spla
+    r = b - A @ x
+    return float(np.linalg.norm(r) / (spla.norm(A) * np.linalg.norm(x) + np.linalg.norm(b)))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        load = [s for s in sm if smax and s > 0.3 * smax] or sm
+        return {"sm_mhz": float(np.median(load)) if load else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def fp64_peak_tflops(torch) -> float:
+    """cuBLAS DGEMM throughput measured in this run (the FP64 roofline denominator)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def update_flops(info) -> float:
+    """Algorithmic flops of the update GEMMs (the update term of the reference's
+    sum1d for LL^T: N*M*(M+1) per cblk, symbol/symbol_cost.c:53-88)."""
+    N = (info["cb_lcol"] - info["cb_fcol"] + 1).astype(np.float64)
+    M = (info["cb_stride"] - N).astype(np.float64)
+    return float((N * M * (M + 1)).sum())
+
+
+def solve_bytes(info) -> float:
+    """Algorithmic bytes of one FP64 LL^T solve: the factor read twice (forward and backward)."""
+    return 2.0 * 8.0 * float(info["coefnbr"])
+
+
+def run_b200(args, ws, rank, local):
+    import torch
+    from pastix_b200 import gen
+    from pastix_b200 import pastix as px
+    from pastix_b200.spm import mtxtype, spmatrix
+
+    torch.cuda.set_device(local)
+    grid, fact, refine, seed = WORKLOADS[args.workload]
+    A = gen.laplacian7(*grid)
+    n = A.shape[0]
+    S = spmatrix(A, mtxtype.Symmetric)
+    Af = S.full()
+    xt = gen.rhs_uniform(n, 1, seed)[:, 0]
+    b_h = np.ascontiguousarray(Af @ xt)
+    vals = torch.from_numpy(S.values).cuda()
+    b = torch.from_numpy(b_h).cuda()
+
+    results = {}
+    for mode in ("mixed", "fp64"):
+        ip, dp = px.initParam()
+        ip[px.iparm.factorization] = px.factotype.POTRF
+        ip[px.iparm.mixed] = 1 if mode == "mixed" else 0
+        ip[px.iparm.refinement] = px.refine.CG
+        dp[px.dparm.epsilon_refinement] = BERR_TARGET
+        pd = px.init(ip, dp)
+        t0 = time.time()
+        px.analyze_grid(pd, S, *grid)
+        t_an = time.time() - t0
+        info = px.solver_info(pd)
+        x = torch.zeros_like(b)
+        stream = torch.cuda.ExternalStream(px.stream_ptr(pd))
+
+        def step():
+            px.numfact_device(pd, vals)
+            px.solve_refine_device(pd, b, x)
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        sampler = ClockSampler(local) if mode == "mixed" else None
+        if sampler:
+            sampler.start()
+        px.profile(pd, False)  # count launches, no per-launch events
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / args.steps
+        launches = sum(v[1] for v in px.profile_get(pd).values())
+        clocks = sampler.stop() if sampler else None
+        if ws > 1:
+            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            t = float(tt.item())
+        xh = x.cpu().numpy()
+        berr = backward_error(Af, xh, b_h)
+        results[mode] = dict(t=t, berr=berr, fwd=float(np.linalg.norm(xh - xt) / np.linalg.norm(xt)),
+                             fact_time=float(dp[px.dparm.fact_time]), iters=int(ip[px.iparm.nbiter]),
+                             npiv=int(ip[px.iparm.static_pivoting]), launches=launches / args.steps,
+                             analyze_s=t_an, clocks=clocks, thflops=info["thflops"])
+        # profiled pass (per-class device times) for the roofline of the dominant kernel
+        if mode == "fp64":
+            px.profile(pd, True)
+            step()
+            prof = px.profile_get(pd)
+            px.profile(pd, False)
+            results[mode]["profile"] = prof
+            results[mode]["info"] = {k: info[k] for k in ("cb_lcol", "cb_fcol", "cb_stride", "coefnbr")}
+        if mode == "mixed":
+            # e2e through the C ABI with host buffers
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            xe = np.asfortranarray(b_h.copy())
+            px.task_numfact(pd, S)  # warm
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(max(1, min(args.steps, 3))):
+                px.task_numfact(pd, S)
+                xe[:] = b_h
+                px.task_solve(pd, S, xe)
+                px.task_refine(pd, S, b_h, xe)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            results[mode]["e2e"] = e0.elapsed_time(e1) / 1e3 / max(1, min(args.steps, 3))
+            results[mode]["e2e_berr"] = backward_error(Af, xe, b_h)
+            results[mode]["h2d"] = 8 * S.nnz + 8 * n + 2 * 8 * n
+            results[mode]["d2h"] = 8 * n + 8 * n
+        px.finalize(pd)
+    return results, n
+
+
+def run_cpu_baseline(args, sample_small: bool):
+    """The oracle (CPU port of the reference's numerical phase, OpenBLAS, all
+    host threads) on the same workload: factor + solve + CG refinement."""
+    from oracle import oracle as ora
+    from pastix_b200 import gen
+    from pastix_b200 import pastix as px
+    from pastix_b200.spm import mtxtype, spmatrix
+    blas = ora.use_blas(True)
+    grid, fact, refine, seed = WORKLOADS[args.workload]
+    if sample_small:
+        grid = tuple(min(g, args.cpu_sample_grid) for g in grid)
+    A = gen.laplacian7(*grid)
+    n = A.shape[0]
+    S = spmatrix(A, mtxtype.Symmetric)
+    ip, dp = px.initParam()
+    ip[px.iparm.factorization] = px.factotype.POTRF
+    pd = px.init(ip, dp)
+    px.analyze_grid(pd, S, *grid)
+    info = px.solver_info(pd)
+    sym = ora.Symbol(info)
+    Af = S.full()
+    Ap = ora.permuted_full(Af, info["permtab"])
+    perm = info["permtab"]
+    xt = gen.rhs_uniform(n, 1, seed)[:, 0]
+    b = Af @ xt
+    threads = os.cpu_count() or 1
+    t0 = time.time()
+    L, _, _ = ora.factor(sym, Ap, "POTRF", ora.criterion(Ap), nthreads=threads)
+    bp = np.zeros(n)
+    bp[perm] = b
+    prec = lambda r: ora.solve(sym, "POTRF", L, None, r)[:, 0]  # noqa: E731
+    xp = prec(bp)
+    xp, it = ora.refine_cg(Ap, bp, xp, prec, eps=BERR_TARGET)
+    t = time.time() - t0
+    x = xp[perm]
+    return dict(t=t, threads=threads, blas=blas, thflops=info["thflops"], grid=grid,
+                berr=backward_error(Af, x, b), iters=it)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="lap100", choices=list(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-grid", type=int, default=100)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    ws, rank, local = (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+                       int(os.environ.get("LOCAL_RANK", "0")))
+    grid = WORKLOADS[args.workload][0]
+    config = {"workload": f"{args.workload}: 3D 7-point Laplacian {grid[0]}x{grid[1]}x{grid[2]} (n=10^6), LL^T, "
+                          "1 RHS x_true~U[-1,1] seed 1, grid nested dissection",
+              "global_batch": ws, "seq_len": None, "parallelism": f"replicas{ws}",
+              "l2": "inputs larger than L2 (factor 8.5 GB FP64)"}
+    metric = "time-to-solution at backward error 1e-12 (factor + solve + refine)"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        steps = []
+        for _ in range(args.steps):
+            steps.append(run_cpu_baseline(args, sample_small=args.cpu_sample_grid < 100))
+        r = steps[-1]
+        v = float(np.median([s["t"] for s in steps]))
+        line = {"metric": metric, "value": v, "unit": "s", "n_gpus": 0, "steps": args.steps, "warmup": 0,
+                "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic", "config": config, "impl": "reference",
+                "cpu_baseline": {"value": v, "unit": "s", "cores": r["threads"], "kind": "port",
+                                 "sample": f"full workload {r['grid']}: oracle factor (dynamic scheduler, "
+                                           f"OpenBLAS {'on' if r['blas'] else 'off'}) + solve + CG, "
+                                           f"berr {r['berr']:.1e}"},
+                "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    ws, rank, local = dist_setup()
+    res, n = run_b200(args, ws, rank, local)
+    mixed, fp64 = res["mixed"], res["fp64"]
+    best = "mixed" if (mixed["berr"] <= BERR_TARGET and mixed["t"] <= fp64["t"]) else "fp64"
+    value = res[best]["t"]
+    prof = fp64["profile"]
+    upd_ms, upd_launch = prof["update"]
+    uflops = update_flops(fp64["info"])
+    peak = fp64_peak_tflops(torch) if rank == 0 else None
+    achieved = uflops / (upd_ms / 1e3) / 1e12 if upd_ms > 0 else None
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        try:
+            traffic = json.loads(tfile.read_text()).get("k_update_fp64_lap100")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": metric, "value": value, "unit": "s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if best == "mixed" else "f64", "data": "synthetic", "config": config,
+        "path": best,
+        "fp32_refine": {"s": mixed["t"], "berr": mixed["berr"], "fwd_err": mixed["fwd"], "cg_iters": mixed["iters"],
+                        "factor_s": mixed["fact_time"]},
+        "fp64": {"s": fp64["t"], "berr": fp64["berr"], "fwd_err": fp64["fwd"], "refine_iters": fp64["iters"],
+                 "factor_s": fp64["fact_time"], "factor_tflops": fp64["thflops"] / fp64["fact_time"] / 1e12},
+        "factor_tflops_fp32": mixed["thflops"] / mixed["fact_time"] / 1e12,
+        "static_pivots": fp64["npiv"],
+        "roofline": {"kernel": "k_update (FP64 supernode update GEMM + scatter-add)", "bound": "tensor",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in the measured "
+                                    "peaks file)",
+                     "launches": upd_launch, "ms_total": upd_ms, "algorithmic_flops": uflops},
+        "profile_ms": {k: v[0] for k, v in prof.items() if v[1]},
+        "clocks": mixed["clocks"],
+        "gpu_launches": int(res[best]["launches"]),
+        "e2e": {"value": mixed["e2e"], "unit": "s", "h2d_bytes_per_step": mixed["h2d"],
+                "d2h_bytes_per_step": mixed["d2h"], "berr": mixed["e2e_berr"]},
+    }
+    if rank == 0 and not args.no_cpu_baseline and ws == 1:
+        cb = run_cpu_baseline(args, sample_small=args.cpu_sample_grid < 100)
+        scale = WORKLOADS[args.workload][0][0] ** 3 / n
+        line["cpu_baseline"] = {"value": cb["t"], "unit": "s", "cores": cb["threads"], "kind": "port",
+                                "sample": f"grid {cb['grid']} ({cb['thflops']:.2e} flops), oracle factor + solve + "
+                                          f"CG to berr {cb['berr']:.1e}, OpenBLAS {'on' if cb['blas'] else 'off'}"}
+    if rank == 0:
+        print(json.dumps(line))
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

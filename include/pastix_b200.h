@@ -275,6 +275,24 @@ int pgpu_spmv_device(pastix_data_t *pastix_data, double alpha, const double *x, 
 /* Last device status word (0 = fine); non-zero after a bounded wait expired. */
 int pgpu_device_status(const pastix_data_t *pastix_data);
 
+/* The library's CUDA stream (cudaStream_t) after the analysis; every entry
+ * point above orders its work on it.  NULL before pastix_task_analyze. */
+void *pgpu_stream(pastix_data_t *pastix_data);
+
+/* Solve then refine on device memory (pastix_task_solve_and_refine on the GPU):
+ * B, X are n x nrhs FP64 arrays in the original numbering, X receives the
+ * refined solution; IPARM_REFINEMENT selects GMRES / CG / SR / BiCGStab. */
+int pgpu_solve_refine_device(pastix_data_t *pastix_data, pastix_int_t nrhs, const double *B, pastix_int_t ldb,
+                             double *X, pastix_int_t ldx);
+
+/* Launch accounting.  pgpu_profile(pd, 1) resets the counters and times every
+ * launch with CUDA events on the library stream; pgpu_profile(pd, 0) resets
+ * and only counts.  pgpu_profile_get returns, per kernel class (fill, panel,
+ * diag, trsm, update, fwd diag, fwd update, bwd update, bwd diag, spmv, vec),
+ * the summed device milliseconds and the launch counts. */
+int pgpu_profile(pastix_data_t *pastix_data, int enable);
+int pgpu_profile_get(pastix_data_t *pastix_data, double *ms, long long *launches, int nclass);
+
 #ifdef __cplusplus
 }
 #endif

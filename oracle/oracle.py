@@ -68,7 +68,15 @@ def use_blas(enable: bool = True) -> bool:
         lib.ora_unload_blas()
         return False
     for p in OPENBLAS_CANDIDATES + [os.environ.get("ORACLE_BLAS", "")]:
-        if p and Path(p).exists() and lib.ora_load_blas(p.encode()) == 0:
+        if not p or not Path(p).exists():
+            continue
+        # the wheel's OpenBLAS needs its bundled gfortran / quadmath, loaded globally first
+        for dep in sorted(Path(p).parent.glob("libquadmath*.so*")) + sorted(Path(p).parent.glob("libgfortran*.so*")):
+            try:
+                C.CDLL(str(dep), mode=C.RTLD_GLOBAL)
+            except OSError:
+                pass
+        if lib.ora_load_blas(p.encode()) == 0:
             return True
     return False
 

@@ -30,7 +30,12 @@ EXPORTS = [
     "pastixOrderGrid", "pastixOrderExit",
     "pgpu_solver_info", "pgpu_get_coeftab", "pgpu_solve_device", "pgpu_solve_transposed_device",
     "pgpu_numfact_device", "pgpu_sampled_outer", "pgpu_spmv_device", "pgpu_device_status",
+    "pgpu_stream", "pgpu_solve_refine_device", "pgpu_profile", "pgpu_profile_get",
 ]
+
+# kernel classes of pgpu_profile_get, in order
+PROFILE_CLASSES = ["fill", "panel_small", "diag_large", "trsm", "update", "fwd_diag", "fwd_update",
+                   "bwd_update", "bwd_diag", "spmv", "vec"]
 
 
 class spmatrix_t(C.Structure):
@@ -114,6 +119,10 @@ def load() -> C.CDLL:
         "pgpu_sampled_outer": (C.c_int, [P, C.c_double, VP, VP, VP, VP]),
         "pgpu_spmv_device": (C.c_int, [P, C.c_double, VP, C.c_double, VP, VP]),
         "pgpu_device_status": (C.c_int, [P]),
+        "pgpu_stream": (C.c_void_p, [P]),
+        "pgpu_solve_refine_device": (C.c_int, [P, pastix_int_t, VP, pastix_int_t, VP, pastix_int_t]),
+        "pgpu_profile": (C.c_int, [P, C.c_int]),
+        "pgpu_profile_get": (C.c_int, [P, PDBL, C.POINTER(C.c_longlong), C.c_int]),
     }
     for name, (res, args) in proto.items():
         fn = getattr(lib, name)

@@ -38,7 +38,7 @@ void launch_panel_small(const DevStruct &, const int *, int, size_t, T *, T *, c
 template <typename T, int F>
 void launch_diag_large(const DevStruct &, const int *, int, size_t, T *, T *, const FactParams &, cudaStream_t);
 template <typename T, int F>
-void launch_trsm(const DevStruct &, const RowTile *, int, int, size_t, T *, T *, cudaStream_t);
+void launch_trsm(const DevStruct &, const RowTile *, int, size_t, T *, T *, cudaStream_t);
 template <typename T, int F>
 void launch_update(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);
 template <typename T, int F>
@@ -73,6 +73,12 @@ void launch_sampled(int64_t, const int *, const int *, double, const double *, c
 }  // namespace pgpu
 
 using pgpu::idx_t;
+
+// kernel classes for launch accounting (pgpu_profile_get)
+enum : int {
+    PC_FILL = 0, PC_PANEL_SMALL, PC_DIAG_LARGE, PC_TRSM, PC_UPDATE, PC_FWD_DIAG, PC_FWD_UPDATE, PC_BWD_UPDATE,
+    PC_BWD_DIAG, PC_SPMV, PC_VEC, PGPU_NCLASS
+};
 
 // ---------------------------------------------------------------------------
 // internal state
@@ -186,7 +192,27 @@ struct pastix_data_s {
     int mixed = 0;
     double anorm = 0.0;
     Device dev;
+    // launch accounting: per kernel class, launches always counted, device time when profiling
+    bool prof_on = false;
+    int64_t launches[PGPU_NCLASS] = {0};
+    double prof_ms[PGPU_NCLASS] = {0};
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_ev;
 };
+
+// Run one launch of kernel class `cls` with `count` blocks through `fn`.
+template <typename Fn>
+static inline void launch_cls(pastix_data_t *pd, int cls, long long count, Fn &&fn) {
+    if (count <= 0) return;
+    pd->launches[cls]++;
+    if (!pd->prof_on) { fn(); return; }
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, pd->dev.stream);
+    fn();
+    cudaEventRecord(b, pd->dev.stream);
+    pd->prof_ev.push_back({cls, {a, b}});
+}
 
 // ---------------------------------------------------------------------------
 // helpers
@@ -578,12 +604,12 @@ static int build_maps_and_lists(pastix_data_t *pd) {
     // exclusive tasks: dst targeted by a single source in the level
     pd->tasks.resize(sv.tasks.size());
     {
+        // number of distinct sources writing each dst within a level
         std::vector<int> last_src(sv.cblknbr, -1), nsrc(sv.cblknbr, 0);
         for (idx_t l = 0; l < sv.nlevels; l++) {
             for (idx_t t = sv.lvl_task_ptr[l]; t < sv.lvl_task_ptr[l + 1]; t++) {
                 const auto &tk = sv.tasks[t];
                 if (last_src[tk.dst] != (int)tk.src) {
-                    if (last_src[tk.dst] == -1 || nsrc[tk.dst] == 0) nsrc[tk.dst] = 0;
                     nsrc[tk.dst]++;
                     last_src[tk.dst] = (int)tk.src;
                 }
@@ -622,7 +648,7 @@ static int build_maps_and_lists(pastix_data_t *pd) {
             } else {
                 pd->large_list.push_back((int)k);
                 L.diag_smem_elems = std::max<size_t>(L.diag_smem_elems, (size_t)32 * nc * (fk == pgpu::FACT_GETRF ? 2 : 1));
-                int bm = nc <= 160 ? 64 : 32;
+                int bm = pgpu::trsm_tile_rows((int)nc);
                 for (idx_t r = nc; r < st; r += bm) pd->trsm_tiles.push_back(pgpu::RowTile{(int)k, (int)r});
                 if (st > nc) L.trsm_smem_elems = std::max<size_t>(L.trsm_smem_elems, (size_t)bm * nc);
             }
@@ -815,13 +841,21 @@ static int run_factor(pastix_data_t *pd, double criterion) {
     pgpu::FactParams fp{criterion, d.counters.p, d.counters.p + 1};
     for (size_t l = 0; l < pd->levels.size(); l++) {
         const LevelLists &lv = pd->levels[l];
-        pgpu::launch_panel_small<T, F>(d.ds, d.small_list.p + lv.small0, lv.small1 - lv.small0,
-                                       lv.small_smem_elems * sizeof(T), L, U, fp, st);
-        pgpu::launch_diag_large<T, F>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0,
-                                      lv.diag_smem_elems * sizeof(T), L, U, fp, st);
-        pgpu::launch_trsm<T, F>(d.ds, d.trsm_tiles.p + lv.trsm0, lv.trsm1 - lv.trsm0, 0,
-                                lv.trsm_smem_elems * sizeof(T), L, U, st);
-        pgpu::launch_update<T, F>(d.ds, d.upd_tiles.p + lv.upd0, lv.upd1 - lv.upd0, L, U, st);
+        launch_cls(pd, PC_PANEL_SMALL, lv.small1 - lv.small0, [&] {
+            pgpu::launch_panel_small<T, F>(d.ds, d.small_list.p + lv.small0, lv.small1 - lv.small0,
+                                           lv.small_smem_elems * sizeof(T), L, U, fp, st);
+        });
+        launch_cls(pd, PC_DIAG_LARGE, lv.large1 - lv.large0, [&] {
+            pgpu::launch_diag_large<T, F>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0,
+                                          lv.diag_smem_elems * sizeof(T), L, U, fp, st);
+        });
+        launch_cls(pd, PC_TRSM, lv.trsm1 - lv.trsm0, [&] {
+            pgpu::launch_trsm<T, F>(d.ds, d.trsm_tiles.p + lv.trsm0, lv.trsm1 - lv.trsm0,
+                                    lv.trsm_smem_elems * sizeof(T), L, U, st);
+        });
+        launch_cls(pd, PC_UPDATE, lv.upd1 - lv.upd0, [&] {
+            pgpu::launch_update<T, F>(d.ds, d.upd_tiles.p + lv.upd0, lv.upd1 - lv.upd0, L, U, st);
+        });
     }
     CUDA_TRY(cudaGetLastError());
     return PASTIX_SUCCESS;
@@ -913,10 +947,13 @@ extern "C" int pastix_subtask_bcsc2ctab(pastix_data_t *pd) {
     CUDA_TRY(cudaMemsetAsync(d.Lc.p, 0, bytes, d.stream));
     if (d.Uc.p) CUDA_TRY(cudaMemsetAsync(d.Uc.p, 0, bytes, d.stream));
     const int64_t *um = d.Uc.p ? d.umap.p : nullptr;
-    if (pd->mixed)
-        pgpu::launch_fill_coef<float>(pd->nnz, d.vals.p, d.lmap.p, um, (float *)d.Lc.p, (float *)d.Uc.p, d.stream);
-    else
-        pgpu::launch_fill_coef<double>(pd->nnz, d.vals.p, d.lmap.p, um, (double *)d.Lc.p, (double *)d.Uc.p, d.stream);
+    launch_cls(pd, PC_FILL, pd->nnz, [&] {
+        if (pd->mixed)
+            pgpu::launch_fill_coef<float>(pd->nnz, d.vals.p, d.lmap.p, um, (float *)d.Lc.p, (float *)d.Uc.p, d.stream);
+        else
+            pgpu::launch_fill_coef<double>(pd->nnz, d.vals.p, d.lmap.p, um, (double *)d.Lc.p, (double *)d.Uc.p,
+                                           d.stream);
+    });
     CUDA_TRY(cudaGetLastError());
     pd->dparm[DPARM_MEM_FR] = (double)bytes * (d.Uc.p ? 2 : 1);
     pd->steps |= STEP_BCSC2CTAB;
@@ -1008,10 +1045,14 @@ static void sweep_forward(pastix_data_t *pd, const T *P, int unit, T *Y, int ldy
     Device &d = pd->dev;
     for (size_t l = 0; l < pd->levels.size(); l++) {
         const LevelLists &lv = pd->levels[l];
-        pgpu::launch_fwd_diag<T>(d.ds, d.level_cblks.p + lv.cb0, lv.cb1 - lv.cb0, lv.maxnc, P, unit, Y, ldy, nrhs,
-                                 d.stream);
-        pgpu::launch_fwd_update<T>(d.ds, d.solve_tiles.p + lv.st0, lv.st1 - lv.st0, lv.maxnc, P, Y, ldy, nrhs,
-                                   d.stream);
+        launch_cls(pd, PC_FWD_DIAG, lv.cb1 - lv.cb0, [&] {
+            pgpu::launch_fwd_diag<T>(d.ds, d.level_cblks.p + lv.cb0, lv.cb1 - lv.cb0, lv.maxnc, P, unit, Y, ldy,
+                                     nrhs, d.stream);
+        });
+        launch_cls(pd, PC_FWD_UPDATE, lv.st1 - lv.st0, [&] {
+            pgpu::launch_fwd_update<T>(d.ds, d.solve_tiles.p + lv.st0, lv.st1 - lv.st0, lv.maxnc, P, Y, ldy, nrhs,
+                                       d.stream);
+        });
     }
 }
 // backward: solve P^T x = y with P lower
@@ -1020,9 +1061,13 @@ static void sweep_backward(pastix_data_t *pd, const T *P, int unit, T *Y, int ld
     Device &d = pd->dev;
     for (size_t l = pd->levels.size(); l-- > 0;) {
         const LevelLists &lv = pd->levels[l];
-        pgpu::launch_bwd_update<T>(d.ds, d.solve_tiles.p + lv.st0, lv.st1 - lv.st0, P, Y, ldy, nrhs, d.stream);
-        pgpu::launch_bwd_diag<T>(d.ds, d.level_cblks.p + lv.cb0, lv.cb1 - lv.cb0, lv.maxnc, P, unit, Y, ldy, nrhs,
-                                 d.stream);
+        launch_cls(pd, PC_BWD_UPDATE, lv.st1 - lv.st0, [&] {
+            pgpu::launch_bwd_update<T>(d.ds, d.solve_tiles.p + lv.st0, lv.st1 - lv.st0, P, Y, ldy, nrhs, d.stream);
+        });
+        launch_cls(pd, PC_BWD_DIAG, lv.cb1 - lv.cb0, [&] {
+            pgpu::launch_bwd_diag<T>(d.ds, d.level_cblks.p + lv.cb0, lv.cb1 - lv.cb0, lv.maxnc, P, unit, Y, ldy,
+                                     nrhs, d.stream);
+        });
     }
 }
 
@@ -1299,7 +1344,10 @@ struct Refiner {
         return v;
     }
     void spmv(double alpha, const double *x, double beta, double *y) {
-        pgpu::launch_spmv((int)n, pd->csr_nnz, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha, x, beta, y, d.stream);
+        launch_cls(pd, PC_SPMV, 1, [&] {
+            pgpu::launch_spmv((int)n, pd->csr_nnz, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha, x, beta, y,
+                              d.stream);
+        });
     }
     void copy(const double *a, double *b) { cudaMemcpyAsync(b, a, n * 8, cudaMemcpyDeviceToDevice, d.stream); }
     void axpy(double a, const double *x, double *y) { pgpu::launch_axpy(n, a, x, y, d.stream); }
@@ -1644,4 +1692,73 @@ extern "C" int pastix(pastix_data_t **pdp, PASTIX_Comm comm, pastix_int_t n, pas
     }
     if (!rc && end >= PastixTaskClean) pastixFinalize(pdp);
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// B200 extensions: stream, refinement on device, launch accounting
+// ---------------------------------------------------------------------------
+extern "C" void *pgpu_stream(pastix_data_t *pd) {
+    if (!pd || !(pd->steps & STEP_ANALYSE)) return nullptr;
+    if (device_setup(pd) != PASTIX_SUCCESS) return nullptr;
+    return (void *)pd->dev.stream;
+}
+
+extern "C" int pgpu_solve_refine_device(pastix_data_t *pd, pastix_int_t nrhs, const double *B, pastix_int_t ldb,
+                                        double *X, pastix_int_t ldx) {
+    int rc = check_numfact(pd, "pgpu_solve_refine_device");
+    if (rc) return rc;
+    if (nrhs < 1 || ldb < pd->n || ldx < pd->n || !B || !X) return PASTIX_ERR_BADPARAMETER;
+    Device &d = pd->dev;
+    CUDA_TRY(cudaSetDevice(d.dev));
+    const idx_t n = pd->n;
+    DBuf<double> bp, xp;
+    CUDA_TRY(bp.alloc((size_t)n * nrhs));
+    CUDA_TRY(xp.alloc((size_t)n * nrhs));
+    launch_cls(pd, PC_VEC, 1, [&] { pgpu::launch_permute<double, double>((int)n, (int)nrhs, d.perm.p, 1, B, ldb, bp.p, n, d.stream); });
+    CUDA_TRY(cudaMemcpyAsync(xp.p, bp.p, (size_t)n * nrhs * 8, cudaMemcpyDeviceToDevice, d.stream));
+    rc = solve_perm_d(pd, 0, xp.p, (int)n, (int)nrhs);
+    if (rc) return rc;
+    if (pd->dparm[DPARM_EPSILON_REFINEMENT] < 0.) pd->dparm[DPARM_EPSILON_REFINEMENT] = 1e-12;
+    double t0 = now_s();
+    pd->iparm[IPARM_NBITER] = 0;
+    for (pastix_int_t j = 0; j < nrhs; j++) {
+        int it = 0;
+        rc = refine_perm(pd, xp.p + j * n, bp.p + j * n, it);
+        if (rc) return rc;
+        pd->iparm[IPARM_NBITER] = std::max<pastix_int_t>(pd->iparm[IPARM_NBITER], it);
+    }
+    launch_cls(pd, PC_VEC, 1, [&] { pgpu::launch_permute<double, double>((int)n, (int)nrhs, d.perm.p, 0, xp.p, n, X, ldx, d.stream); });
+    CUDA_TRY(cudaStreamSynchronize(d.stream));
+    pd->dparm[DPARM_REFINE_TIME] = now_s() - t0;
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pgpu_profile(pastix_data_t *pd, int enable) {
+    if (!pd) return PASTIX_ERR_BADPARAMETER;
+    for (auto &e : pd->prof_ev) {
+        cudaEventDestroy(e.second.first);
+        cudaEventDestroy(e.second.second);
+    }
+    pd->prof_ev.clear();
+    for (int i = 0; i < PGPU_NCLASS; i++) { pd->prof_ms[i] = 0; pd->launches[i] = 0; }
+    pd->prof_on = enable != 0;
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pgpu_profile_get(pastix_data_t *pd, double *ms, long long *launches, int nclass) {
+    if (!pd || nclass < 1) return PASTIX_ERR_BADPARAMETER;
+    if (pd->dev.ready) CUDA_TRY(cudaStreamSynchronize(pd->dev.stream));
+    for (auto &e : pd->prof_ev) {
+        float t = 0;
+        CUDA_TRY(cudaEventElapsedTime(&t, e.second.first, e.second.second));
+        pd->prof_ms[e.first] += t;
+        cudaEventDestroy(e.second.first);
+        cudaEventDestroy(e.second.second);
+    }
+    pd->prof_ev.clear();
+    for (int i = 0; i < nclass && i < PGPU_NCLASS; i++) {
+        if (ms) ms[i] = pd->prof_ms[i];
+        if (launches) launches[i] = pd->launches[i];
+    }
+    return PASTIX_SUCCESS;
 }

@@ -27,6 +27,10 @@ struct UpdTile {
     int side;         // 0: L side, 1: U side (LU only)
 };
 
+// Rows of one off-diagonal TRSM tile of a cblk of width nc (its shared-memory
+// tile is rows x nc elements).
+__host__ __device__ inline int trsm_tile_rows(int nc) { return nc <= 160 ? 64 : 32; }
+
 // One row tile of a cblk's off-diagonal panel (TRSM and solve updates).
 struct RowTile {
     int cblk;

@@ -278,13 +278,14 @@ __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__re
 // blockIdx.y selects the GETRF side.
 // ---------------------------------------------------------------------------
 template <typename T, int FACT>
-__global__ void __launch_bounds__(256) k_trsm(DevStruct s, const RowTile *__restrict__ tiles, int bm, T *L, T *U) {
+__global__ void __launch_bounds__(256) k_trsm(DevStruct s, const RowTile *__restrict__ tiles, T *L, T *U) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *X = reinterpret_cast<T *>(smem_raw);  // bm x nc, ld = bm
     const RowTile tl = tiles[blockIdx.x];
     const int side = blockIdx.y;
     const int k = tl.cblk;
     const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+    const int bm = trsm_tile_rows(nc);
     const int st = s.cb_stride[k];
     const int rows = min(bm, st - tl.r0);
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -463,11 +464,10 @@ void launch_diag_large(const DevStruct &s, const int *list, int count, size_t sm
 }
 
 template <typename T, int FACT>
-void launch_trsm(const DevStruct &s, const RowTile *tiles, int count, int bm, size_t smem, T *L, T *U,
-                 cudaStream_t st) {
+void launch_trsm(const DevStruct &s, const RowTile *tiles, int count, size_t smem, T *L, T *U, cudaStream_t st) {
     if (count <= 0) return;
     dim3 grid(count, FACT == FACT_GETRF ? 2 : 1);
-    k_trsm<T, FACT><<<grid, 256, smem, st>>>(s, tiles, bm, L, U);
+    k_trsm<T, FACT><<<grid, 256, smem, st>>>(s, tiles, L, U);
 }
 
 template <typename T, int FACT>
@@ -491,8 +491,7 @@ cudaError_t set_smem_attrs(size_t small_max, size_t diag_max, size_t trsm_max) {
                                            const FactParams &, cudaStream_t);                                    \
     template void launch_diag_large<T, F>(const DevStruct &, const int *, int, size_t, T *, T *,                 \
                                           const FactParams &, cudaStream_t);                                     \
-    template void launch_trsm<T, F>(const DevStruct &, const RowTile *, int, int, size_t, T *, T *,              \
-                                    cudaStream_t);                                                               \
+    template void launch_trsm<T, F>(const DevStruct &, const RowTile *, int, size_t, T *, T *, cudaStream_t);     \
     template void launch_update<T, F>(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);          \
     template cudaError_t set_smem_attrs<T, F>(size_t, size_t, size_t);
 

@@ -272,3 +272,56 @@ class solver:
 
     def finalize(self):
         finalize(self.pastix_data)
+
+
+# ---------------- device-resident entry points (torch CUDA tensors) ----------------
+def stream_ptr(pd: Data) -> int:
+    """cudaStream_t of the library (after the analysis)."""
+    p = _lib.load().pgpu_stream(pd.ptr)
+    if not p:
+        raise PastixError("pgpu_stream", int(error.INTERNAL))
+    return int(p)
+
+
+def numfact_device(pd: Data, values) -> None:
+    """Numerical factorization from a CUDA float64 tensor of the spm values."""
+    _check("pgpu_numfact_device", _lib.load().pgpu_numfact_device(pd.ptr, C.c_void_p(values.data_ptr())))
+
+
+def solve_device(pd: Data, B, transposed: bool = False) -> None:
+    """In-place solve of a CUDA float64 tensor B (n or n x nrhs, column-major storage)."""
+    n = B.shape[0]
+    nrhs = 1 if B.dim() == 1 else B.shape[1]
+    ld = n if B.dim() == 1 else B.stride(1)
+    fn = _lib.load().pgpu_solve_transposed_device if transposed else _lib.load().pgpu_solve_device
+    _check("pgpu_solve_device", fn(pd.ptr, nrhs, C.c_void_p(B.data_ptr()), ld, None))
+
+
+def solve_refine_device(pd: Data, B, X) -> None:
+    """X <- refined solution of A X = B (CUDA float64 tensors, column-major)."""
+    n = B.shape[0]
+    nrhs = 1 if B.dim() == 1 else B.shape[1]
+    ldb = n if B.dim() == 1 else B.stride(1)
+    ldx = n if X.dim() == 1 else X.stride(1)
+    _check("pgpu_solve_refine_device",
+           _lib.load().pgpu_solve_refine_device(pd.ptr, nrhs, C.c_void_p(B.data_ptr()), ldb,
+                                                C.c_void_p(X.data_ptr()), ldx))
+
+
+def spmv_device(pd: Data, alpha: float, x, beta: float, y) -> None:
+    _check("pgpu_spmv_device", _lib.load().pgpu_spmv_device(pd.ptr, alpha, C.c_void_p(x.data_ptr()), beta,
+                                                            C.c_void_p(y.data_ptr()), None))
+
+
+def profile(pd: Data, enable: bool) -> None:
+    _check("pgpu_profile", _lib.load().pgpu_profile(pd.ptr, int(enable)))
+
+
+def profile_get(pd: Data) -> dict:
+    """{class: (device ms, launches)} accumulated since the last profile() call."""
+    k = len(_lib.PROFILE_CLASSES)
+    ms = np.zeros(k, dtype=np.float64)
+    ln = np.zeros(k, dtype=np.int64)
+    _check("pgpu_profile_get", _lib.load().pgpu_profile_get(pd.ptr, ms.ctypes.data_as(PDBL),
+                                                            ln.ctypes.data_as(C.POINTER(C.c_longlong)), k))
+    return {c: (float(ms[i]), int(ln[i])) for i, c in enumerate(_lib.PROFILE_CLASSES)}

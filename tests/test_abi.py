@@ -1,0 +1,111 @@
+"""CPU checks of the C ABI: the library loads, exports every entry point the
+header declares, keeps the reference's parameter indices, and its numerical
+entry points fail loudly without a GPU (no CPU fallback)."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, gpu_available
+
+HEADER = ROOT / "include" / "pastix_b200.h"
+
+
+def declared_functions():
+    src = HEADER.read_text()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^\s*(?:void|int)\s*\*?\s*([A-Za-z_]\w*)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_exports_every_declared_symbol(lib):
+    names = declared_functions()
+    assert len(names) >= 40
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_matches_header(lib):
+    from pastix_b200 import _lib
+    assert sorted(_lib.EXPORTS) == declared_functions()
+
+
+def _enum_names(name):
+    src = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    m = re.search(r"typedef enum %s \{(.*?)\}" % name, src, re.S)
+    return [x.strip() for x in m.group(1).split(",") if x.strip()]
+
+
+def test_parameter_indices():
+    from pastix_b200 import pastix as px
+    ip = _enum_names("pastix_iparm_e")
+    dp = _enum_names("pastix_dparm_e")
+    assert ip[-1] == "IPARM_SIZE" and len(ip) - 1 == int(px.iparm.size)
+    assert dp[-1] == "DPARM_SIZE" and len(dp) - 1 == int(px.dparm.size)
+    for e in px.iparm:
+        if e.name in ("size", "float_"):
+            continue
+        assert ip.index("IPARM_" + e.name.upper()) == int(e), e
+    for e in px.dparm:
+        if e.name == "size":
+            continue
+        assert dp.index("DPARM_" + e.name.upper()) == int(e), e
+
+
+def test_init_param_defaults(lib):
+    from pastix_b200 import pastix as px
+    ip, dp = px.initParam()
+    # common/api.c:420-571 defaults
+    assert ip[px.iparm.factorization] == px.factotype.LU
+    assert ip[px.iparm.min_blocksize] == 160 and ip[px.iparm.max_blocksize] == 320
+    assert ip[px.iparm.refinement] == px.refine.GMRES
+    assert ip[px.iparm.itermax] == 250 and ip[px.iparm.gmres_im] == 25
+    assert ip[px.iparm.mixed] == 0
+    assert dp[px.dparm.epsilon_refinement] == -1.0 and dp[px.dparm.epsilon_magn_ctrl] == 0.0
+
+
+def test_step_order_errors(lib):
+    from pastix_b200 import gen
+    from pastix_b200 import pastix as px
+    from pastix_b200.spm import mtxtype, spmatrix
+    ip, dp = px.initParam()
+    pd = px.init(ip, dp)
+    S = spmatrix(gen.laplacian7(4, 4, 4), mtxtype.Symmetric)
+    with pytest.raises(px.PastixError) as e:
+        px.subtask_symbfact(pd)  # before ordering
+    assert e.value.code == px.error.BADPARAMETER
+    with pytest.raises(px.PastixError):
+        px.task_numfact(pd, S)  # before analysis
+    x = np.zeros(64)
+    with pytest.raises(px.PastixError):
+        px.task_solve(pd, S, x)  # before numfact
+
+
+def test_bad_spm_rejected(lib):
+    from pastix_b200 import pastix as px
+    from pastix_b200.spm import spmatrix
+    import scipy.sparse as sps
+    ip, dp = px.initParam()
+    pd = px.init(ip, dp)
+    S = spmatrix(sps.identity(5, format="csc"))
+    S.spm.fmttype = 1  # CSR is not accepted
+    with pytest.raises(px.PastixError):
+        px.task_analyze(pd, S)
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU behaviour")
+def test_numeric_without_gpu_fails_loudly(lib):
+    from pastix_b200 import gen
+    from pastix_b200 import pastix as px
+    from pastix_b200.spm import mtxtype, spmatrix
+    ip, dp = px.initParam()
+    ip[px.iparm.factorization] = px.factotype.POTRF
+    pd = px.init(ip, dp)
+    S = spmatrix(gen.laplacian7(6, 6, 6), mtxtype.Symmetric)
+    px.analyze_grid(pd, S, 6, 6, 6)
+    with pytest.raises(px.PastixError) as e:
+        px.task_numfact(pd, S)
+    assert e.value.code == px.error.INTERNAL

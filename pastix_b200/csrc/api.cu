@@ -647,10 +647,10 @@ static int build_maps_and_lists(pastix_data_t *pd) {
                 L.small_smem_elems = std::max<size_t>(L.small_smem_elems, (size_t)(st * nc) * (fk == pgpu::FACT_GETRF ? 2 : 1));
             } else {
                 pd->large_list.push_back((int)k);
-                L.diag_smem_elems = std::max<size_t>(L.diag_smem_elems, (size_t)32 * nc * (fk == pgpu::FACT_GETRF ? 2 : 1));
+                L.diag_smem_elems = std::max<size_t>(L.diag_smem_elems, (size_t)pgpu::diag_smem_elems((int)nc, fk));
                 int bm = pgpu::trsm_tile_rows((int)nc);
                 for (idx_t r = nc; r < st; r += bm) pd->trsm_tiles.push_back(pgpu::RowTile{(int)k, (int)r});
-                if (st > nc) L.trsm_smem_elems = std::max<size_t>(L.trsm_smem_elems, (size_t)bm * nc);
+                if (st > nc) L.trsm_smem_elems = std::max<size_t>(L.trsm_smem_elems, (size_t)pgpu::trsm_smem_elems((int)nc));
             }
             for (idx_t r = nc; r < st; r += SR) pd->solve_tiles.push_back(pgpu::RowTile{(int)k, (int)r});
         }

@@ -27,9 +27,16 @@ struct UpdTile {
     int side;         // 0: L side, 1: U side (LU only)
 };
 
-// Rows of one off-diagonal TRSM tile of a cblk of width nc (its shared-memory
-// tile is rows x nc elements).
-__host__ __device__ inline int trsm_tile_rows(int nc) { return nc <= 160 ? 64 : 32; }
+// Rows of one off-diagonal TRSM tile (k_trsm); its shared memory holds the
+// tile and a 32-row strip of the triangular factor, 2 x 32 x (nc + 1) elements.
+__host__ __device__ inline int trsm_tile_rows(int) { return 32; }
+__host__ __device__ inline long long trsm_smem_elems(int nc) { return 2LL * 32 * (nc + 1); }
+
+// Shared memory of k_diag_large for a cblk of width nc: the nc x 32 column
+// panel (ld 33) and, for GETRF, the 32 x nc strip of U (ld nc + 1).
+__host__ __device__ inline long long diag_smem_elems(int nc, int fact) {
+    return (long long)nc * 33 + (fact == FACT_GETRF ? 32LL * (nc + 1) : 0);
+}
 
 // One row tile of a cblk's off-diagonal panel (TRSM and solve updates).
 struct RowTile {

@@ -144,10 +144,18 @@ __global__ void __launch_bounds__(256) k_panel_small(DevStruct s, const int *__r
 
 // ---------------------------------------------------------------------------
 // Wide cblks, diagonal block: blocked right-looking factorization by column
-// panels of DNB columns staged in shared memory, trailing update from shared
-// memory into the (L2-resident) diagonal block.
+// panels of DNB = 32 columns held row-major in shared memory.  Per panel:
+//   1. warp 0 factors the 32 x 32 top block column by column (pivot, scale,
+//      rank-1 update), as potf2 / getf2 / sytf2;
+//   2. the panel rows below are solved against that block, one warp per row,
+//      block columns on the lanes (the TRSM of the blocked algorithm);
+//   3. the trailing part of the diagonal block is updated from shared memory
+//      with 4 x 4 register tiles (SYRK / GEMM of the blocked algorithm).
+// GETRF keeps the 32-row strip of U to the right of the panel in shared
+// memory as well (its rows are solved with the unit lower factor).
 // ---------------------------------------------------------------------------
 constexpr int DNB = 32;
+constexpr int DLDW = DNB + 1;
 
 template <typename T, int FACT>
 __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__restrict__ list, T *L, T *U,
@@ -155,99 +163,147 @@ __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__re
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int k = list[blockIdx.x];
     const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
-    T *W = reinterpret_cast<T *>(smem_raw);  // m x DNB column panel, ld = nc
-    T *R = W + (size_t)DNB * nc;             // GETRF: DNB x nc row panel, ld = DNB
     const int st = s.cb_stride[k];
-    const int tid = threadIdx.x, nt = blockDim.x;
+    T *W = reinterpret_cast<T *>(smem_raw);  // m x DNB panel, row major, ld DLDW
+    T *R = W + (size_t)nc * DLDW;            // GETRF: DNB x t strip of U, row major, ld nc + 1
+    const int ldr = nc + 1;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     T *A = L + s.cb_coef[k];
     __shared__ int npiv;
     __shared__ T dsh[DNB];
     if (tid == 0) npiv = 0;
-    if (FACT == FACT_GETRF) {
+    if (FACT == FACT_GETRF) {  // L_kk += (U^T)_kk^T : the full diagonal block
         const T *Ut = U + s.cb_coef[k];
         for (int e = tid; e < nc * nc; e += nt) {
             int i = e % nc, j = e / nc;
-            A[i + j * st] += Ut[j + i * st];
+            A[i + (size_t)j * st] += Ut[j + (size_t)i * st];
         }
     }
     __syncthreads();
     for (int jb = 0; jb < nc; jb += DNB) {
         const int nb = min(DNB, nc - jb);
-        const int m = nc - jb;  // rows of the column panel
+        const int m = nc - jb;       // panel rows
+        const int t = m - nb;        // trailing size
         for (int e = tid; e < m * nb; e += nt) {
-            int i = e % m, j = e / m;
-            W[i + j * nc] = A[(jb + i) + (size_t)(jb + j) * st];
+            int i = e % m, c = e / m;
+            W[i * DLDW + c] = A[(jb + i) + (size_t)(jb + c) * st];
         }
-        if (FACT == FACT_GETRF) {  // row panel U12 = A[jb:jb+nb, jb+nb:nc]
-            const int w2 = nc - jb - nb;
-            for (int e = tid; e < nb * w2; e += nt) {
-                int i = e % nb, j = e / nb;
-                R[i + j * DNB] = A[(jb + i) + (size_t)(jb + nb + j) * st];
+        if (FACT == FACT_GETRF)
+            for (int e = tid; e < nb * t; e += nt) {
+                int c = e % nb, q = e / nb;
+                R[c * ldr + q] = A[(jb + c) + (size_t)(jb + nb + q) * st];
             }
+        __syncthreads();
+        // 1. the nb x nb top block, by warp 0
+        if (warp == 0) {
+            int np = 0;
+            for (int c = 0; c < nb; c++) {
+                T d = static_pivot<T, FACT>(W[c * DLDW + c], fp.criterion, np);
+                __syncwarp();
+                if (lane == c) W[c * DLDW + c] = d;
+                const T inv = T(1) / d;
+                if (lane > c && lane < nb) {
+                    if (FACT == FACT_SYTRF) W[c * DLDW + lane] = W[lane * DLDW + c];  // D L^T copy
+                    W[lane * DLDW + c] *= inv;
+                }
+                __syncwarp();
+                if (lane > c && lane < nb) {
+                    const T lic = W[lane * DLDW + c];
+                    for (int j = c + 1; j < nb; j++) {
+                        if (FACT == FACT_POTRF) {
+                            if (lane >= j) W[lane * DLDW + j] -= lic * W[j * DLDW + c];
+                        } else if (FACT == FACT_SYTRF) {
+                            if (lane >= j) W[lane * DLDW + j] -= lic * W[c * DLDW + j];
+                        } else {
+                            W[lane * DLDW + j] -= lic * W[c * DLDW + j];
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            if (lane == 0 && np) npiv += np;
         }
         __syncthreads();
-        for (int c = 0; c < nb; c++) {
-            if (tid == 0) {
-                int np = npiv;
-                W[c + c * nc] = static_pivot<T, FACT>(W[c + c * nc], fp.criterion, np);
-                npiv = np;
-                dsh[c] = W[c + c * nc];
-            }
-            __syncthreads();
-            const T inv = T(1) / W[c + c * nc];
-            for (int i = c + 1 + tid; i < m; i += nt) {
-                if (FACT == FACT_SYTRF && i < nb) W[c + i * nc] = W[i + c * nc];
-                W[i + c * nc] *= inv;
-            }
-            __syncthreads();
-            const int w = nb - c - 1;
-            const int h = m - c - 1;
-            for (int e = tid; e < h * w; e += nt) {
-                int i = c + 1 + e % h, j = c + 1 + e / h;
-                if (FACT == FACT_POTRF) {
-                    if (i >= j) W[i + j * nc] -= W[i + c * nc] * W[j + c * nc];
-                } else if (FACT == FACT_SYTRF) {
-                    if (i >= j) W[i + j * nc] -= W[i + c * nc] * W[c + j * nc];
-                } else {
-                    W[i + j * nc] -= W[i + c * nc] * W[c + j * nc];
+        if (FACT == FACT_SYTRF && tid < nb) dsh[tid] = W[tid * DLDW + tid];
+        // 2. panel rows below the block: x T = a, lanes = block columns
+        for (int r = nb + warp; r < m; r += nt / 32) {
+            T x = (lane < nb) ? W[r * DLDW + lane] : T(0);
+            for (int c = 0; c < nb; c++) {
+                if (lane == c) x /= W[c * DLDW + c];
+                T xc = __shfl_sync(0xffffffffu, x, c);
+                if (lane > c && lane < nb) {
+                    T tcl = (FACT == FACT_POTRF) ? W[lane * DLDW + c] : W[c * DLDW + lane];
+                    x -= xc * tcl;
                 }
             }
-            if (FACT == FACT_GETRF) {  // U12 rows: R[j, :] -= L[j,c] * R[c, :] for j > c
-                const int w2 = nc - jb - nb;
-                for (int e = tid; e < w * w2; e += nt) {
-                    int j = c + 1 + e % w, q = e / w;
-                    R[j + q * DNB] -= W[j + c * nc] * R[c + q * DNB];
+            if (lane < nb) W[r * DLDW + lane] = x;
+        }
+        if (FACT == FACT_GETRF)  // U12 <- L11^{-1} U12 (unit lower), one column per thread
+            for (int q = tid; q < t; q += nt)
+                for (int c = 0; c < nb; c++) {
+                    const T u = R[c * ldr + q];
+                    for (int j = c + 1; j < nb; j++) R[j * ldr + q] -= W[j * DLDW + c] * u;
                 }
-            }
-            __syncthreads();
-        }
-        for (int e = tid; e < m * nb; e += nt) {
-            int i = e % m, j = e / m;
-            A[(jb + i) + (size_t)(jb + j) * st] = W[i + j * nc];
-        }
-        if (FACT == FACT_GETRF) {
-            const int w2 = nc - jb - nb;
-            for (int e = tid; e < nb * w2; e += nt) {
-                int i = e % nb, j = e / nb;
-                A[(jb + i) + (size_t)(jb + nb + j) * st] = R[i + j * DNB];
-            }
-        }
         __syncthreads();
-        // trailing update of A[jb+nb:nc, jb+nb:nc]
-        const int t = nc - jb - nb;
+        for (int e = tid; e < m * nb; e += nt) {
+            int i = e % m, c = e / m;
+            A[(jb + i) + (size_t)(jb + c) * st] = W[i * DLDW + c];
+        }
+        if (FACT == FACT_GETRF)
+            for (int e = tid; e < nb * t; e += nt) {
+                int c = e % nb, q = e / nb;
+                A[(jb + c) + (size_t)(jb + nb + q) * st] = R[c * ldr + q];
+            }
+        // 3. trailing update A22 -= L21 * B^T (4x4 blocks; lower triangle for the symmetric kinds)
         if (t > 0) {
-            for (int e = tid; e < t * t; e += nt) {
-                int i = e % t, j = e / t;
-                if (FACT != FACT_GETRF && i < j) continue;
-                T acc = T(0);
-                if (FACT == FACT_POTRF) {
-                    for (int c = 0; c < nb; c++) acc += W[(nb + i) + c * nc] * W[(nb + j) + c * nc];
-                } else if (FACT == FACT_SYTRF) {
-                    for (int c = 0; c < nb; c++) acc += W[(nb + i) + c * nc] * (dsh[c] * W[(nb + j) + c * nc]);
+            const int nbt = (t + 3) / 4;
+            const int nblk = (FACT == FACT_GETRF) ? nbt * nbt : nbt * (nbt + 1) / 2;
+            for (int id = tid; id < nblk; id += nt) {
+                int bi, bj;
+                if (FACT == FACT_GETRF) {
+                    bi = id % nbt;
+                    bj = id / nbt;
                 } else {
-                    for (int c = 0; c < nb; c++) acc += W[(nb + i) + c * nc] * R[c + j * DNB];
+                    bi = (int)((sqrt(8.0 * id + 1.0) - 1.0) * 0.5);
+                    while (bi * (bi + 1) / 2 > id) bi--;
+                    while ((bi + 1) * (bi + 2) / 2 <= id) bi++;
+                    bj = id - bi * (bi + 1) / 2;
                 }
-                A[(jb + nb + i) + (size_t)(jb + nb + j) * st] -= acc;
+                T acc[4][4];
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) acc[i][j] = T(0);
+                for (int c = 0; c < nb; c++) {
+                    T a[4], b[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        int r = bi * 4 + i;
+                        a[i] = (r < t) ? W[(nb + r) * DLDW + c] : T(0);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        int q = bj * 4 + j;
+                        if (FACT == FACT_GETRF) b[j] = (q < t) ? R[c * ldr + q] : T(0);
+                        else if (FACT == FACT_SYTRF) b[j] = (q < t) ? dsh[c] * W[(nb + q) * DLDW + c] : T(0);
+                        else b[j] = (q < t) ? W[(nb + q) * DLDW + c] : T(0);
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int j = 0; j < 4; j++) acc[i][j] += a[i] * b[j];
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    int q = bj * 4 + j;
+                    if (q >= t) continue;
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        int r = bi * 4 + i;
+                        if (r >= t || (FACT != FACT_GETRF && r < q)) continue;
+                        A[(jb + nb + r) + (size_t)(jb + nb + q) * st] -= acc[i][j];
+                    }
+                }
             }
         }
         __syncthreads();
@@ -259,6 +315,7 @@ __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__re
         }
     }
     if (FACT == FACT_GETRF) {  // (U^T)_kk = (L\U)_kk^T
+        __syncthreads();
         T *Ut = U + s.cb_coef[k];
         for (int e = tid; e < nc * nc; e += nt) {
             int i = e % nc, j = e / nc;
@@ -269,55 +326,108 @@ __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__re
 }
 
 // ---------------------------------------------------------------------------
-// Wide cblks, off-diagonal TRSM: X T = A on a tile of rows held in shared
-// memory, T the upper triangular factor of the diagonal block:
+// Wide cblks, off-diagonal TRSM: X T = A for a tile of TRSM_ROWS panel rows,
+// T the upper triangular factor of the diagonal block:
 //   POTRF       T = L_kk^T            (Right, Lower, Trans, NonUnit)
 //   SYTRF       T = D_kk L_kk^T        (Right, Upper, NoTrans, NonUnit on DL^T)
 //   GETRF side0 T = U_kk  (upper of L) (Right, Upper, NoTrans, NonUnit)
 //   GETRF side1 T = L_kk^T (unit)      (Right, Upper, NoTrans, Unit on U panel)
-// blockIdx.y selects the GETRF side.
+// blockIdx.y selects the GETRF side.  Blocked by 32 columns (the blocked
+// algorithm of a BLAS TRSM): a 32-wide block is solved by substitution, one
+// warp per 4 rows with the block's columns on the lanes, then the columns to
+// its right are updated by a register-tiled GEMM from shared memory.  The tile
+// of X (row major) and the current 32-row strip of T live in shared memory.
 // ---------------------------------------------------------------------------
+constexpr int TRSM_ROWS = 32;
+constexpr int TRSM_MAXT = 10;  // column chunks of 32 per GEMM pass
+
 template <typename T, int FACT>
 __global__ void __launch_bounds__(256) k_trsm(DevStruct s, const RowTile *__restrict__ tiles, T *L, T *U) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *X = reinterpret_cast<T *>(smem_raw);  // bm x nc, ld = bm
     const RowTile tl = tiles[blockIdx.x];
     const int side = blockIdx.y;
     const int k = tl.cblk;
     const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
-    const int bm = trsm_tile_rows(nc);
     const int st = s.cb_stride[k];
-    const int rows = min(bm, st - tl.r0);
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int rows = min(TRSM_ROWS, st - tl.r0);
+    const int ld = nc + 1;
+    T *X = reinterpret_cast<T *>(smem_raw);  // TRSM_ROWS x nc, row major, ld
+    T *Ts = X + TRSM_ROWS * ld;              // 32 x (nc - jb) strip of T, row major, ld
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const T *D = L + s.cb_coef[k];  // diagonal block (ld = st) of the L panel
     T *A = ((FACT == FACT_GETRF && side == 1) ? U : L) + s.cb_coef[k] + tl.r0;
-    for (int e = tid; e < rows * nc; e += nt) {
-        int i = e % rows, j = e / rows;
-        X[i + j * bm] = A[i + (size_t)j * st];
-    }
-    __syncthreads();
     const bool unit = (FACT == FACT_GETRF && side == 1);
-    for (int c = 0; c < nc; c++) {
-        if (!unit) {
-            const T inv = T(1) / D[c + (size_t)c * st];
-            for (int i = tid; i < rows; i += nt) X[i + c * bm] *= inv;
-            __syncthreads();
-        }
-        const int w = nc - c - 1;
-        for (int e = tid; e < rows * w; e += nt) {
-            int i = e % rows, j = c + 1 + e / rows;
+    for (int e = tid; e < TRSM_ROWS * nc; e += blockDim.x) {
+        int i = e % TRSM_ROWS, j = e / TRSM_ROWS;
+        X[i * ld + j] = (i < rows) ? A[i + (size_t)j * st] : T(0);
+    }
+    for (int jb = 0; jb < nc; jb += 32) {
+        const int nb = min(32, nc - jb);
+        const int wdt = nc - jb;
+        __syncthreads();
+        for (int e = tid; e < nb * wdt; e += blockDim.x) {  // Ts[a][q] = T(jb + a, jb + q)
+            int q = e % wdt, a = e / wdt;
+            int ga = jb + a, gb = jb + q;
             T t;
-            if (FACT == FACT_POTRF) t = D[j + (size_t)c * st];
-            else if (FACT == FACT_SYTRF) t = D[c + (size_t)c * st] * D[j + (size_t)c * st];
-            else if (side == 0) t = D[c + (size_t)j * st];
-            else t = D[j + (size_t)c * st];
-            X[i + j * bm] -= X[i + c * bm] * t;
+            if (gb < ga) t = T(0);
+            else if (FACT == FACT_POTRF) t = D[gb + (size_t)ga * st];
+            else if (FACT == FACT_SYTRF) t = (gb == ga) ? D[ga + (size_t)ga * st]
+                                                          : D[ga + (size_t)ga * st] * D[gb + (size_t)ga * st];
+            else if (side == 0) t = D[ga + (size_t)gb * st];
+            else t = D[gb + (size_t)ga * st];
+            Ts[a * ld + q] = t;
         }
         __syncthreads();
+        // substitution on the 32-wide block: warp w owns rows 4w .. 4w+3
+#pragma unroll
+        for (int rr = 0; rr < 4; rr++) {
+            const int r = warp * 4 + rr;
+            T x = (lane < nb) ? X[r * ld + jb + lane] : T(0);
+            for (int c = 0; c < nb; c++) {
+                if (!unit && lane == c) x /= Ts[c * ld + c];
+                T xc = __shfl_sync(0xffffffffu, x, c);
+                if (lane > c && lane < nb) x -= xc * Ts[c * ld + lane];
+            }
+            if (lane < nb) X[r * ld + jb + lane] = x;
+        }
+        __syncthreads();
+        // X[:, jb+nb:] -= X[:, jb:jb+nb] * Ts[:, nb:]
+        const int rest = wdt - nb;
+        for (int cb = 0; cb < rest; cb += 32 * TRSM_MAXT) {
+            T acc[4][TRSM_MAXT];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int t = 0; t < TRSM_MAXT; t++) acc[i][t] = T(0);
+            const int r0 = warp * 4;
+            for (int kk = 0; kk < nb; kk++) {
+                T a[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) a[i] = X[(r0 + i) * ld + jb + kk];
+#pragma unroll
+                for (int t = 0; t < TRSM_MAXT; t++) {
+                    const int q = cb + lane + 32 * t;
+                    if (q < rest) {
+                        const T bq = Ts[kk * ld + nb + q];
+#pragma unroll
+                        for (int i = 0; i < 4; i++) acc[i][t] += a[i] * bq;
+                    }
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < TRSM_MAXT; t++) {
+                const int q = cb + lane + 32 * t;
+                if (q < rest) {
+#pragma unroll
+                    for (int i = 0; i < 4; i++) X[(r0 + i) * ld + jb + nb + q] -= acc[i][t];
+                }
+            }
+        }
     }
-    for (int e = tid; e < rows * nc; e += nt) {
+    __syncthreads();
+    for (int e = tid; e < rows * nc; e += blockDim.x) {
         int i = e % rows, j = e / rows;
-        A[i + (size_t)j * st] = X[i + j * bm];
+        A[i + (size_t)j * st] = X[i * ld + j];
     }
 }
 

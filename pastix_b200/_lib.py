@@ -35,7 +35,7 @@ EXPORTS = [
 
 # kernel classes of pgpu_profile_get, in order
 PROFILE_CLASSES = ["fill", "panel_small", "diag_large", "trsm", "update", "fwd_diag", "fwd_update",
-                   "bwd_update", "bwd_diag", "spmv", "vec"]
+                   "bwd_update", "bwd_diag", "spmv", "vec", "update_big"]
 
 
 class spmatrix_t(C.Structure):

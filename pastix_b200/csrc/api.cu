@@ -36,11 +36,13 @@ void launch_fill_coef(int64_t, const double *, const int64_t *, const int64_t *,
 template <typename T, int F>
 void launch_panel_small(const DevStruct &, const int *, int, size_t, T *, T *, const FactParams &, cudaStream_t);
 template <typename T, int F>
-void launch_diag_large(const DevStruct &, const int *, int, size_t, T *, T *, const FactParams &, cudaStream_t);
+void launch_diag_large(const DevStruct &, const int *, int, size_t, T *, T *, T *, const FactParams &, cudaStream_t);
 template <typename T, int F>
-void launch_trsm(const DevStruct &, const RowTile *, int, size_t, T *, T *, cudaStream_t);
+void launch_trsm(const DevStruct &, const RowTile *, int, size_t, T *, T *, const T *, cudaStream_t);
 template <typename T, int F>
 void launch_update(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);
+template <typename T, int F>
+void launch_update_big(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);
 template <typename T, int F>
 cudaError_t set_smem_attrs(size_t, size_t, size_t);
 // solve.cu
@@ -49,7 +51,13 @@ void launch_fwd_diag(const DevStruct &, const int *, int, int, const T *, int, T
 template <typename T>
 void launch_fwd_update(const DevStruct &, const RowTile *, int, int, const T *, T *, int, int, cudaStream_t);
 template <typename T>
-void launch_bwd_update(const DevStruct &, const RowTile *, int, const T *, T *, int, int, cudaStream_t);
+void launch_bwd_update(const DevStruct &, const RowTile *, int, int, const T *, T *, int, int, cudaStream_t);
+template <typename T>
+void launch_fwd_diag_inv(const DevStruct &, const int *, int, int, const T *, const T *, int, int, const T *, T *,
+                         int, int, cudaStream_t);
+template <typename T>
+void launch_bwd_diag_inv(const DevStruct &, const int *, int, int, const T *, const T *, int, int, const T *, T *,
+                         int, int, cudaStream_t);
 template <typename T>
 void launch_bwd_diag(const DevStruct &, const int *, int, int, const T *, int, T *, int, int, cudaStream_t);
 template <typename T>
@@ -77,7 +85,7 @@ using pgpu::idx_t;
 // kernel classes for launch accounting (pgpu_profile_get)
 enum : int {
     PC_FILL = 0, PC_PANEL_SMALL, PC_DIAG_LARGE, PC_TRSM, PC_UPDATE, PC_FWD_DIAG, PC_FWD_UPDATE, PC_BWD_UPDATE,
-    PC_BWD_DIAG, PC_SPMV, PC_VEC, PGPU_NCLASS
+    PC_BWD_DIAG, PC_SPMV, PC_VEC, PC_UPDATE_BIG, PGPU_NCLASS
 };
 
 // ---------------------------------------------------------------------------
@@ -123,7 +131,8 @@ struct LevelLists {
     int small0, small1;     // k_panel_small cblks
     int large0, large1;     // k_diag_large cblks
     int trsm0, trsm1;       // k_trsm row tiles
-    int upd0, upd1;         // k_update tiles
+    int upd0, upd1;         // k_update tiles (64 x 64)
+    int updb0, updb1;       // big update tiles (128 x 64): DMMA for FP64
     int cb0, cb1;           // all cblks of the level (solve diag)
     int st0, st1;           // solve row tiles
     int maxnc;
@@ -136,23 +145,24 @@ struct Device {
     cudaStream_t stream = nullptr;
     // structure
     DBuf<int> cb_fcol, cb_lcol, cb_stride, cb_fblok, bk_frow, bk_lrow, bk_rowoff, bk_fcblk, rowidx;
-    DBuf<int64_t> cb_coef, cb_rowidx;
+    DBuf<int64_t> cb_coef, cb_rowidx, cb_dinv;
     DBuf<pgpu::TaskDev> tasks;
     DBuf<int> small_list, large_list, level_cblks;
     DBuf<pgpu::RowTile> trsm_tiles, solve_tiles;
-    DBuf<pgpu::UpdTile> upd_tiles;
+    DBuf<pgpu::UpdTile> upd_tiles, upd_big_tiles;
     // matrix
     DBuf<double> vals, csr_val;
     DBuf<int64_t> lmap, umap, csr_src, perm;
     DBuf<int> csr_rowptr, csr_col, e_row, e_col;
     // factor
-    DBuf<unsigned char> Lc, Uc;
+    DBuf<unsigned char> Lc, Uc, dinv;  // panels; inverted 32x32 diagonal sub-blocks of wide cblks
     int fltsize = 0;
     // work
     DBuf<int> counters;      // [0] nbpivots, [1] status
     DBuf<double> part, scal; // reduction partials, scalars
     DBuf<double> w1, w2;     // permuted double work vectors
     DBuf<float> wf;          // float work for mixed precision
+    DBuf<double> ws[12];     // grow-only work areas (no allocation in the steady state)
     pgpu::DevStruct ds{};
 };
 
@@ -186,8 +196,10 @@ struct pastix_data_s {
     // host copies of the launch lists
     std::vector<int> small_list, large_list, level_cblks;
     std::vector<pgpu::RowTile> trsm_tiles, solve_tiles;
-    std::vector<pgpu::UpdTile> upd_tiles;
+    std::vector<pgpu::UpdTile> upd_tiles, upd_big_tiles;
     std::vector<pgpu::TaskDev> tasks;
+    std::vector<int64_t> cb_dinv;
+    int64_t dinv_total = 0;
     int factotype = PastixFactPOTRF;
     int mixed = 0;
     double anorm = 0.0;
@@ -217,6 +229,16 @@ static inline void launch_cls(pastix_data_t *pd, int cls, long long count, Fn &&
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
+enum : int { WS_SOLVE = 0, WS_ORDER, WS_GMV, WS_GMW, WS_GMG, WS_VEC, WS_BP, WS_XP, WS_RB, WS_RX };
+
+// Persistent device work area `slot` of at least `count` doubles (grown, never shrunk).
+static double *work(Device &d, int slot, size_t count) {
+    DBuf<double> &b = d.ws[slot];
+    if (b.n < count) {
+        if (b.alloc(count) != cudaSuccess) return nullptr;
+    }
+    return b.p;
+}
 static void perr(const char *fmt, ...) {
     va_list ap;
     va_start(ap, fmt);
@@ -600,7 +622,7 @@ static int build_maps_and_lists(pastix_data_t *pd) {
     // ---- launch lists per level ----
     pd->levels.assign(sv.nlevels, LevelLists{});
     pd->small_list.clear(); pd->large_list.clear(); pd->level_cblks.clear();
-    pd->trsm_tiles.clear(); pd->solve_tiles.clear(); pd->upd_tiles.clear();
+    pd->trsm_tiles.clear(); pd->solve_tiles.clear(); pd->upd_tiles.clear(); pd->upd_big_tiles.clear();
     // exclusive tasks: dst targeted by a single source in the level
     pd->tasks.resize(sv.tasks.size());
     {
@@ -628,6 +650,8 @@ static int build_maps_and_lists(pastix_data_t *pd) {
         }
     }
     const int SR = pgpu::solve_rows_per_tile();
+    pd->cb_dinv.assign(sv.cblknbr, -1);
+    pd->dinv_total = 0;
     for (idx_t l = 0; l < sv.nlevels; l++) {
         LevelLists &L = pd->levels[l];
         L.small0 = (int)pd->small_list.size();
@@ -647,6 +671,8 @@ static int build_maps_and_lists(pastix_data_t *pd) {
                 L.small_smem_elems = std::max<size_t>(L.small_smem_elems, (size_t)(st * nc) * (fk == pgpu::FACT_GETRF ? 2 : 1));
             } else {
                 pd->large_list.push_back((int)k);
+                pd->cb_dinv[k] = pd->dinv_total;
+                pd->dinv_total += pgpu::dinv_elems((int)nc, fk);
                 L.diag_smem_elems = std::max<size_t>(L.diag_smem_elems, (size_t)pgpu::diag_smem_elems((int)nc, fk));
                 int bm = pgpu::trsm_tile_rows((int)nc);
                 for (idx_t r = nc; r < st; r += bm) pd->trsm_tiles.push_back(pgpu::RowTile{(int)k, (int)r});
@@ -660,22 +686,27 @@ static int build_maps_and_lists(pastix_data_t *pd) {
         L.cb1 = (int)pd->level_cblks.size();
         L.st1 = (int)pd->solve_tiles.size();
         L.upd0 = (int)pd->upd_tiles.size();
+        L.updb0 = (int)pd->upd_big_tiles.size();
         for (idx_t t = sv.lvl_task_ptr[l]; t < sv.lvl_task_ptr[l + 1]; t++) {
             const auto &tk = sv.tasks[t];
-            const int B = 64;
+            const idx_t K = sv.cb_lcol[tk.src] - sv.cb_fcol[tk.src] + 1;
+            const bool big = tk.n >= 32 && K >= 32;
+            const idx_t BM = big ? 128 : 64, BN = 64;
+            auto &list = big ? pd->upd_big_tiles : pd->upd_tiles;
             for (int side = 0; side < (fk == pgpu::FACT_GETRF ? 2 : 1); side++) {
                 idx_t M = tk.m - (side ? tk.n : 0);
                 if (M <= 0) continue;
-                idx_t mt = (M + B - 1) / B, ntl = (tk.n + B - 1) / B;
+                idx_t mt = (M + BM - 1) / BM, ntl = (tk.n + BN - 1) / BN;
                 for (idx_t a = 0; a < mt; a++)
                     for (idx_t c = 0; c < ntl; c++) {
                         // symmetric kinds: skip tiles strictly above the diagonal of the square part
-                        if (fk != pgpu::FACT_GETRF && (a + 1) * B <= c * B) continue;
-                        pd->upd_tiles.push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
+                        if (fk != pgpu::FACT_GETRF && (a + 1) * BM <= c * BN) continue;
+                        list.push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
                     }
             }
         }
         L.upd1 = (int)pd->upd_tiles.size();
+        L.updb1 = (int)pd->upd_big_tiles.size();
     }
     return PASTIX_SUCCESS;
 }
@@ -690,6 +721,8 @@ extern "C" int pastix_subtask_blend(pastix_data_t *pd) {
     double t0 = now_s();
     idx_t bmin = pd->iparm[IPARM_MIN_BLOCKSIZE], bmax = pd->iparm[IPARM_MAX_BLOCKSIZE];
     if (bmin > bmax || bmin < 1) { perr("IPARM_MIN_BLOCKSIZE > IPARM_MAX_BLOCKSIZE"); return PASTIX_ERR_BADPARAMETER; }
+    // the wide-cblk kernels keep a (32 x width) strip per operand in shared memory
+    if (bmax > 384) { perr("IPARM_MAX_BLOCKSIZE above 384 is not supported by the GPU kernels"); return PASTIX_ERR_BADPARAMETER; }
     pgpu::symbol_split(pd->symbol, bmin, bmax);
     std::string err = pgpu::symbol_check(pd->symbol);
     if (!err.empty()) { perr("symbol check failed: %s", err.c_str()); return PASTIX_ERR_INTERNAL; }
@@ -782,6 +815,7 @@ static int device_setup(pastix_data_t *pd) {
     std::vector<int64_t> coef(sv.cb_coef.begin(), sv.cb_coef.end()), ridx(sv.cb_rowidx.begin(), sv.cb_rowidx.end());
     CUDA_TRY(d.cb_coef.upload(coef, st));
     CUDA_TRY(d.cb_rowidx.upload(ridx, st));
+    CUDA_TRY(d.cb_dinv.upload(pd->cb_dinv, st));
     CUDA_TRY(d.tasks.upload(pd->tasks, st));
     CUDA_TRY(d.small_list.upload(pd->small_list, st));
     CUDA_TRY(d.large_list.upload(pd->large_list, st));
@@ -789,6 +823,7 @@ static int device_setup(pastix_data_t *pd) {
     CUDA_TRY(d.trsm_tiles.upload(pd->trsm_tiles, st));
     CUDA_TRY(d.solve_tiles.upload(pd->solve_tiles, st));
     CUDA_TRY(d.upd_tiles.upload(pd->upd_tiles, st));
+    CUDA_TRY(d.upd_big_tiles.upload(pd->upd_big_tiles, st));
     CUDA_TRY(d.lmap.upload(pd->lmap, st));
     if (!pd->umap.empty()) CUDA_TRY(d.umap.upload(pd->umap, st));
     else d.umap.reset();
@@ -809,7 +844,7 @@ static int device_setup(pastix_data_t *pd) {
     s.n = (int)sv.n;
     s.cblknbr = (int)sv.cblknbr;
     s.cb_fcol = d.cb_fcol.p; s.cb_lcol = d.cb_lcol.p; s.cb_stride = d.cb_stride.p; s.cb_fblok = d.cb_fblok.p;
-    s.cb_coef = d.cb_coef.p; s.cb_rowidx = d.cb_rowidx.p;
+    s.cb_coef = d.cb_coef.p; s.cb_rowidx = d.cb_rowidx.p; s.cb_dinv = d.cb_dinv.p;
     s.bk_frow = d.bk_frow.p; s.bk_lrow = d.bk_lrow.p; s.bk_rowoff = d.bk_rowoff.p; s.bk_fcblk = d.bk_fcblk.p;
     s.rowidx = d.rowidx.p;
     s.tasks = d.tasks.p;
@@ -838,6 +873,7 @@ static int run_factor(pastix_data_t *pd, double criterion) {
     cudaStream_t st = d.stream;
     T *L = reinterpret_cast<T *>(d.Lc.p);
     T *U = reinterpret_cast<T *>(d.Uc.p);
+    T *Dinv = reinterpret_cast<T *>(d.dinv.p);
     pgpu::FactParams fp{criterion, d.counters.p, d.counters.p + 1};
     for (size_t l = 0; l < pd->levels.size(); l++) {
         const LevelLists &lv = pd->levels[l];
@@ -847,14 +883,17 @@ static int run_factor(pastix_data_t *pd, double criterion) {
         });
         launch_cls(pd, PC_DIAG_LARGE, lv.large1 - lv.large0, [&] {
             pgpu::launch_diag_large<T, F>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0,
-                                          lv.diag_smem_elems * sizeof(T), L, U, fp, st);
+                                          lv.diag_smem_elems * sizeof(T), L, U, Dinv, fp, st);
         });
         launch_cls(pd, PC_TRSM, lv.trsm1 - lv.trsm0, [&] {
             pgpu::launch_trsm<T, F>(d.ds, d.trsm_tiles.p + lv.trsm0, lv.trsm1 - lv.trsm0,
-                                    lv.trsm_smem_elems * sizeof(T), L, U, st);
+                                    lv.trsm_smem_elems * sizeof(T), L, U, Dinv, st);
         });
         launch_cls(pd, PC_UPDATE, lv.upd1 - lv.upd0, [&] {
             pgpu::launch_update<T, F>(d.ds, d.upd_tiles.p + lv.upd0, lv.upd1 - lv.upd0, L, U, st);
+        });
+        launch_cls(pd, PC_UPDATE_BIG, lv.updb1 - lv.updb0, [&] {
+            pgpu::launch_update_big<T, F>(d.ds, d.upd_big_tiles.p + lv.updb0, lv.updb1 - lv.updb0, L, U, st);
         });
     }
     CUDA_TRY(cudaGetLastError());
@@ -943,6 +982,8 @@ extern "C" int pastix_subtask_bcsc2ctab(pastix_data_t *pd) {
     if (d.Lc.n != bytes) CUDA_TRY(d.Lc.alloc(bytes));
     if (fk == pgpu::FACT_GETRF) { if (d.Uc.n != bytes) CUDA_TRY(d.Uc.alloc(bytes)); }
     else d.Uc.reset();
+    const size_t dbytes = (size_t)std::max<int64_t>(1, pd->dinv_total) * fs;
+    if (d.dinv.n != dbytes) CUDA_TRY(d.dinv.alloc(dbytes));
     d.fltsize = fs;
     CUDA_TRY(cudaMemsetAsync(d.Lc.p, 0, bytes, d.stream));
     if (d.Uc.p) CUDA_TRY(cudaMemsetAsync(d.Uc.p, 0, bytes, d.stream));
@@ -1039,15 +1080,23 @@ extern "C" int pgpu_device_status(const pastix_data_t *pd) {
 // ---------------------------------------------------------------------------
 // solve on permuted device vectors
 // ---------------------------------------------------------------------------
-// forward with panel P (lower), unit or not
+// Forward sweep with the block-lower panel P (unit diagonal or not).  Wide
+// cblks apply their diagonal blocks with the inverted sub-blocks (set zside,
+// D scaling for LDL^T), narrow ones by substitution.
 template <typename T>
-static void sweep_forward(pastix_data_t *pd, const T *P, int unit, T *Y, int ldy, int nrhs) {
+static void sweep_forward(pastix_data_t *pd, const T *P, int unit, int zside, int scaled, T *Y, int ldy, int nrhs) {
     Device &d = pd->dev;
+    const T *Ld = reinterpret_cast<const T *>(d.Lc.p);
+    const T *Dinv = reinterpret_cast<const T *>(d.dinv.p);
     for (size_t l = 0; l < pd->levels.size(); l++) {
         const LevelLists &lv = pd->levels[l];
-        launch_cls(pd, PC_FWD_DIAG, lv.cb1 - lv.cb0, [&] {
-            pgpu::launch_fwd_diag<T>(d.ds, d.level_cblks.p + lv.cb0, lv.cb1 - lv.cb0, lv.maxnc, P, unit, Y, ldy,
-                                     nrhs, d.stream);
+        launch_cls(pd, PC_FWD_DIAG, lv.small1 - lv.small0, [&] {
+            pgpu::launch_fwd_diag<T>(d.ds, d.small_list.p + lv.small0, lv.small1 - lv.small0, lv.maxnc, P, unit, Y,
+                                     ldy, nrhs, d.stream);
+        });
+        launch_cls(pd, PC_FWD_DIAG, lv.large1 - lv.large0, [&] {
+            pgpu::launch_fwd_diag_inv<T>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0, lv.maxnc, P, Dinv,
+                                         zside, scaled, Ld, Y, ldy, nrhs, d.stream);
         });
         launch_cls(pd, PC_FWD_UPDATE, lv.st1 - lv.st0, [&] {
             pgpu::launch_fwd_update<T>(d.ds, d.solve_tiles.p + lv.st0, lv.st1 - lv.st0, lv.maxnc, P, Y, ldy, nrhs,
@@ -1055,18 +1104,25 @@ static void sweep_forward(pastix_data_t *pd, const T *P, int unit, T *Y, int ldy
         });
     }
 }
-// backward: solve P^T x = y with P lower
+// Backward sweep: solve P^T x = y with P block lower.
 template <typename T>
-static void sweep_backward(pastix_data_t *pd, const T *P, int unit, T *Y, int ldy, int nrhs) {
+static void sweep_backward(pastix_data_t *pd, const T *P, int unit, int zside, int scaled, T *Y, int ldy, int nrhs) {
     Device &d = pd->dev;
+    const T *Ld = reinterpret_cast<const T *>(d.Lc.p);
+    const T *Dinv = reinterpret_cast<const T *>(d.dinv.p);
     for (size_t l = pd->levels.size(); l-- > 0;) {
         const LevelLists &lv = pd->levels[l];
         launch_cls(pd, PC_BWD_UPDATE, lv.st1 - lv.st0, [&] {
-            pgpu::launch_bwd_update<T>(d.ds, d.solve_tiles.p + lv.st0, lv.st1 - lv.st0, P, Y, ldy, nrhs, d.stream);
+            pgpu::launch_bwd_update<T>(d.ds, d.solve_tiles.p + lv.st0, lv.st1 - lv.st0, lv.maxnc, P, Y, ldy, nrhs,
+                                       d.stream);
         });
-        launch_cls(pd, PC_BWD_DIAG, lv.cb1 - lv.cb0, [&] {
-            pgpu::launch_bwd_diag<T>(d.ds, d.level_cblks.p + lv.cb0, lv.cb1 - lv.cb0, lv.maxnc, P, unit, Y, ldy,
-                                     nrhs, d.stream);
+        launch_cls(pd, PC_BWD_DIAG, lv.small1 - lv.small0, [&] {
+            pgpu::launch_bwd_diag<T>(d.ds, d.small_list.p + lv.small0, lv.small1 - lv.small0, lv.maxnc, P, unit, Y,
+                                     ldy, nrhs, d.stream);
+        });
+        launch_cls(pd, PC_BWD_DIAG, lv.large1 - lv.large0, [&] {
+            pgpu::launch_bwd_diag_inv<T>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0, lv.maxnc, P, Dinv,
+                                         zside, scaled, Ld, Y, ldy, nrhs, d.stream);
         });
     }
 }
@@ -1080,18 +1136,20 @@ static void solve_perm(pastix_data_t *pd, int trans, T *Y, int ldy, int nrhs) {
     const T *U = reinterpret_cast<const T *>(d.Uc.p);
     int fk = fact_kind(pd);
     if (fk == pgpu::FACT_POTRF) {
-        sweep_forward<T>(pd, L, 0, Y, ldy, nrhs);
-        sweep_backward<T>(pd, L, 0, Y, ldy, nrhs);
+        sweep_forward<T>(pd, L, 0, 0, 0, Y, ldy, nrhs);
+        sweep_backward<T>(pd, L, 0, 0, 0, Y, ldy, nrhs);
     } else if (fk == pgpu::FACT_SYTRF) {
-        sweep_forward<T>(pd, L, 1, Y, ldy, nrhs);
-        pgpu::launch_diag_scale<T>(d.ds, (int)pd->solver.cblknbr, L, Y, ldy, nrhs, d.stream);
-        sweep_backward<T>(pd, L, 1, Y, ldy, nrhs);
+        sweep_forward<T>(pd, L, 1, 0, 1, Y, ldy, nrhs);
+        launch_cls(pd, PC_VEC, 1, [&] {
+            pgpu::launch_diag_scale<T>(d.ds, (int)pd->solver.cblknbr, L, Y, ldy, nrhs, d.stream);
+        });
+        sweep_backward<T>(pd, L, 1, 0, 1, Y, ldy, nrhs);
     } else if (!trans) {  // L (unit) then U through U^T
-        sweep_forward<T>(pd, L, 1, Y, ldy, nrhs);
-        sweep_backward<T>(pd, U, 0, Y, ldy, nrhs);
+        sweep_forward<T>(pd, L, 1, 1, 0, Y, ldy, nrhs);
+        sweep_backward<T>(pd, U, 0, 0, 0, Y, ldy, nrhs);
     } else {  // A^T = U^T L^T
-        sweep_forward<T>(pd, U, 0, Y, ldy, nrhs);
-        sweep_backward<T>(pd, L, 1, Y, ldy, nrhs);
+        sweep_forward<T>(pd, U, 0, 0, 0, Y, ldy, nrhs);
+        sweep_backward<T>(pd, L, 1, 1, 0, Y, ldy, nrhs);
     }
 }
 
@@ -1169,14 +1227,14 @@ extern "C" int pastix_task_solve(pastix_data_t *pd, pastix_int_t m, pastix_int_t
     Device &d = pd->dev;
     CUDA_TRY(cudaSetDevice(d.dev));
     double t0 = now_s();
-    DBuf<double> buf;
-    CUDA_TRY(buf.alloc((size_t)m * nrhs));
-    CUDA_TRY(cudaMemcpy2DAsync(buf.p, m * sizeof(double), B, ldb * sizeof(double), m * sizeof(double), nrhs,
+    double *buf = work(d, WS_SOLVE, (size_t)m * nrhs);
+    if (!buf) return PASTIX_ERR_OUTOFMEMORY;
+    CUDA_TRY(cudaMemcpy2DAsync(buf, m * sizeof(double), B, ldb * sizeof(double), m * sizeof(double), nrhs,
                                cudaMemcpyHostToDevice, d.stream));
     int trans = pd->iparm[IPARM_TRANSPOSE_SOLVE] == PastixTrans ? 1 : 0;
-    rc = solve_device_orig(pd, trans, (int)nrhs, buf.p, m, d.stream);
+    rc = solve_device_orig(pd, trans, (int)nrhs, buf, m, d.stream);
     if (rc) return rc;
-    CUDA_TRY(cudaMemcpy2DAsync(B, ldb * sizeof(double), buf.p, m * sizeof(double), m * sizeof(double), nrhs,
+    CUDA_TRY(cudaMemcpy2DAsync(B, ldb * sizeof(double), buf, m * sizeof(double), m * sizeof(double), nrhs,
                                cudaMemcpyDeviceToHost, d.stream));
     CUDA_TRY(cudaStreamSynchronize(d.stream));
     pd->dparm[DPARM_SOLV_TIME] = now_s() - t0;
@@ -1236,19 +1294,19 @@ extern "C" int pastix_subtask_applyorder(pastix_data_t *pd, pastix_dir_t dir, pa
     int rc = device_setup(pd);
     if (rc) return rc;
     Device &d = pd->dev;
-    DBuf<double> tmp;
-    CUDA_TRY(tmp.alloc((size_t)m * n));
+    double *tmp = work(d, WS_ORDER, (size_t)m * n);
+    if (!tmp) return PASTIX_ERR_OUTOFMEMORY;
     if (dir == PastixDirForward) {
-        if (!(Bp->b && Bp->allocated && Bp->m == m && Bp->n == n && Bp->flttype == SpmDouble)) {
+        if (!(Bp->b && Bp->m == m && Bp->n == n && Bp->flttype == SpmDouble)) {
             rc = rhs_alloc(Bp, SpmDouble, m, n);
             if (rc) return rc;
         }
-        CUDA_TRY(cudaMemcpy2DAsync(tmp.p, m * 8, B, ldb * 8, m * 8, n, cudaMemcpyHostToDevice, d.stream));
-        pgpu::launch_permute<double, double>((int)m, (int)n, d.perm.p, 1, tmp.p, m, (double *)Bp->b, Bp->ld, d.stream);
+        CUDA_TRY(cudaMemcpy2DAsync(tmp, m * 8, B, ldb * 8, m * 8, n, cudaMemcpyHostToDevice, d.stream));
+        pgpu::launch_permute<double, double>((int)m, (int)n, d.perm.p, 1, tmp, m, (double *)Bp->b, Bp->ld, d.stream);
     } else {
         if (!Bp->b || Bp->flttype != SpmDouble) return PASTIX_ERR_BADPARAMETER;
-        pgpu::launch_permute<double, double>((int)m, (int)n, d.perm.p, 0, (const double *)Bp->b, Bp->ld, tmp.p, m, d.stream);
-        CUDA_TRY(cudaMemcpy2DAsync(B, ldb * 8, tmp.p, m * 8, m * 8, n, cudaMemcpyDeviceToHost, d.stream));
+        pgpu::launch_permute<double, double>((int)m, (int)n, d.perm.p, 0, (const double *)Bp->b, Bp->ld, tmp, m, d.stream);
+        CUDA_TRY(cudaMemcpy2DAsync(B, ldb * 8, tmp, m * 8, m * 8, n, cudaMemcpyDeviceToHost, d.stream));
     }
     CUDA_TRY(cudaStreamSynchronize(d.stream));
     return PASTIX_SUCCESS;
@@ -1276,11 +1334,16 @@ extern "C" int pastix_subtask_trsm(pastix_data_t *pd, pastix_side_t side, pastix
         using T = std::remove_pointer_t<decltype(Y)>;
         const T *L = reinterpret_cast<const T *>(d.Lc.p);
         const T *U = reinterpret_cast<const T *>(d.Uc.p);
-        if (uplo == PastixLower && trans == PastixNoTrans) sweep_forward<T>(pd, L, unit, Y, (int)b->ld, (int)b->n);
-        else if (uplo == PastixLower) sweep_backward<T>(pd, L, unit, Y, (int)b->ld, (int)b->n);
+        // inverted diagonal sub-blocks: LU keeps U^{-1} (set 0) and L^{-T} (set 1);
+        // LL^T / LDL^T keep one set (LDL^T folds D into it)
+        const int sy = fk == pgpu::FACT_SYTRF;
+        if (uplo == PastixLower && trans == PastixNoTrans)
+            sweep_forward<T>(pd, L, unit, fk == pgpu::FACT_GETRF ? 1 : 0, sy, Y, (int)b->ld, (int)b->n);
+        else if (uplo == PastixLower)
+            sweep_backward<T>(pd, L, unit, fk == pgpu::FACT_GETRF ? 1 : 0, sy, Y, (int)b->ld, (int)b->n);
         else if (uplo == PastixUpper && trans == PastixNoTrans)
-            sweep_backward<T>(pd, fk == pgpu::FACT_GETRF ? U : L, unit, Y, (int)b->ld, (int)b->n);
-        else sweep_forward<T>(pd, fk == pgpu::FACT_GETRF ? U : L, unit, Y, (int)b->ld, (int)b->n);
+            sweep_backward<T>(pd, fk == pgpu::FACT_GETRF ? U : L, unit, 0, sy, Y, (int)b->ld, (int)b->n);
+        else sweep_forward<T>(pd, fk == pgpu::FACT_GETRF ? U : L, unit, 0, sy, Y, (int)b->ld, (int)b->n);
     };
     if (isd) run((double *)b->b);
     else run((float *)b->b);
@@ -1359,11 +1422,10 @@ struct Refiner {
 static int refine_gmres(Refiner &R, double *x, const double *b, double eps, int itermax, int im, int &iters_out) {
     const int64_t n = R.n;
     const int im1 = im + 1;
-    DBuf<double> V, W;
-    if (V.alloc((size_t)n * im1) || W.alloc((size_t)n * im)) return PASTIX_ERR_OUTOFMEMORY;
+    struct { double *p; } V{work(R.d, WS_GMV, (size_t)n * im1)}, W{work(R.d, WS_GMW, (size_t)n * im)},
+        gdev{work(R.d, WS_GMG, im1)};
+    if (!V.p || !W.p || !gdev.p) return PASTIX_ERR_OUTOFMEMORY;
     std::vector<double> H((size_t)im * im1, 0.0), gcos(im), gsin(im), G(im1);
-    DBuf<double> gdev;
-    if (gdev.alloc(im1)) return PASTIX_ERR_OUTOFMEMORY;
     double normb = R.norm(b);
     if (normb == 0.) normb = 1;
     double normx = R.norm(x);
@@ -1435,17 +1497,22 @@ static int refine_gmres(Refiner &R, double *x, const double *b, double eps, int 
 // preconditioned CG (refinement/z_refine_grad.c:49-175)
 static int refine_cg(Refiner &R, double *x, const double *b, double eps, int itermax, int &iters_out) {
     const int64_t n = R.n;
-    DBuf<double> r, p, z, q;
-    if (r.alloc(n) || p.alloc(n) || z.alloc(n) || q.alloc(n)) return PASTIX_ERR_OUTOFMEMORY;
+    double *wv = work(R.d, WS_VEC, (size_t)n * 4);
+    if (!wv) return PASTIX_ERR_OUTOFMEMORY;
+    struct { double *p; } r{wv}, p{wv + n}, z{wv + 2 * n}, q{wv + 3 * n};
     double normb = R.norm(b);
     if (normb == 0.) normb = 1;
     double normx = R.norm(x);
     R.copy(b, r.p);
     if (normx > 0.) R.spmv(-1., x, 1., r.p);
     double resid_b = R.norm(r.p) / normb;
-    R.copy(r.p, z.p);
-    if (R.spsv(z.p)) return PASTIX_ERR_INTERNAL;
-    R.copy(z.p, p.p);
+    // z = M^{-1} r is only needed when the loop runs; the residual test is
+    // taken before the preconditioner solve (same iterates as the reference)
+    if (resid_b > eps && itermax > 0) {
+        R.copy(r.p, z.p);
+        if (R.spsv(z.p)) return PASTIX_ERR_INTERNAL;
+        R.copy(z.p, p.p);
+    }
     int it = 0;
     while (resid_b > eps && it < itermax) {
         it++;
@@ -1454,12 +1521,13 @@ static int refine_cg(Refiner &R, double *x, const double *b, double eps, int ite
         double alpha = beta / R.dot(q.p, p.p);
         R.axpy(alpha, p.p, x);
         R.axpy(-alpha, q.p, r.p);
+        resid_b = R.norm(r.p) / normb;
+        if (resid_b <= eps || it >= itermax) break;
         R.copy(r.p, z.p);
         if (R.spsv(z.p)) return PASTIX_ERR_INTERNAL;
         double rz = R.dot(r.p, z.p);
         beta = rz / beta;
         pgpu::launch_xpby(n, z.p, beta, p.p, R.d.stream);  // p = z + beta p
-        resid_b = R.norm(r.p) / normb;
     }
     iters_out = it;
     return PASTIX_SUCCESS;
@@ -1468,10 +1536,10 @@ static int refine_cg(Refiner &R, double *x, const double *b, double eps, int ite
 // preconditioned BiCGStab (refinement/z_refine_bicgstab.c:49-228)
 static int refine_bicgstab(Refiner &R, double *x, const double *b, double eps, int itermax, int &iters_out) {
     const int64_t n = R.n;
-    DBuf<double> r, r2, p, y, v, s, z, t, t2;
-    if (r.alloc(n) || r2.alloc(n) || p.alloc(n) || y.alloc(n) || v.alloc(n) || s.alloc(n) || z.alloc(n) ||
-        t.alloc(n) || t2.alloc(n))
-        return PASTIX_ERR_OUTOFMEMORY;
+    double *wv = work(R.d, WS_VEC, (size_t)n * 9);
+    if (!wv) return PASTIX_ERR_OUTOFMEMORY;
+    struct { double *p; } r{wv}, r2{wv + n}, p{wv + 2 * n}, y{wv + 3 * n}, v{wv + 4 * n}, s{wv + 5 * n},
+        z{wv + 6 * n}, t{wv + 7 * n}, t2{wv + 8 * n};
     double normb = R.norm(b);
     if (normb == 0.) normb = 1;
     double normx = R.norm(x);
@@ -1516,8 +1584,9 @@ static int refine_bicgstab(Refiner &R, double *x, const double *b, double eps, i
 static int refine_sr(Refiner &R, double *x, const double *b, double eps, int itermax, int &iters_out) {
     const int64_t n = R.n;
     if (!R.precond) return PASTIX_ERR_BADPARAMETER;
-    DBuf<double> r, dx;
-    if (r.alloc(n) || dx.alloc(n)) return PASTIX_ERR_OUTOFMEMORY;
+    double *wv = work(R.d, WS_VEC, (size_t)n * 2);
+    if (!wv) return PASTIX_ERR_OUTOFMEMORY;
+    struct { double *p; } r{wv}, dx{wv + n};
     double normb = R.norm(b);
     if (normb == 0.) normb = 1;
     int it = 0;
@@ -1578,15 +1647,20 @@ extern "C" int pastix_task_refine(pastix_data_t *pd, pastix_int_t n, pastix_int_
         return PASTIX_ERR_BADPARAMETER;
     }
     if (n != pd->n || nrhs < 1 || ldb < n || ldx < n || !B || !X) return PASTIX_ERR_BADPARAMETER;
-    pastix_rhs_t Bp, Xp;
-    pastixRhsInit(&Bp);
-    pastixRhsInit(&Xp);
-    int rc = pastix_subtask_applyorder(pd, PastixDirForward, n, nrhs, B, ldb, Bp);
-    if (!rc) rc = pastix_subtask_applyorder(pd, PastixDirForward, n, nrhs, X, ldx, Xp);
-    if (!rc) rc = pastix_subtask_refine(pd, Bp, Xp);
-    if (!rc) rc = pastix_subtask_applyorder(pd, PastixDirBackward, n, nrhs, X, ldx, Xp);
-    pastixRhsFinalize(Bp);
-    pastixRhsFinalize(Xp);
+    int rc = device_setup(pd);
+    if (rc) return rc;
+    struct pastix_rhs_s Bs{}, Xs{};  // permuted copies in the library's work areas
+    Bs.flttype = Xs.flttype = SpmDouble;
+    Bs.m = Xs.m = n;
+    Bs.n = Xs.n = nrhs;
+    Bs.ld = Xs.ld = n;
+    Bs.b = work(pd->dev, WS_RB, (size_t)n * nrhs);
+    Xs.b = work(pd->dev, WS_RX, (size_t)n * nrhs);
+    if (!Bs.b || !Xs.b) return PASTIX_ERR_OUTOFMEMORY;
+    rc = pastix_subtask_applyorder(pd, PastixDirForward, n, nrhs, B, ldb, &Bs);
+    if (!rc) rc = pastix_subtask_applyorder(pd, PastixDirForward, n, nrhs, X, ldx, &Xs);
+    if (!rc) rc = pastix_subtask_refine(pd, &Bs, &Xs);
+    if (!rc) rc = pastix_subtask_applyorder(pd, PastixDirBackward, n, nrhs, X, ldx, &Xs);
     return rc;
 }
 
@@ -1711,9 +1785,8 @@ extern "C" int pgpu_solve_refine_device(pastix_data_t *pd, pastix_int_t nrhs, co
     Device &d = pd->dev;
     CUDA_TRY(cudaSetDevice(d.dev));
     const idx_t n = pd->n;
-    DBuf<double> bp, xp;
-    CUDA_TRY(bp.alloc((size_t)n * nrhs));
-    CUDA_TRY(xp.alloc((size_t)n * nrhs));
+    struct { double *p; } bp{work(d, WS_BP, (size_t)n * nrhs)}, xp{work(d, WS_XP, (size_t)n * nrhs)};
+    if (!bp.p || !xp.p) return PASTIX_ERR_OUTOFMEMORY;
     launch_cls(pd, PC_VEC, 1, [&] { pgpu::launch_permute<double, double>((int)n, (int)nrhs, d.perm.p, 1, B, ldb, bp.p, n, d.stream); });
     CUDA_TRY(cudaMemcpyAsync(xp.p, bp.p, (size_t)n * nrhs * 8, cudaMemcpyDeviceToDevice, d.stream));
     rc = solve_perm_d(pd, 0, xp.p, (int)n, (int)nrhs);

@@ -31,6 +31,10 @@ struct UpdTile {
 // tile and a 32-row strip of the triangular factor, 2 x 32 x (nc + 1) elements.
 __host__ __device__ inline int trsm_tile_rows(int) { return 32; }
 __host__ __device__ inline long long trsm_smem_elems(int nc) { return 2LL * 32 * (nc + 1); }
+// Elements of the inverted diagonal sub-blocks kept for a wide cblk of width nc.
+__host__ __device__ inline long long dinv_elems(int nc, int fact) {
+    return (long long)((nc + 31) / 32) * 1024 * (fact == FACT_GETRF ? 2 : 1);
+}
 
 // Shared memory of k_diag_large for a cblk of width nc: the nc x 32 column
 // panel (ld 33) and, for GETRF, the 32 x nc strip of U (ld nc + 1).
@@ -50,6 +54,7 @@ struct DevStruct {
     const int *cb_fcol, *cb_lcol, *cb_stride, *cb_fblok;
     const int64_t *cb_coef;     // panel offset (elements) of each cblk
     const int64_t *cb_rowidx;   // offset of each cblk in rowidx
+    const int64_t *cb_dinv;     // offset of each wide cblk's inverted 32x32 diagonal sub-blocks (-1: none)
     const int *bk_frow, *bk_lrow, *bk_rowoff, *bk_fcblk;
     const int *rowidx;          // global row of every panel row
     const TaskDev *tasks;

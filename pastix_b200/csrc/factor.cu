@@ -143,22 +143,53 @@ __global__ void __launch_bounds__(256) k_panel_small(DevStruct s, const int *__r
 }
 
 // ---------------------------------------------------------------------------
-// Wide cblks, diagonal block: blocked right-looking factorization by column
-// panels of DNB = 32 columns held row-major in shared memory.  Per panel:
-//   1. warp 0 factors the 32 x 32 top block column by column (pivot, scale,
-//      rank-1 update), as potf2 / getf2 / sytf2;
-//   2. the panel rows below are solved against that block, one warp per row,
-//      block columns on the lanes (the TRSM of the blocked algorithm);
-//   3. the trailing part of the diagonal block is updated from shared memory
-//      with 4 x 4 register tiles (SYRK / GEMM of the blocked algorithm).
-// GETRF keeps the 32-row strip of U to the right of the panel in shared
-// memory as well (its rows are solved with the unit lower factor).
+// Wide cblks.  The diagonal block is factored by column panels of DNB = 32;
+// for every 32 x 32 diagonal sub-block jj the inverse Z_jj of its upper
+// triangular factor T_jj is formed and kept (device scratch `dinv`, one or two
+// 32 x 32 blocks per sub-block), so that the off-diagonal TRSM X T = A becomes
+// a blocked sequence of GEMMs: X_j = A_j Z_jj, A_{>j} -= X_j T_{j,>j} (the
+// inverted-diagonal-block TRSM used by GPU BLAS libraries).  T per kind:
+//   POTRF  T = L_kk^T           SYTRF  T = D_kk L_kk^T
+//   GETRF  side 0: T = U_kk      side 1: T = L_kk^T (unit)
 // ---------------------------------------------------------------------------
 constexpr int DNB = 32;
 constexpr int DLDW = DNB + 1;
 
+// T_jj(i, k) of the 32 x 32 sub-block whose factored rows are in Wb (row major, ld DLDW)
 template <typename T, int FACT>
-__global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__restrict__ list, T *L, T *U,
+__device__ __forceinline__ T tblk(const T *Wb, int i, int k, int side) {
+    if (k < i) return T(0);
+    if (FACT == FACT_POTRF) return Wb[k * DLDW + i];
+    if (FACT == FACT_SYTRF) return (k == i) ? Wb[i * DLDW + i] : Wb[i * DLDW + i] * Wb[k * DLDW + i];
+    if (side == 0) return Wb[i * DLDW + k];
+    return (k == i) ? T(1) : Wb[k * DLDW + i];
+}
+
+// Warp: Z = T^{-1} (upper, 32 x 32), lane j forms column j by back substitution.
+// rinv (smem, 32) receives 1 / T(i, i).  nb <= 32 valid rows/cols; the rest is identity.
+template <typename T, int FACT>
+__device__ __forceinline__ void warp_upper_inverse(const T *Wb, int nb, int side, T *rinv, T *Z, int ldz, T *gZ) {
+    const int lane = threadIdx.x & 31;
+    rinv[lane] = (lane < nb) ? T(1) / tblk<T, FACT>(Wb, lane, lane, side) : T(1);
+    __syncwarp();
+    T z[32];
+#pragma unroll
+    for (int i = 31; i >= 0; i--) {
+        T acc = T(0);
+#pragma unroll
+        for (int k = i + 1; k < 32; k++)
+            if (k < nb && i < nb) acc += tblk<T, FACT>(Wb, i, k, side) * z[k];
+        z[i] = (i > lane) ? T(0) : ((i == lane) ? rinv[i] : -acc * rinv[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+        Z[i * ldz + lane] = z[i];
+        if (gZ) gZ[i * 32 + lane] = z[i];
+    }
+}
+
+template <typename T, int FACT>
+__global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__restrict__ list, T *L, T *U, T *dinv,
                                                      FactParams fp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int k = list[blockIdx.x];
@@ -167,8 +198,12 @@ __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__re
     T *W = reinterpret_cast<T *>(smem_raw);  // m x DNB panel, row major, ld DLDW
     T *R = W + (size_t)nc * DLDW;            // GETRF: DNB x t strip of U, row major, ld nc + 1
     const int ldr = nc + 1;
+    __shared__ T Z0[DNB * DLDW], Z1[DNB * DLDW];
+    __shared__ T rinv[DNB];
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     T *A = L + s.cb_coef[k];
+    T *gZ = dinv + s.cb_dinv[k];
+    const int nzb = (nc + DNB - 1) / DNB;
     __shared__ int npiv;
     __shared__ T dsh[DNB];
     if (tid == 0) npiv = 0;
@@ -194,56 +229,97 @@ __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__re
                 R[c * ldr + q] = A[(jb + c) + (size_t)(jb + nb + q) * st];
             }
         __syncthreads();
-        // 1. the nb x nb top block, by warp 0
         if (warp == 0) {
+            // 1. factor the nb x nb top block in registers, one row per lane
+            T r[32];
+#pragma unroll
+            for (int j = 0; j < 32; j++)
+                r[j] = (lane < nb && j < nb) ? W[lane * DLDW + j] : (lane == j ? T(1) : T(0));
             int np = 0;
-            for (int c = 0; c < nb; c++) {
-                T d = static_pivot<T, FACT>(W[c * DLDW + c], fp.criterion, np);
-                __syncwarp();
-                if (lane == c) W[c * DLDW + c] = d;
-                const T inv = T(1) / d;
-                if (lane > c && lane < nb) {
-                    if (FACT == FACT_SYTRF) W[c * DLDW + lane] = W[lane * DLDW + c];  // D L^T copy
-                    W[lane * DLDW + c] *= inv;
-                }
-                __syncwarp();
-                if (lane > c && lane < nb) {
-                    const T lic = W[lane * DLDW + c];
-                    for (int j = c + 1; j < nb; j++) {
-                        if (FACT == FACT_POTRF) {
-                            if (lane >= j) W[lane * DLDW + j] -= lic * W[j * DLDW + c];
-                        } else if (FACT == FACT_SYTRF) {
-                            if (lane >= j) W[lane * DLDW + j] -= lic * W[c * DLDW + j];
-                        } else {
-                            W[lane * DLDW + j] -= lic * W[c * DLDW + j];
+#pragma unroll
+            for (int c = 0; c < 32; c++) {
+                if (c < nb) {
+                    const T d = static_pivot<T, FACT>(__shfl_sync(0xffffffffu, r[c], c), fp.criterion, np);
+                    const T inv = T(1) / d;
+                    const T u = r[c];
+                    if (lane == c) r[c] = d;
+                    else if (lane > c) r[c] *= inv;
+#pragma unroll
+                    for (int j = c + 1; j < 32; j++) {
+                        if (j < nb) {
+                            if (FACT == FACT_POTRF) {
+                                const T ljc = __shfl_sync(0xffffffffu, r[c], j);
+                                if (lane >= j) r[j] -= r[c] * ljc;
+                            } else if (FACT == FACT_SYTRF) {
+                                const T ujc = __shfl_sync(0xffffffffu, u, j);
+                                if (lane >= j) r[j] -= r[c] * ujc;
+                            } else {
+                                const T ucj = __shfl_sync(0xffffffffu, r[j], c);
+                                if (lane > c) r[j] -= r[c] * ucj;
+                            }
                         }
                     }
                 }
-                __syncwarp();
             }
+            if (lane < nb)
+#pragma unroll
+                for (int j = 0; j < 32; j++)
+                    if (j < nb) W[lane * DLDW + j] = r[j];
             if (lane == 0 && np) npiv += np;
+            __syncwarp();
+            // 2. inverse of the triangular factor of the block (and of L^T for GETRF's U side)
+            warp_upper_inverse<T, FACT>(W, nb, 0, rinv, Z0, DLDW, gZ + (size_t)(jb / DNB) * 1024);
+            if (FACT == FACT_GETRF) {
+                __syncwarp();
+                warp_upper_inverse<T, FACT>(W, nb, 1, rinv, Z1, DLDW, gZ + (size_t)(nzb + jb / DNB) * 1024);
+            }
         }
         __syncthreads();
         if (FACT == FACT_SYTRF && tid < nb) dsh[tid] = W[tid * DLDW + tid];
-        // 2. panel rows below the block: x T = a, lanes = block columns
-        for (int r = nb + warp; r < m; r += nt / 32) {
-            T x = (lane < nb) ? W[r * DLDW + lane] : T(0);
-            for (int c = 0; c < nb; c++) {
-                if (lane == c) x /= W[c * DLDW + c];
-                T xc = __shfl_sync(0xffffffffu, x, c);
-                if (lane > c && lane < nb) {
-                    T tcl = (FACT == FACT_POTRF) ? W[lane * DLDW + c] : W[c * DLDW + lane];
-                    x -= xc * tcl;
+        // 3. panel rows below the block, X T_jj = A by substitution: one row per
+        //    thread held in registers, T_jj (staged in Z1 unless GETRF) and the
+        //    reciprocals of its diagonal in shared memory
+        if (FACT != FACT_GETRF) {
+            for (int e = tid; e < 1024; e += nt) {
+                int i = e >> 5, j = e & 31;
+                Z1[i * DLDW + j] = (i < nb && j < nb) ? tblk<T, FACT>(W, i, j, 0) : T(0);
+            }
+        }
+        if (tid < 32) rinv[tid] = (tid < nb) ? T(1) / tblk<T, FACT>(W, tid, tid, 0) : T(1);
+        __syncthreads();
+        for (int r = nb + tid; r < m; r += nt) {
+            T x[32];
+#pragma unroll
+            for (int c = 0; c < 32; c++) x[c] = (c < nb) ? W[r * DLDW + c] : T(0);
+#pragma unroll
+            for (int c = 0; c < 32; c++) {
+                x[c] *= rinv[c];
+#pragma unroll
+                for (int j = c + 1; j < 32; j++) {
+                    T tcj;
+                    if (FACT == FACT_GETRF) tcj = (c < nb && j < nb) ? W[c * DLDW + j] : T(0);
+                    else tcj = Z1[c * DLDW + j];
+                    x[j] -= x[c] * tcj;
                 }
             }
-            if (lane < nb) W[r * DLDW + lane] = x;
+#pragma unroll
+            for (int c = 0; c < 32; c++)
+                if (c < nb) W[r * DLDW + c] = x[c];
         }
         if (FACT == FACT_GETRF)  // U12 <- L11^{-1} U12 (unit lower), one column per thread
-            for (int q = tid; q < t; q += nt)
-                for (int c = 0; c < nb; c++) {
-                    const T u = R[c * ldr + q];
-                    for (int j = c + 1; j < nb; j++) R[j * ldr + q] -= W[j * DLDW + c] * u;
-                }
+            for (int q = tid; q < t; q += nt) {
+                T col[32];
+#pragma unroll
+                for (int i = 0; i < 32; i++) col[i] = (i < nb) ? R[i * ldr + q] : T(0);
+#pragma unroll
+                for (int c = 0; c < 32; c++)
+#pragma unroll
+                    for (int i = c + 1; i < 32; i++)
+                        if (i < nb && c < nb) col[i] -= W[i * DLDW + c] * col[c];
+#pragma unroll
+                for (int i = 0; i < 32; i++)
+                    if (i < nb) R[i * ldr + q] = col[i];
+            }
         __syncthreads();
         for (int e = tid; e < m * nb; e += nt) {
             int i = e % m, c = e / m;
@@ -254,7 +330,7 @@ __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__re
                 int c = e % nb, q = e / nb;
                 A[(jb + c) + (size_t)(jb + nb + q) * st] = R[c * ldr + q];
             }
-        // 3. trailing update A22 -= L21 * B^T (4x4 blocks; lower triangle for the symmetric kinds)
+        // 4. trailing update A22 -= L21 * B^T (4x4 blocks; lower triangle for the symmetric kinds)
         if (t > 0) {
             const int nbt = (t + 3) / 4;
             const int nblk = (FACT == FACT_GETRF) ? nbt * nbt : nbt * (nbt + 1) / 2;
@@ -325,19 +401,9 @@ __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__re
     if (tid == 0 && npiv) atomicAdd(fp.nbpivots, npiv);
 }
 
-// ---------------------------------------------------------------------------
-// Wide cblks, off-diagonal TRSM: X T = A for a tile of TRSM_ROWS panel rows,
-// T the upper triangular factor of the diagonal block:
-//   POTRF       T = L_kk^T            (Right, Lower, Trans, NonUnit)
-//   SYTRF       T = D_kk L_kk^T        (Right, Upper, NoTrans, NonUnit on DL^T)
-//   GETRF side0 T = U_kk  (upper of L) (Right, Upper, NoTrans, NonUnit)
-//   GETRF side1 T = L_kk^T (unit)      (Right, Upper, NoTrans, Unit on U panel)
-// blockIdx.y selects the GETRF side.  Blocked by 32 columns (the blocked
-// algorithm of a BLAS TRSM): a 32-wide block is solved by substitution, one
-// warp per 4 rows with the block's columns on the lanes, then the columns to
-// its right are updated by a register-tiled GEMM from shared memory.  The tile
-// of X (row major) and the current 32-row strip of T live in shared memory.
-// ---------------------------------------------------------------------------
+// Off-diagonal TRSM of a wide cblk on a tile of TRSM_ROWS panel rows held
+// row-major in shared memory, blocked by 32 columns with the inverted
+// diagonal sub-blocks from k_diag_large.  blockIdx.y = GETRF side.
 constexpr int TRSM_ROWS = 32;
 constexpr int TRSM_MAXT = 10;  // column chunks of 32 per GEMM pass
 
@@ -352,7 +418,8 @@ __global__ void __launch_bounds__(256) k_trsm(DevStruct s, const RowTile *__rest
     const int rows = min(TRSM_ROWS, st - tl.r0);
     const int ld = nc + 1;
     T *X = reinterpret_cast<T *>(smem_raw);  // TRSM_ROWS x nc, row major, ld
-    T *Ts = X + TRSM_ROWS * ld;              // 32 x (nc - jb) strip of T, row major, ld
+    T *Ts = X + TRSM_ROWS * ld;              // 32 x (nc - jb) strip of T from column jb, row major, ld
+    __shared__ T rinv[32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const T *D = L + s.cb_coef[k];  // diagonal block (ld = st) of the L panel
     T *A = ((FACT == FACT_GETRF && side == 1) ? U : L) + s.cb_coef[k] + tl.r0;
@@ -378,17 +445,23 @@ __global__ void __launch_bounds__(256) k_trsm(DevStruct s, const RowTile *__rest
             Ts[a * ld + q] = t;
         }
         __syncthreads();
-        // substitution on the 32-wide block: warp w owns rows 4w .. 4w+3
+        if (tid < 32) rinv[tid] = (tid < nb && !unit) ? T(1) / Ts[tid * ld + tid] : T(1);
+        __syncthreads();
+        // substitution on the 32-wide block: one tile row per thread of warp 0
+        if (warp == 0) {
+            T x[32];
 #pragma unroll
-        for (int rr = 0; rr < 4; rr++) {
-            const int r = warp * 4 + rr;
-            T x = (lane < nb) ? X[r * ld + jb + lane] : T(0);
-            for (int c = 0; c < nb; c++) {
-                if (!unit && lane == c) x /= Ts[c * ld + c];
-                T xc = __shfl_sync(0xffffffffu, x, c);
-                if (lane > c && lane < nb) x -= xc * Ts[c * ld + lane];
+            for (int c = 0; c < 32; c++) x[c] = (c < nb) ? X[lane * ld + jb + c] : T(0);
+#pragma unroll
+            for (int c = 0; c < 32; c++) {
+                x[c] *= rinv[c];
+#pragma unroll
+                for (int j = c + 1; j < 32; j++)
+                    if (j < nb) x[j] -= x[c] * Ts[c * ld + j];
             }
-            if (lane < nb) X[r * ld + jb + lane] = x;
+#pragma unroll
+            for (int c = 0; c < 32; c++)
+                if (c < nb) X[lane * ld + jb + c] = x[c];
         }
         __syncthreads();
         // X[:, jb+nb:] -= X[:, jb:jb+nb] * Ts[:, nb:]
@@ -549,6 +622,156 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
 }
 
 // ---------------------------------------------------------------------------
+// FP64 update on the tensor cores: the same task/tile semantics as k_update
+// with a 128 x 64 output tile, 16-deep k steps double-buffered in shared
+// memory by cp.async, and DMMA (mma.sync m8n8k4 f64) on 8 warps arranged
+// 4 x 2, each warp owning a 32 x 32 block of 4 x 4 DMMA tiles.  The scatter
+// into the facing panel is the epilogue, as in k_update.
+// ---------------------------------------------------------------------------
+constexpr int DM_BM = 128, DM_BN = 64, DM_BK = 16;
+constexpr int DM_LDA = DM_BM + 8, DM_LDB = DM_BN + 8;  // row strides = 8 mod 16 doubles: 2 wavefronts per fragment load
+constexpr size_t DM_SMEM = sizeof(double) * 2 * DM_BK * (DM_LDA + DM_LDB);
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    int sz = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <int FACT>
+__global__ void __launch_bounds__(256) k_update_dmma(DevStruct s, const UpdTile *__restrict__ tiles, double *L,
+                                                      double *U) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *As = reinterpret_cast<double *>(smem_raw);  // [2][DM_BK][DM_LDA]
+    double *Bs = As + 2 * DM_BK * DM_LDA;               // [2][DM_BK][DM_LDB]
+    __shared__ int rt[DM_BM];
+    __shared__ int ct[DM_BN];
+    __shared__ double dsc[2][DM_BK];
+
+    const UpdTile tl = tiles[blockIdx.x];
+    const TaskDev tk = s.tasks[tl.task];
+    const int k = tk.src, f = tk.dst;
+    const int K = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+    const int st = s.cb_stride[k];
+    const int shift = tl.side ? tk.n : 0;
+    const int M = tk.m - shift;
+    const int arow = tk.row0 + shift + tl.mt * DM_BM;
+    const int brow = tk.row0 + tl.nt * DM_BN;
+    const int mrows = min(DM_BM, M - tl.mt * DM_BM);
+    const int ncols = min(DM_BN, tk.n - tl.nt * DM_BN);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const double *Ap = ((FACT == FACT_GETRF && tl.side == 1) ? U : L) + s.cb_coef[k];
+    const double *Bp = ((FACT == FACT_GETRF && tl.side == 0) ? U : L) + s.cb_coef[k];
+    const double *Dk = L + s.cb_coef[k];
+    double *Cp = ((FACT == FACT_GETRF && tl.side == 1) ? U : L) + s.cb_coef[f];
+    const int stf = s.cb_stride[f];
+
+    const int *ridx = s.rowidx + s.cb_rowidx[k];
+    if (tid < DM_BM) {
+        int r = -1;
+        if (tid < mrows) {
+            int g = ridx[arow + tid];
+            int lo = s.cb_fblok[f], hi = s.cb_fblok[f + 1] - 1;
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (s.bk_frow[mid] <= g) lo = mid; else hi = mid - 1;
+            }
+            r = s.bk_rowoff[lo] + (g - s.bk_frow[lo]);
+        }
+        rt[tid] = r;
+    }
+    if (tid < DM_BN) ct[tid] = (tid < ncols) ? (ridx[brow + tid] - s.cb_fcol[f]) : -1;
+
+    auto load_stage = [&](int buf, int k0) {
+        double *as = As + buf * DM_BK * DM_LDA;
+        double *bs = Bs + buf * DM_BK * DM_LDB;
+#pragma unroll
+        for (int q = 0; q < (DM_BK * DM_BM) / 256; q++) {
+            int e = tid + q * 256;
+            int kk = e / DM_BM, r = e % DM_BM;
+            bool v = (r < mrows) && (k0 + kk < K);
+            const double *src = v ? Ap + (arow + r) + (size_t)(k0 + kk) * st : Ap;
+            cp_async8(as + kk * DM_LDA + r, src, v);
+        }
+#pragma unroll
+        for (int q = 0; q < (DM_BK * DM_BN) / 256; q++) {
+            int e = tid + q * 256;
+            int kk = e / DM_BN, c = e % DM_BN;
+            bool v = (c < ncols) && (k0 + kk < K);
+            const double *src = v ? Bp + (brow + c) + (size_t)(k0 + kk) * st : Bp;
+            cp_async8(bs + kk * DM_LDB + c, src, v);
+        }
+        if (FACT == FACT_SYTRF && tid < DM_BK)
+            dsc[buf][tid] = (k0 + tid < K) ? Dk[(k0 + tid) + (size_t)(k0 + tid) * st] : 0.0;
+        cp_async_commit();
+    };
+
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
+    const int g = lane >> 2, q4 = lane & 3;
+    const int nk = (K + DM_BK - 1) / DM_BK;
+    load_stage(0, 0);
+    for (int kt = 0; kt < nk; kt++) {
+        if (kt + 1 < nk) {
+            load_stage((kt + 1) & 1, (kt + 1) * DM_BK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double *as = As + (kt & 1) * DM_BK * DM_LDA;
+        const double *bs = Bs + (kt & 1) * DM_BK * DM_LDB;
+#pragma unroll
+        for (int kk = 0; kk < DM_BK; kk += 4) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) a[i] = as[(kk + q4) * DM_LDA + wm + i * 8 + g];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                b[j] = bs[(kk + q4) * DM_LDB + wn + j * 8 + g];
+                if (FACT == FACT_SYTRF) b[j] *= dsc[kt & 1][kk + q4];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) dmma884(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int r = wm + i * 8 + g;
+        const int rr = rt[r];
+        if (rr < 0) continue;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int cc = ct[wn + j * 8 + q4 * 2 + h];
+                if (cc < 0) continue;
+                double *dst = Cp + rr + (size_t)cc * stf;
+                if (tk.excl) *dst -= acc[i][j][h];
+                else atomicAdd(dst, -acc[i][j][h]);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Host launch wrappers (called from the driver with level lists in device memory)
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -567,14 +790,15 @@ void launch_panel_small(const DevStruct &s, const int *list, int count, size_t s
 }
 
 template <typename T, int FACT>
-void launch_diag_large(const DevStruct &s, const int *list, int count, size_t smem, T *L, T *U,
+void launch_diag_large(const DevStruct &s, const int *list, int count, size_t smem, T *L, T *U, T *dinv,
                        const FactParams &fp, cudaStream_t st) {
     if (count <= 0) return;
-    k_diag_large<T, FACT><<<count, 256, smem, st>>>(s, list, L, U, fp);
+    k_diag_large<T, FACT><<<count, 256, smem, st>>>(s, list, L, U, dinv, fp);
 }
 
 template <typename T, int FACT>
-void launch_trsm(const DevStruct &s, const RowTile *tiles, int count, size_t smem, T *L, T *U, cudaStream_t st) {
+void launch_trsm(const DevStruct &s, const RowTile *tiles, int count, size_t smem, T *L, T *U, const T *,
+                 cudaStream_t st) {
     if (count <= 0) return;
     dim3 grid(count, FACT == FACT_GETRF ? 2 : 1);
     k_trsm<T, FACT><<<grid, 256, smem, st>>>(s, tiles, L, U);
@@ -586,23 +810,52 @@ void launch_update(const DevStruct &s, const UpdTile *tiles, int count, T *L, T 
     k_update<T, FACT, 64, 64, 16, 4, 4><<<count, 256, 0, st>>>(s, tiles, L, U);
 }
 
+// big tiles (128 x 64): DMMA for FP64, SIMT 8 x 4 per thread for FP32
 template <typename T, int FACT>
-cudaError_t set_smem_attrs(size_t small_max, size_t diag_max, size_t trsm_max) {
+void launch_update_big(const DevStruct &s, const UpdTile *tiles, int count, T *L, T *U, cudaStream_t st) {
+    if (count <= 0) return;
+    if constexpr (sizeof(T) == 8)
+        k_update_dmma<FACT><<<count, 256, DM_SMEM, st>>>(s, tiles, L, U);
+    else
+        k_update<T, FACT, 128, 64, 16, 8, 4><<<count, 256, 0, st>>>(s, tiles, L, U);
+}
+
+// Opt every kernel with dynamic shared memory into the largest size the
+// device allows next to its static shared memory.
+template <typename K>
+static cudaError_t opt_in_smem(K kernel) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
+template <typename T, int FACT>
+cudaError_t set_smem_attrs(size_t, size_t, size_t) {
     cudaError_t e;
-    e = cudaFuncSetAttribute(k_panel_small<T, FACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_max);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_diag_large<T, FACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_max);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_trsm<T, FACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_max);
+    if ((e = opt_in_smem(k_panel_small<T, FACT>)) != cudaSuccess) return e;
+    if ((e = opt_in_smem(k_diag_large<T, FACT>)) != cudaSuccess) return e;
+    if ((e = opt_in_smem(k_trsm<T, FACT>)) != cudaSuccess) return e;
+    if constexpr (sizeof(T) == 8) {
+        if ((e = opt_in_smem(k_update_dmma<FACT>)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 #define PGPU_INST_FACT(T, F)                                                                                     \
     template void launch_panel_small<T, F>(const DevStruct &, const int *, int, size_t, T *, T *,                \
                                            const FactParams &, cudaStream_t);                                    \
-    template void launch_diag_large<T, F>(const DevStruct &, const int *, int, size_t, T *, T *,                 \
+    template void launch_diag_large<T, F>(const DevStruct &, const int *, int, size_t, T *, T *, T *,            \
                                           const FactParams &, cudaStream_t);                                     \
-    template void launch_trsm<T, F>(const DevStruct &, const RowTile *, int, size_t, T *, T *, cudaStream_t);     \
+    template void launch_trsm<T, F>(const DevStruct &, const RowTile *, int, size_t, T *, T *, const T *,        \
+                                    cudaStream_t);                                                               \
     template void launch_update<T, F>(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);          \
+    template void launch_update_big<T, F>(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);      \
     template cudaError_t set_smem_attrs<T, F>(size_t, size_t, size_t);
 
 PGPU_INST_FACT(double, FACT_POTRF)

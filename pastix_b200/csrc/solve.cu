@@ -1,29 +1,33 @@
 // Supernodal triangular solve kernels (sm_100a).
 //
 // The right-hand sides live on the device in the permuted numbering, column
-// major with leading dimension n.  A solve with a block-lower panel P (the L
+// major with leading dimension ldy.  A solve with a block-lower panel P (the L
 // panel, or the U^T panel of an LU factor) is, level by level:
-//   forward   y_k <- P_kk^{-1} y_k;  y[rows(k)] -= P_off(k) y_k       (k_fwd_diag, k_fwd_update)
-//   backward  x_k <- P_kk^{-T} (x_k - P_off(k)^T x[rows(k)])            (k_bwd_update, k_bwd_diag)
+//   forward   y_k <- P_kk^{-1} y_k;  y[rows(k)] -= P_off(k) y_k       (diag kernels, k_fwd_update)
+//   backward  x_k <- P_kk^{-T} (x_k - P_off(k)^T x[rows(k)])            (k_bwd_update, diag kernels)
 // which restates solve_cblk_ztrsmsp_forward / _backward
 // (kernels/solve_ztrsmsp.c:302, :468) and solve_blok_ztrsm / _zgemm (:76, :160)
 // with the step table of pastix_subtask_solve_adv (sopalin/pastix_task_solve.c:543-649):
 //   POTRF  L (non-unit) then L^T;  SYTRF  L (unit), D, L^T (unit);
 //   GETRF  L (unit) then U through the stored U^T panel (non-unit).
-// Independent cblks of one level run in one launch; the scatter of the
-// forward update uses atomics because several cblks of a level can face the
-// same rows.
+// Independent cblks of one level run in one launch.  The off-diagonal
+// products use 64 x 64 tiles of the panel (rows x columns) so that a level's
+// wide cblks spread over many CTAs; partial sums go to the right-hand sides by
+// atomics.  Diagonal blocks of wide cblks are applied with the inverted 32 x 32
+// sub-blocks kept by the factorization (a blocked triangular solve whose
+// diagonal steps are small matrix-vector products); narrow cblks use
+// substitution by one warp per right-hand side.
 #include "device.cuh"
 
 namespace pgpu {
 
-constexpr int RC = 8;      // right-hand sides per CTA (gridDim.y covers nrhs)
-constexpr int SROWS = 128; // panel rows per update tile (one per thread)
+constexpr int ST_R = 64, ST_C = 64;  // solve update tile: panel rows x panel columns
 
-// Forward diagonal solve: y_k <- P_kk^{-1} y_k (lower, unit or not).  One CTA
-// per cblk; blocks of 32 columns are solved by warp 0 with shuffles, the rest
-// of the block column is updated by all threads.
-template <typename T>
+// ---------------------------------------------------------------------------
+// Narrow cblks: substitution, blocks of 32 rows on the lanes of a warp, one
+// warp per right-hand side.
+// ---------------------------------------------------------------------------
+template <typename T, int RC>
 __global__ void __launch_bounds__(256) k_fwd_diag(DevStruct s, const int *__restrict__ list, const T *P, int unit,
                                                    T *Y, int ldy, int nrhs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -43,12 +47,13 @@ __global__ void __launch_bounds__(256) k_fwd_diag(DevStruct s, const int *__rest
     __syncthreads();
     for (int jb = 0; jb < nc; jb += 32) {
         const int nb = min(32, nc - jb);
-        if (tid < 32) {
-            const int lane = tid;
-            for (int j = 0; j < nr; j++) {
+        {
+            const int lane = tid & 31, warp = tid >> 5;
+            const T rd = (!unit && lane < nb) ? T(1) / D[(jb + lane) + (size_t)(jb + lane) * st] : T(1);
+            for (int j = warp; j < nr; j += nt / 32) {
                 T v = (lane < nb) ? y[jb + lane + j * nc] : T(0);
                 for (int c = 0; c < nb; c++) {
-                    if (lane == c && !unit) v /= D[(jb + c) + (size_t)(jb + c) * st];
+                    if (lane == c) v *= rd;
                     T vc = __shfl_sync(0xffffffffu, v, c);
                     if (lane > c && lane < nb) v -= D[(jb + lane) + (size_t)(jb + c) * st] * vc;
                 }
@@ -70,88 +75,7 @@ __global__ void __launch_bounds__(256) k_fwd_diag(DevStruct s, const int *__rest
     }
 }
 
-// Forward update: y[row(r)] -= sum_c P[r, c] y_k[c] for the off-diagonal rows
-// of a row tile (one thread per row).
-template <typename T>
-__global__ void __launch_bounds__(SROWS) k_fwd_update(DevStruct s, const RowTile *__restrict__ tiles, const T *P,
-                                                       T *Y, int ldy, int nrhs) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *yk = reinterpret_cast<T *>(smem_raw);  // nc x RC
-    const RowTile tl = tiles[blockIdx.x];
-    const int k = tl.cblk;
-    const int fc = s.cb_fcol[k];
-    const int nc = s.cb_lcol[k] - fc + 1;
-    const int st = s.cb_stride[k];
-    const int j0 = blockIdx.y * RC;
-    const int nr = min(RC, nrhs - j0);
-    const int tid = threadIdx.x;
-    for (int e = tid; e < nc * nr; e += blockDim.x) {
-        int i = e % nc, j = e / nc;
-        yk[i + j * nc] = Y[(fc + i) + (size_t)(j0 + j) * ldy];
-    }
-    __syncthreads();
-    const int r = tl.r0 + tid;
-    if (r >= st || tid >= SROWS) return;
-    const T *Pr = P + s.cb_coef[k] + r;
-    T acc[RC];
-#pragma unroll
-    for (int j = 0; j < RC; j++) acc[j] = T(0);
-    for (int c = 0; c < nc; c++) {
-        T p = Pr[(size_t)c * st];
-#pragma unroll
-        for (int j = 0; j < RC; j++) acc[j] += p * yk[c + j * nc];
-    }
-    const int g = s.rowidx[s.cb_rowidx[k] + r];
-#pragma unroll
-    for (int j = 0; j < RC; j++)
-        if (j < nr) atomicAdd(&Y[g + (size_t)(j0 + j) * ldy], -acc[j]);
-}
-
-// Backward update: x_k[c] -= sum_r P[r, c] x[row(r)] over a row tile; warps
-// reduce over rows, one shared accumulator per (column, rhs).
-template <typename T>
-__global__ void __launch_bounds__(SROWS) k_bwd_update(DevStruct s, const RowTile *__restrict__ tiles, const T *P,
-                                                       T *Y, int ldy, int nrhs) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *xr = reinterpret_cast<T *>(smem_raw);  // SROWS x RC gathered x[row(r)]
-    const RowTile tl = tiles[blockIdx.x];
-    const int k = tl.cblk;
-    const int fc = s.cb_fcol[k];
-    const int nc = s.cb_lcol[k] - fc + 1;
-    const int st = s.cb_stride[k];
-    const int j0 = blockIdx.y * RC;
-    const int nr = min(RC, nrhs - j0);
-    const int tid = threadIdx.x;
-    const int rows = min(SROWS, st - tl.r0);
-    const int *ridx = s.rowidx + s.cb_rowidx[k] + tl.r0;
-    for (int e = tid; e < SROWS * RC; e += blockDim.x) {
-        int i = e % SROWS, j = e / SROWS;
-        xr[e] = (i < rows && j < nr) ? Y[ridx[i] + (size_t)(j0 + j) * ldy] : T(0);
-    }
-    __syncthreads();
-    const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    const T *Pk = P + s.cb_coef[k] + tl.r0;
-    // each warp owns columns c = warp, warp+nw, ...; lanes stride over rows
-    for (int c = warp; c < nc; c += nw) {
-        T acc[RC];
-#pragma unroll
-        for (int j = 0; j < RC; j++) acc[j] = T(0);
-        for (int i = lane; i < rows; i += 32) {
-            T p = Pk[i + (size_t)c * st];
-#pragma unroll
-            for (int j = 0; j < RC; j++) acc[j] += p * xr[i + j * SROWS];
-        }
-#pragma unroll
-        for (int j = 0; j < RC; j++) {
-            T v = acc[j];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0 && j < nr) atomicAdd(&Y[(fc + c) + (size_t)(j0 + j) * ldy], -v);
-        }
-    }
-}
-
-// Backward diagonal solve: x_k <- P_kk^{-T} x_k (P_kk lower; unit or not).
-template <typename T>
+template <typename T, int RC>
 __global__ void __launch_bounds__(256) k_bwd_diag(DevStruct s, const int *__restrict__ list, const T *P, int unit,
                                                    T *Y, int ldy, int nrhs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -169,17 +93,16 @@ __global__ void __launch_bounds__(256) k_bwd_diag(DevStruct s, const int *__rest
         y[i + j * nc] = Y[(fc + i) + (size_t)(j0 + j) * ldy];
     }
     __syncthreads();
-    // blocks of 32 from the bottom: solve the block with warp 0, then update
-    // the rows above it (x_i -= sum_c P[c, i] x_c for c in the block).
     for (int je = nc; je > 0; je -= 32) {
         const int jb = max(0, je - 32);
         const int nb = je - jb;
-        if (tid < 32) {
-            const int lane = tid;
-            for (int j = 0; j < nr; j++) {
+        {
+            const int lane = tid & 31, warp = tid >> 5;
+            const T rd = (!unit && lane < nb) ? T(1) / D[(jb + lane) + (size_t)(jb + lane) * st] : T(1);
+            for (int j = warp; j < nr; j += nt / 32) {
                 T v = (lane < nb) ? y[jb + lane + j * nc] : T(0);
                 for (int c = nb - 1; c >= 0; c--) {
-                    if (lane == c && !unit) v /= D[(jb + c) + (size_t)(jb + c) * st];
+                    if (lane == c) v *= rd;
                     T vc = __shfl_sync(0xffffffffu, v, c);
                     if (lane < c) v -= D[(jb + c) + (size_t)(jb + lane) * st] * vc;
                 }
@@ -201,6 +124,225 @@ __global__ void __launch_bounds__(256) k_bwd_diag(DevStruct s, const int *__rest
     }
 }
 
+// ---------------------------------------------------------------------------
+// Wide cblks: blocked diagonal solves with the inverted 32 x 32 sub-blocks Z
+// (Z = T^{-1}, T the upper factor of the sub-block, see factor.cu):
+//   forward   y_j <- S Z^T y_j,  then  y[below] -= P[below, j] y_j
+//   backward  x_j -= P[below, j]^T x[below],  then  x_j <- Z S x_j
+// with S = D (LDL^T, scaled) or I.  zside picks the Z set (GETRF: 0 = U, 1 = L^T).
+// ---------------------------------------------------------------------------
+template <typename T, int RC>
+__global__ void __launch_bounds__(256) k_fwd_diag_inv(DevStruct s, const int *__restrict__ list, const T *P,
+                                                       const T *__restrict__ dinv, int zside, int scaled,
+                                                       const T *Ldiag, T *Y, int ldy, int nrhs) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *y = reinterpret_cast<T *>(smem_raw);  // nc x RC
+    __shared__ T Z[32 * 33];
+    __shared__ T yb[32 * RC];
+    const int k = list[blockIdx.x];
+    const int fc = s.cb_fcol[k];
+    const int nc = s.cb_lcol[k] - fc + 1;
+    const int st = s.cb_stride[k];
+    const int j0 = blockIdx.y * RC;
+    const int nr = min(RC, nrhs - j0);
+    const T *D = P + s.cb_coef[k];
+    const T *Dl = Ldiag + s.cb_coef[k];
+    const int nzb = (nc + 31) / 32;
+    const T *gZ = dinv + s.cb_dinv[k] + (size_t)(zside ? nzb : 0) * 1024;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < nc * nr; e += nt) {
+        int i = e % nc, j = e / nc;
+        y[i + j * nc] = Y[(fc + i) + (size_t)(j0 + j) * ldy];
+    }
+    for (int jb = 0; jb < nc; jb += 32) {
+        const int nb = min(32, nc - jb);
+        for (int e = tid; e < 1024; e += nt) Z[(e >> 5) * 33 + (e & 31)] = gZ[(size_t)(jb / 32) * 1024 + e];
+        __syncthreads();
+        for (int e = tid; e < 32 * RC; e += nt) {  // yb = S Z^T y_j
+            int i = e & 31, j = e >> 5;
+            T acc = T(0);
+            if (i < nb && j < nr) {
+                for (int c = 0; c <= i; c++) acc += Z[c * 33 + i] * y[jb + c + j * nc];
+                if (scaled) acc *= Dl[(jb + i) + (size_t)(jb + i) * st];
+            }
+            yb[e] = acc;
+        }
+        __syncthreads();
+        for (int e = tid; e < 32 * RC; e += nt) {
+            int i = e & 31, j = e >> 5;
+            if (i < nb && j < nr) y[jb + i + j * nc] = yb[e];
+        }
+        __syncthreads();
+        for (int e = tid; e < (nc - jb - nb) * nr; e += nt) {
+            int i = jb + nb + e % (nc - jb - nb), j = e / (nc - jb - nb);
+            T acc = T(0);
+            for (int c = 0; c < nb; c++) acc += D[i + (size_t)(jb + c) * st] * y[jb + c + j * nc];
+            y[i + j * nc] -= acc;
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < nc * nr; e += nt) {
+        int i = e % nc, j = e / nc;
+        Y[(fc + i) + (size_t)(j0 + j) * ldy] = y[i + j * nc];
+    }
+}
+
+template <typename T, int RC>
+__global__ void __launch_bounds__(256) k_bwd_diag_inv(DevStruct s, const int *__restrict__ list, const T *P,
+                                                       const T *__restrict__ dinv, int zside, int scaled,
+                                                       const T *Ldiag, T *Y, int ldy, int nrhs) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *y = reinterpret_cast<T *>(smem_raw);  // nc x RC
+    __shared__ T Z[32 * 33];
+    __shared__ T yb[32 * RC];
+    const int k = list[blockIdx.x];
+    const int fc = s.cb_fcol[k];
+    const int nc = s.cb_lcol[k] - fc + 1;
+    const int st = s.cb_stride[k];
+    const int j0 = blockIdx.y * RC;
+    const int nr = min(RC, nrhs - j0);
+    const T *D = P + s.cb_coef[k];
+    const T *Dl = Ldiag + s.cb_coef[k];
+    const int nzb = (nc + 31) / 32;
+    const T *gZ = dinv + s.cb_dinv[k] + (size_t)(zside ? nzb : 0) * 1024;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < nc * nr; e += nt) {
+        int i = e % nc, j = e / nc;
+        y[i + j * nc] = Y[(fc + i) + (size_t)(j0 + j) * ldy];
+    }
+    __syncthreads();
+    const int nblk = (nc + 31) / 32;
+    for (int b = nblk - 1; b >= 0; b--) {
+        const int jb = b * 32;
+        const int nb = min(32, nc - jb);
+        const int below = nc - jb - nb;
+        for (int e = tid; e < 1024; e += nt) Z[(e >> 5) * 33 + (e & 31)] = gZ[(size_t)b * 1024 + e];
+        for (int e = tid; e < 32 * RC; e += nt) {  // yb = S (x_j - P[below, j]^T x[below])
+            int i = e & 31, j = e >> 5;
+            T acc = T(0);
+            if (i < nb && j < nr) {
+                acc = y[jb + i + j * nc];
+                for (int r = 0; r < below; r++) acc -= D[(jb + nb + r) + (size_t)(jb + i) * st] * y[jb + nb + r + j * nc];
+                if (scaled) acc *= Dl[(jb + i) + (size_t)(jb + i) * st];
+            }
+            yb[e] = acc;
+        }
+        __syncthreads();
+        for (int e = tid; e < 32 * RC; e += nt) {  // x_j = Z yb
+            int i = e & 31, j = e >> 5;
+            if (i < nb && j < nr) {
+                T acc = T(0);
+                for (int c = i; c < nb; c++) acc += Z[i * 33 + c] * yb[c + j * 32];
+                y[jb + i + j * nc] = acc;
+            }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < nc * nr; e += nt) {
+        int i = e % nc, j = e / nc;
+        Y[(fc + i) + (size_t)(j0 + j) * ldy] = y[i + j * nc];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Off-diagonal products on 64 x 64 panel tiles (RowTile.r0 = first row, the
+// tile's column block is blockIdx.z).  Forward: y[row(r)] -= P[r, cols] y_k[cols];
+// backward: x_k[c] -= sum_r P[r, c] x[row(r)].
+// ---------------------------------------------------------------------------
+template <typename T, int RC>
+__global__ void __launch_bounds__(256) k_fwd_update(DevStruct s, const RowTile *__restrict__ tiles, const T *P,
+                                                     T *Y, int ldy, int nrhs) {
+    __shared__ T yk[ST_C * RC];
+    __shared__ T part[4][ST_R * RC];
+    const RowTile tl = tiles[blockIdx.x];
+    const int k = tl.cblk;
+    const int fc = s.cb_fcol[k];
+    const int nc = s.cb_lcol[k] - fc + 1;
+    const int c0 = blockIdx.z * ST_C;
+    if (c0 >= nc) return;
+    const int ncol = min(ST_C, nc - c0);
+    const int st = s.cb_stride[k];
+    const int rows = min(ST_R, st - tl.r0);
+    const int j0 = blockIdx.y * RC;
+    const int nr = min(RC, nrhs - j0);
+    const int tid = threadIdx.x;
+    for (int e = tid; e < ST_C * RC; e += 256) {
+        int c = e % ST_C, j = e / ST_C;
+        yk[e] = (c < ncol && j < nr) ? Y[(fc + c0 + c) + (size_t)(j0 + j) * ldy] : T(0);
+    }
+    __syncthreads();
+    const int r = tid % ST_R, g = tid / ST_R;  // 4 column groups of 16
+    T acc[RC];
+#pragma unroll
+    for (int j = 0; j < RC; j++) acc[j] = T(0);
+    if (r < rows) {
+        const T *Pr = P + s.cb_coef[k] + tl.r0 + r + (size_t)c0 * st;
+        const int cb = g * 16, ce = min(ncol, cb + 16);
+        for (int c = cb; c < ce; c++) {
+            const T p = Pr[(size_t)c * st];
+#pragma unroll
+            for (int j = 0; j < RC; j++) acc[j] += p * yk[c + j * ST_C];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < RC; j++) part[g][r + j * ST_R] = acc[j];
+    __syncthreads();
+    if (tid < ST_R && tid < rows) {
+        const int gr = s.rowidx[s.cb_rowidx[k] + tl.r0 + tid];
+#pragma unroll
+        for (int j = 0; j < RC; j++) {
+            if (j >= nr) break;
+            T v = part[0][tid + j * ST_R] + part[1][tid + j * ST_R] + part[2][tid + j * ST_R] + part[3][tid + j * ST_R];
+            atomicAdd(&Y[gr + (size_t)(j0 + j) * ldy], -v);
+        }
+    }
+}
+
+template <typename T, int RC>
+__global__ void __launch_bounds__(256) k_bwd_update(DevStruct s, const RowTile *__restrict__ tiles, const T *P,
+                                                     T *Y, int ldy, int nrhs) {
+    __shared__ T xr[ST_R * RC];
+    const RowTile tl = tiles[blockIdx.x];
+    const int k = tl.cblk;
+    const int fc = s.cb_fcol[k];
+    const int nc = s.cb_lcol[k] - fc + 1;
+    const int c0 = blockIdx.z * ST_C;
+    if (c0 >= nc) return;
+    const int ncol = min(ST_C, nc - c0);
+    const int st = s.cb_stride[k];
+    const int rows = min(ST_R, st - tl.r0);
+    const int j0 = blockIdx.y * RC;
+    const int nr = min(RC, nrhs - j0);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int *ridx = s.rowidx + s.cb_rowidx[k] + tl.r0;
+    for (int e = tid; e < ST_R * RC; e += 256) {
+        int i = e % ST_R, j = e / ST_R;
+        xr[e] = (i < rows && j < nr) ? Y[ridx[i] + (size_t)(j0 + j) * ldy] : T(0);
+    }
+    __syncthreads();
+    const T *Pk = P + s.cb_coef[k] + tl.r0 + (size_t)c0 * st;
+    for (int c = warp; c < ncol; c += 8) {  // warp per column, lanes over the 64 rows
+        T acc[RC];
+#pragma unroll
+        for (int j = 0; j < RC; j++) acc[j] = T(0);
+#pragma unroll
+        for (int h = 0; h < ST_R; h += 32) {
+            const int i = h + lane;
+            if (i < rows) {
+                const T p = Pk[i + (size_t)c * st];
+#pragma unroll
+                for (int j = 0; j < RC; j++) acc[j] += p * xr[i + j * ST_R];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < RC; j++) {
+            T v = acc[j];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0 && j < nr) atomicAdd(&Y[(fc + c0 + c) + (size_t)(j0 + j) * ldy], -v);
+        }
+    }
+}
+
 // Diagonal step of LDL^T: x_i /= D_i (solve_cblk_zdiag, kernels/solve_ztrsmsp.c:664).
 template <typename T>
 __global__ void k_diag_scale(DevStruct s, const T *L, T *Y, int ldy, int nrhs) {
@@ -215,49 +357,80 @@ __global__ void k_diag_scale(DevStruct s, const T *L, T *Y, int ldy, int nrhs) {
     }
 }
 
-template <typename T>
-static inline dim3 rgrid(int count, int nrhs) { return dim3(count, (nrhs + RC - 1) / RC); }
+// ------------------------------ launchers ---------------------------------
+#define PGPU_RC_DISPATCH(nrhs, KERNEL, GRIDX, SMEM_PER_RC, ...)                                      \
+    do {                                                                                            \
+        if ((nrhs) == 1) {                                                                          \
+            KERNEL<T, 1><<<dim3(GRIDX, 1, ZDIM), 256, (SMEM_PER_RC) * 1, st>>>(__VA_ARGS__);       \
+        } else {                                                                                    \
+            KERNEL<T, 8><<<dim3(GRIDX, ((nrhs) + 7) / 8, ZDIM), 256, (SMEM_PER_RC) * 8, st>>>(__VA_ARGS__); \
+        }                                                                                           \
+    } while (0)
 
 template <typename T>
 void launch_fwd_diag(const DevStruct &s, const int *list, int count, int maxnc, const T *P, int unit, T *Y, int ldy,
                      int nrhs, cudaStream_t st) {
     if (count <= 0) return;
-    k_fwd_diag<T><<<rgrid<T>(count, nrhs), 256, (size_t)maxnc * RC * sizeof(T), st>>>(s, list, P, unit, Y, ldy, nrhs);
-}
-template <typename T>
-void launch_fwd_update(const DevStruct &s, const RowTile *tiles, int count, int maxnc, const T *P, T *Y, int ldy,
-                       int nrhs, cudaStream_t st) {
-    if (count <= 0) return;
-    k_fwd_update<T><<<rgrid<T>(count, nrhs), SROWS, (size_t)maxnc * RC * sizeof(T), st>>>(s, tiles, P, Y, ldy, nrhs);
-}
-template <typename T>
-void launch_bwd_update(const DevStruct &s, const RowTile *tiles, int count, const T *P, T *Y, int ldy, int nrhs,
-                       cudaStream_t st) {
-    if (count <= 0) return;
-    k_bwd_update<T><<<rgrid<T>(count, nrhs), SROWS, (size_t)SROWS * RC * sizeof(T), st>>>(s, tiles, P, Y, ldy, nrhs);
+    const int ZDIM = 1;
+    PGPU_RC_DISPATCH(nrhs, k_fwd_diag, count, (size_t)maxnc * sizeof(T), s, list, P, unit, Y, ldy, nrhs);
 }
 template <typename T>
 void launch_bwd_diag(const DevStruct &s, const int *list, int count, int maxnc, const T *P, int unit, T *Y, int ldy,
                      int nrhs, cudaStream_t st) {
     if (count <= 0) return;
-    k_bwd_diag<T><<<rgrid<T>(count, nrhs), 256, (size_t)maxnc * RC * sizeof(T), st>>>(s, list, P, unit, Y, ldy, nrhs);
+    const int ZDIM = 1;
+    PGPU_RC_DISPATCH(nrhs, k_bwd_diag, count, (size_t)maxnc * sizeof(T), s, list, P, unit, Y, ldy, nrhs);
+}
+template <typename T>
+void launch_fwd_diag_inv(const DevStruct &s, const int *list, int count, int maxnc, const T *P, const T *dinv,
+                         int zside, int scaled, const T *Ld, T *Y, int ldy, int nrhs, cudaStream_t st) {
+    if (count <= 0) return;
+    const int ZDIM = 1;
+    PGPU_RC_DISPATCH(nrhs, k_fwd_diag_inv, count, (size_t)maxnc * sizeof(T), s, list, P, dinv, zside, scaled, Ld,
+                     Y, ldy, nrhs);
+}
+template <typename T>
+void launch_bwd_diag_inv(const DevStruct &s, const int *list, int count, int maxnc, const T *P, const T *dinv,
+                         int zside, int scaled, const T *Ld, T *Y, int ldy, int nrhs, cudaStream_t st) {
+    if (count <= 0) return;
+    const int ZDIM = 1;
+    PGPU_RC_DISPATCH(nrhs, k_bwd_diag_inv, count, (size_t)maxnc * sizeof(T), s, list, P, dinv, zside, scaled, Ld,
+                     Y, ldy, nrhs);
+}
+template <typename T>
+void launch_fwd_update(const DevStruct &s, const RowTile *tiles, int count, int maxnc, const T *P, T *Y, int ldy,
+                       int nrhs, cudaStream_t st) {
+    if (count <= 0) return;
+    const int ZDIM = (maxnc + ST_C - 1) / ST_C;
+    PGPU_RC_DISPATCH(nrhs, k_fwd_update, count, 0, s, tiles, P, Y, ldy, nrhs);
+}
+template <typename T>
+void launch_bwd_update(const DevStruct &s, const RowTile *tiles, int count, int maxnc, const T *P, T *Y, int ldy,
+                       int nrhs, cudaStream_t st) {
+    if (count <= 0) return;
+    const int ZDIM = (maxnc + ST_C - 1) / ST_C;
+    PGPU_RC_DISPATCH(nrhs, k_bwd_update, count, 0, s, tiles, P, Y, ldy, nrhs);
 }
 template <typename T>
 void launch_diag_scale(const DevStruct &s, int cblknbr, const T *L, T *Y, int ldy, int nrhs, cudaStream_t st) {
     if (cblknbr <= 0) return;
     k_diag_scale<T><<<cblknbr, 128, 0, st>>>(s, L, Y, ldy, nrhs);
 }
-int solve_rows_per_tile() { return SROWS; }
+int solve_rows_per_tile() { return ST_R; }
 
 #define PGPU_INST_SOLVE(T)                                                                                       \
     template void launch_fwd_diag<T>(const DevStruct &, const int *, int, int, const T *, int, T *, int, int,     \
                                      cudaStream_t);                                                              \
-    template void launch_fwd_update<T>(const DevStruct &, const RowTile *, int, int, const T *, T *, int, int,    \
-                                       cudaStream_t);                                                            \
-    template void launch_bwd_update<T>(const DevStruct &, const RowTile *, int, const T *, T *, int, int,         \
-                                       cudaStream_t);                                                            \
     template void launch_bwd_diag<T>(const DevStruct &, const int *, int, int, const T *, int, T *, int, int,     \
                                      cudaStream_t);                                                              \
+    template void launch_fwd_diag_inv<T>(const DevStruct &, const int *, int, int, const T *, const T *, int,     \
+                                         int, const T *, T *, int, int, cudaStream_t);                           \
+    template void launch_bwd_diag_inv<T>(const DevStruct &, const int *, int, int, const T *, const T *, int,     \
+                                         int, const T *, T *, int, int, cudaStream_t);                           \
+    template void launch_fwd_update<T>(const DevStruct &, const RowTile *, int, int, const T *, T *, int, int,    \
+                                       cudaStream_t);                                                            \
+    template void launch_bwd_update<T>(const DevStruct &, const RowTile *, int, int, const T *, T *, int, int,    \
+                                       cudaStream_t);                                                            \
     template void launch_diag_scale<T>(const DevStruct &, int, const T *, T *, int, int, cudaStream_t);
 
 PGPU_INST_SOLVE(double)

@@ -67,4 +67,26 @@ struct FactParams {
     int *status;                // device status word (0 = fine)
 };
 
+// Element-wise transfer by a whole CTA with UNR independent loads in flight per
+// thread: st(e, ld(e)) for e in [0, total).  All loads of a batch are issued
+// before its stores, so a staging loop costs one memory round trip per UNR
+// elements instead of one per element.
+template <int UNR, typename V, typename LoadF, typename StoreF>
+__device__ __forceinline__ void batched_copy(int total, LoadF ld, StoreF stf) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e0 = tid; e0 < total; e0 += nt * UNR) {
+        V v[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; u++) {
+            const int e = e0 + u * nt;
+            if (e < total) v[u] = ld(e);
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; u++) {
+            const int e = e0 + u * nt;
+            if (e < total) stf(e, v[u]);
+        }
+    }
+}
+
 }  // namespace pgpu

@@ -81,9 +81,8 @@ __global__ void __launch_bounds__(256) k_panel_small(DevStruct s, const int *__r
     T *gL = L + s.cb_coef[k];
     T *gU = (FACT == FACT_GETRF) ? U + s.cb_coef[k] : nullptr;
     T *Q = P + tot;
-    for (int i = tid; i < tot; i += nt) P[i] = gL[i];
-    if (FACT == FACT_GETRF)
-        for (int i = tid; i < tot; i += nt) Q[i] = gU[i];
+    batched_copy<8, T>(tot, [&](int i) { return gL[i]; }, [&](int i, T v) { P[i] = v; });
+    if (FACT == FACT_GETRF) batched_copy<8, T>(tot, [&](int i) { return gU[i]; }, [&](int i, T v) { Q[i] = v; });
     __shared__ int npiv;
     if (tid == 0) npiv = 0;
     __syncthreads();
@@ -209,25 +208,22 @@ __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__re
     if (tid == 0) npiv = 0;
     if (FACT == FACT_GETRF) {  // L_kk += (U^T)_kk^T : the full diagonal block
         const T *Ut = U + s.cb_coef[k];
-        for (int e = tid; e < nc * nc; e += nt) {
-            int i = e % nc, j = e / nc;
-            A[i + (size_t)j * st] += Ut[j + (size_t)i * st];
-        }
+        batched_copy<8, T>(
+            nc * nc, [&](int e) { int i = e % nc, j = e / nc; return A[i + (size_t)j * st] + Ut[j + (size_t)i * st]; },
+            [&](int e, T v) { int i = e % nc, j = e / nc; A[i + (size_t)j * st] = v; });
     }
     __syncthreads();
     for (int jb = 0; jb < nc; jb += DNB) {
         const int nb = min(DNB, nc - jb);
         const int m = nc - jb;       // panel rows
         const int t = m - nb;        // trailing size
-        for (int e = tid; e < m * nb; e += nt) {
-            int i = e % m, c = e / m;
-            W[i * DLDW + c] = A[(jb + i) + (size_t)(jb + c) * st];
-        }
+        batched_copy<8, T>(
+            m * nb, [&](int e) { int i = e % m, c = e / m; return A[(jb + i) + (size_t)(jb + c) * st]; },
+            [&](int e, T v) { int i = e % m, c = e / m; W[i * DLDW + c] = v; });
         if (FACT == FACT_GETRF)
-            for (int e = tid; e < nb * t; e += nt) {
-                int c = e % nb, q = e / nb;
-                R[c * ldr + q] = A[(jb + c) + (size_t)(jb + nb + q) * st];
-            }
+            batched_copy<8, T>(
+                nb * t, [&](int e) { int c = e % nb, q = e / nb; return A[(jb + c) + (size_t)(jb + nb + q) * st]; },
+                [&](int e, T v) { int c = e % nb, q = e / nb; R[c * ldr + q] = v; });
         __syncthreads();
         if (warp == 0) {
             // 1. factor the nb x nb top block in registers, one row per lane
@@ -385,18 +381,20 @@ __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__re
         __syncthreads();
     }
     if (FACT == FACT_SYTRF) {  // upper part of the diagonal block holds D L^T
-        for (int e = tid; e < nc * nc; e += nt) {
-            int i = e % nc, j = e / nc;
-            if (i < j) A[i + (size_t)j * st] = A[i + (size_t)i * st] * A[j + (size_t)i * st];
-        }
+        batched_copy<8, T>(
+            nc * nc,
+            [&](int e) {
+                int i = e % nc, j = e / nc;
+                return (i < j) ? A[i + (size_t)i * st] * A[j + (size_t)i * st] : T(0);
+            },
+            [&](int e, T v) { int i = e % nc, j = e / nc; if (i < j) A[i + (size_t)j * st] = v; });
     }
     if (FACT == FACT_GETRF) {  // (U^T)_kk = (L\U)_kk^T
         __syncthreads();
         T *Ut = U + s.cb_coef[k];
-        for (int e = tid; e < nc * nc; e += nt) {
-            int i = e % nc, j = e / nc;
-            Ut[j + (size_t)i * st] = A[i + (size_t)j * st];
-        }
+        batched_copy<8, T>(
+            nc * nc, [&](int e) { int i = e % nc, j = e / nc; return A[i + (size_t)j * st]; },
+            [&](int e, T v) { int i = e % nc, j = e / nc; Ut[j + (size_t)i * st] = v; });
     }
     if (tid == 0 && npiv) atomicAdd(fp.nbpivots, npiv);
 }
@@ -408,7 +406,8 @@ constexpr int TRSM_ROWS = 32;
 constexpr int TRSM_MAXT = 10;  // column chunks of 32 per GEMM pass
 
 template <typename T, int FACT>
-__global__ void __launch_bounds__(256) k_trsm(DevStruct s, const RowTile *__restrict__ tiles, T *L, T *U) {
+__global__ void __launch_bounds__(256) k_trsm(DevStruct s, const RowTile *__restrict__ tiles, T *L, T *U,
+                                               const T *__restrict__ dinv) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const RowTile tl = tiles[blockIdx.x];
     const int side = blockIdx.y;
@@ -419,49 +418,80 @@ __global__ void __launch_bounds__(256) k_trsm(DevStruct s, const RowTile *__rest
     const int ld = nc + 1;
     T *X = reinterpret_cast<T *>(smem_raw);  // TRSM_ROWS x nc, row major, ld
     T *Ts = X + TRSM_ROWS * ld;              // 32 x (nc - jb) strip of T from column jb, row major, ld
-    __shared__ T rinv[32];
+    __shared__ T Zs[DNB * DLDW], Rs[TRSM_ROWS * DLDW];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const T *D = L + s.cb_coef[k];  // diagonal block (ld = st) of the L panel
     T *A = ((FACT == FACT_GETRF && side == 1) ? U : L) + s.cb_coef[k] + tl.r0;
     const bool unit = (FACT == FACT_GETRF && side == 1);
-    for (int e = tid; e < TRSM_ROWS * nc; e += blockDim.x) {
-        int i = e % TRSM_ROWS, j = e / TRSM_ROWS;
-        X[i * ld + j] = (i < rows) ? A[i + (size_t)j * st] : T(0);
-    }
+    const int nzb = (nc + DNB - 1) / DNB;
+    const T *gZ = dinv + s.cb_dinv[k] + (size_t)(side ? nzb : 0) * 1024;
+    batched_copy<8, T>(
+        TRSM_ROWS * nc,
+        [&](int e) { int i = e % TRSM_ROWS, j = e / TRSM_ROWS; return (i < rows) ? A[i + (size_t)j * st] : T(0); },
+        [&](int e, T v) { int i = e % TRSM_ROWS, j = e / TRSM_ROWS; X[i * ld + j] = v; });
     for (int jb = 0; jb < nc; jb += 32) {
         const int nb = min(32, nc - jb);
         const int wdt = nc - jb;
         __syncthreads();
-        for (int e = tid; e < nb * wdt; e += blockDim.x) {  // Ts[a][q] = T(jb + a, jb + q)
-            int q = e % wdt, a = e / wdt;
-            int ga = jb + a, gb = jb + q;
-            T t;
-            if (gb < ga) t = T(0);
-            else if (FACT == FACT_POTRF) t = D[gb + (size_t)ga * st];
-            else if (FACT == FACT_SYTRF) t = (gb == ga) ? D[ga + (size_t)ga * st]
-                                                          : D[ga + (size_t)ga * st] * D[gb + (size_t)ga * st];
-            else if (side == 0) t = D[ga + (size_t)gb * st];
-            else t = D[gb + (size_t)ga * st];
-            Ts[a * ld + q] = t;
-        }
+        batched_copy<8, T>(
+            nb * wdt,
+            [&](int e) {  // T(jb + a, jb + q)
+                int q = e % wdt, a = e / wdt;
+                int ga = jb + a, gb = jb + q;
+                T t;
+                if (gb < ga) t = T(0);
+                else if (FACT == FACT_POTRF) t = D[gb + (size_t)ga * st];
+                else if (FACT == FACT_SYTRF) t = (gb == ga) ? D[ga + (size_t)ga * st]
+                                                              : D[ga + (size_t)ga * st] * D[gb + (size_t)ga * st];
+                else if (side == 0) t = D[ga + (size_t)gb * st];
+                else t = D[gb + (size_t)ga * st];
+                return t;
+            },
+            [&](int e, T v) { int q = e % wdt, a = e / wdt; Ts[a * ld + q] = v; });
+        batched_copy<4, T>(
+            1024, [&](int e) { return gZ[(size_t)(jb / DNB) * 1024 + e]; },
+            [&](int e, T v) { Zs[(e >> 5) * DLDW + (e & 31)] = v; });
         __syncthreads();
-        if (tid < 32) rinv[tid] = (tid < nb && !unit) ? T(1) / Ts[tid * ld + tid] : T(1);
-        __syncthreads();
-        // substitution on the 32-wide block: one tile row per thread of warp 0
-        if (warp == 0) {
-            T x[32];
+        // X_j <- A_j T_jj^{-1}: product with the inverted block Z, then one residual
+        // correction X_j += (A_j - X_j T_jj) Z; warp w owns rows 4w..4w+3, lane = column
+        {
+            const int r0 = warp * 4;
+            T a[4], x0[4];
 #pragma unroll
-            for (int c = 0; c < 32; c++) x[c] = (c < nb) ? X[lane * ld + jb + c] : T(0);
+            for (int i = 0; i < 4; i++) {
+                a[i] = (lane < nb) ? X[(r0 + i) * ld + jb + lane] : T(0);
+                x0[i] = T(0);
+            }
+            for (int c = 0; c < nb; c++) {
+                const T z = Zs[c * DLDW + lane];
 #pragma unroll
-            for (int c = 0; c < 32; c++) {
-                x[c] *= rinv[c];
+                for (int i = 0; i < 4; i++) x0[i] += X[(r0 + i) * ld + jb + c] * z;
+            }
+            __syncwarp();
 #pragma unroll
-                for (int j = c + 1; j < 32; j++)
-                    if (j < nb) x[j] -= x[c] * Ts[c * ld + j];
+            for (int i = 0; i < 4; i++)
+                if (lane < nb) X[(r0 + i) * ld + jb + lane] = x0[i];
+            __syncwarp();
+            T rr[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) rr[i] = a[i];
+            for (int c = 0; c < nb; c++) {
+                const T t = (c <= lane && lane < nb) ? ((c == lane && unit) ? T(1) : Ts[c * ld + lane]) : T(0);
+#pragma unroll
+                for (int i = 0; i < 4; i++) rr[i] -= X[(r0 + i) * ld + jb + c] * t;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 4; i++) Rs[(r0 + i) * DLDW + lane] = (lane < nb) ? rr[i] : T(0);
+            __syncwarp();
+            for (int c = 0; c < nb; c++) {
+                const T z = Zs[c * DLDW + lane];
+#pragma unroll
+                for (int i = 0; i < 4; i++) x0[i] += Rs[(r0 + i) * DLDW + c] * z;
             }
 #pragma unroll
-            for (int c = 0; c < 32; c++)
-                if (c < nb) X[lane * ld + jb + c] = x[c];
+            for (int i = 0; i < 4; i++)
+                if (lane < nb) X[(r0 + i) * ld + jb + lane] = x0[i];
         }
         __syncthreads();
         // X[:, jb+nb:] -= X[:, jb:jb+nb] * Ts[:, nb:]
@@ -571,18 +601,20 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
 
     const int tx = tid % TX, ty = tid / TX;
     for (int k0 = 0; k0 < K; k0 += BK) {
-        for (int e = tid; e < BK * BM; e += NT) {
-            int kk = e / BM, r = e % BM;
-            T v = T(0);
-            if (r < mrows && k0 + kk < K) v = Ap[(arow + r) + (size_t)(k0 + kk) * st];
-            As[kk][r] = v;
-        }
-        for (int e = tid; e < BK * BN; e += NT) {
-            int kk = e / BN, c = e % BN;
-            T v = T(0);
-            if (c < ncols && k0 + kk < K) v = Bp[(brow + c) + (size_t)(k0 + kk) * st];
-            Bs[kk][c] = v;
-        }
+        batched_copy<(BK * BM + NT - 1) / NT, T>(
+            BK * BM,
+            [&](int e) {
+                int kk = e / BM, r = e % BM;
+                return (r < mrows && k0 + kk < K) ? Ap[(arow + r) + (size_t)(k0 + kk) * st] : T(0);
+            },
+            [&](int e, T v) { As[e / BM][e % BM] = v; });
+        batched_copy<(BK * BN + NT - 1) / NT, T>(
+            BK * BN,
+            [&](int e) {
+                int kk = e / BN, c = e % BN;
+                return (c < ncols && k0 + kk < K) ? Bp[(brow + c) + (size_t)(k0 + kk) * st] : T(0);
+            },
+            [&](int e, T v) { Bs[e / BN][e % BN] = v; });
         if (FACT == FACT_SYTRF && tid < BK)
             dsc[tid] = (k0 + tid < K) ? Dk[(k0 + tid) + (size_t)(k0 + tid) * st] : T(0);
         __syncthreads();
@@ -609,14 +641,23 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
         int c = ty + j * (BN / TN);
         int cc = ct[c];
         if (cc < 0) continue;
+        T *dst[TM];
 #pragma unroll
         for (int i = 0; i < TM; i++) {
-            int r = tx + i * TX;
-            int rr = rt[r];
-            if (rr < 0) continue;
-            T *dst = Cp + rr + (size_t)cc * stf;
-            if (tk.excl) *dst -= acc[i][j];
-            else atomicAdd(dst, -acc[i][j]);
+            int rr = rt[tx + i * TX];
+            dst[i] = (rr < 0) ? nullptr : Cp + rr + (size_t)cc * stf;
+        }
+        if (tk.excl) {
+            T old[TM];
+#pragma unroll
+            for (int i = 0; i < TM; i++) old[i] = dst[i] ? *dst[i] : T(0);
+#pragma unroll
+            for (int i = 0; i < TM; i++)
+                if (dst[i]) *dst[i] = old[i] - acc[i][j];
+        } else {
+#pragma unroll
+            for (int i = 0; i < TM; i++)
+                if (dst[i]) atomicAdd(dst[i], -acc[i][j]);
         }
     }
 }
@@ -752,21 +793,32 @@ __global__ void __launch_bounds__(256) k_update_dmma(DevStruct s, const UpdTile 
         }
         __syncthreads();
     }
+    // epilogue: scatter into the facing panel; exclusive targets are updated by
+    // plain read-modify-write with the 8 reads of a row issued together
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         const int r = wm + i * 8 + g;
         const int rr = rt[r];
         if (rr < 0) continue;
+        double *dst[8];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
+        for (int j = 0; j < 4; j++)
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int cc = ct[wn + j * 8 + q4 * 2 + h];
-                if (cc < 0) continue;
-                double *dst = Cp + rr + (size_t)cc * stf;
-                if (tk.excl) *dst -= acc[i][j][h];
-                else atomicAdd(dst, -acc[i][j][h]);
+                dst[j * 2 + h] = (cc < 0) ? nullptr : Cp + rr + (size_t)cc * stf;
             }
+        if (tk.excl) {
+            double old[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) old[q] = dst[q] ? *dst[q] : 0.0;
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (dst[q]) *dst[q] = old[q] - acc[i][q >> 1][q & 1];
+        } else {
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (dst[q]) atomicAdd(dst[q], -acc[i][q >> 1][q & 1]);
         }
     }
 }
@@ -797,11 +849,11 @@ void launch_diag_large(const DevStruct &s, const int *list, int count, size_t sm
 }
 
 template <typename T, int FACT>
-void launch_trsm(const DevStruct &s, const RowTile *tiles, int count, size_t smem, T *L, T *U, const T *,
+void launch_trsm(const DevStruct &s, const RowTile *tiles, int count, size_t smem, T *L, T *U, const T *dinv,
                  cudaStream_t st) {
     if (count <= 0) return;
     dim3 grid(count, FACT == FACT_GETRF ? 2 : 1);
-    k_trsm<T, FACT><<<grid, 256, smem, st>>>(s, tiles, L, U);
+    k_trsm<T, FACT><<<grid, 256, smem, st>>>(s, tiles, L, U, dinv);
 }
 
 template <typename T, int FACT>

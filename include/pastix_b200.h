@@ -255,8 +255,10 @@ int pgpu_solver_info(const pastix_data_t *pastix_data, pgpu_solver_info_t *info)
 int pgpu_get_coeftab(const pastix_data_t *pastix_data, void *L, void *U);
 
 /* Solve on device memory: B is an n x nrhs column-major FP64 array in the
- * ORIGINAL numbering, on the current CUDA device, overwritten by X.  The call
- * is asynchronous on `stream` (cudaStream_t, NULL = library stream). */
+ * ORIGINAL numbering, on the current CUDA device, overwritten by X.  `stream`
+ * is the caller's cudaStream_t (NULL = the legacy default stream): the solve
+ * starts after the work already queued on it, and work queued on it after the
+ * call sees X.  The call returns without waiting for the result. */
 int pgpu_solve_device(pastix_data_t *pastix_data, pastix_int_t nrhs, double *B, pastix_int_t ldb,
                       void *stream);
 /* Transposed solve A^T X = B on device memory (adjoint), same conventions. */
@@ -266,10 +268,15 @@ int pgpu_solve_transposed_device(pastix_data_t *pastix_data, pastix_int_t nrhs, 
  * order of the spm given to pastix_task_analyze). */
 int pgpu_numfact_device(pastix_data_t *pastix_data, const double *values_dev);
 /* Sampled outer product for the adjoint: G[e] = alpha * lambda[row(e)] * x[col(e)]
- * for every stored entry e of the analysed spm (original numbering, device memory). */
+ * for every stored entry e of the analysed spm (original numbering, device
+ * memory); with SpmSymmetric storage an off-diagonal entry e = (i, j) stands for
+ * a_ij and a_ji and receives alpha * (lambda[i] x[j] + lambda[j] x[i]).  With
+ * lambda = A^{-T} g and alpha = -1 this is the gradient of <g, A^{-1} b> with
+ * respect to the stored values.  No counterpart in the reference. */
 int pgpu_sampled_outer(pastix_data_t *pastix_data, double alpha, const double *lambda,
                        const double *x, double *G, void *stream);
-/* Residual SpMV on device memory: y = alpha*A*x + beta*y (original numbering). */
+/* Residual SpMV on device memory: y = alpha*A*x + beta*y (original numbering),
+ * on the caller's stream (NULL = legacy default stream). */
 int pgpu_spmv_device(pastix_data_t *pastix_data, double alpha, const double *x, double beta,
                      double *y, void *stream);
 /* Last device status word (0 = fine); non-zero after a bounded wait expired. */

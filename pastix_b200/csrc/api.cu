@@ -76,7 +76,7 @@ template <typename TS, typename TD>
 void launch_permute(int, int, const int64_t *, int, const TS *, int64_t, TD *, int64_t, cudaStream_t);
 template <typename TS, typename TD>
 void launch_cast(int64_t, const TS *, TD *, cudaStream_t);
-void launch_sampled(int64_t, const int *, const int *, double, const double *, const double *, double *,
+void launch_sampled(int64_t, const int *, const int *, double, const double *, const double *, double *, int,
                     cudaStream_t);
 }  // namespace pgpu
 
@@ -1187,7 +1187,7 @@ static int solve_device_orig(pastix_data_t *pd, int trans, int nrhs, double *B, 
     size_t need = (size_t)n * nrhs;
     if (d.w1.n < need) CUDA_TRY(d.w1.alloc(need));
     cudaEvent_t ev = nullptr;
-    if (user && user != d.stream) {  // order the library stream after the caller's stream
+    if (user != d.stream) {  // order the library stream after the caller's (NULL = legacy default) stream
         CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         CUDA_TRY(cudaEventRecord(ev, user));
         CUDA_TRY(cudaStreamWaitEvent(d.stream, ev, 0));
@@ -1681,8 +1681,11 @@ extern "C" int pgpu_sampled_outer(pastix_data_t *pd, double alpha, const double 
                                   void *stream) {
     if (!pd || !pd->dev.ready || !lambda || !x || !G) return PASTIX_ERR_BADPARAMETER;
     CUDA_TRY(cudaSetDevice(pd->dev.dev));
-    cudaStream_t st = stream ? (cudaStream_t)stream : pd->dev.stream;
-    pgpu::launch_sampled(pd->nnz, pd->dev.e_row.p, pd->dev.e_col.p, alpha, lambda, x, G, st);
+    cudaStream_t st = (cudaStream_t)stream;  // the caller's stream; NULL = legacy default stream
+    launch_cls(pd, PC_VEC, 1, [&] {
+        pgpu::launch_sampled(pd->nnz, pd->dev.e_row.p, pd->dev.e_col.p, alpha, lambda, x, G,
+                             pd->mtxtype == SpmSymmetric ? 1 : 0, st);
+    });
     CUDA_TRY(cudaGetLastError());
     return PASTIX_SUCCESS;
 }
@@ -1694,7 +1697,8 @@ extern "C" int pgpu_spmv_device(pastix_data_t *pd, double alpha, const double *x
     CUDA_TRY(cudaSetDevice(d.dev));
     if (d.w1.n < (size_t)pd->n) CUDA_TRY(d.w1.alloc(pd->n));
     if (d.w2.n < (size_t)pd->n) CUDA_TRY(d.w2.alloc(pd->n));
-    cudaStream_t st = stream ? (cudaStream_t)stream : d.stream;
+    CUDA_TRY(cudaStreamSynchronize(d.stream));  // the work vectors are shared with the library stream
+    cudaStream_t st = (cudaStream_t)stream;     // the caller's stream; NULL = legacy default stream
     pgpu::launch_permute<double, double>((int)pd->n, 1, d.perm.p, 1, x, pd->n, d.w1.p, pd->n, st);
     pgpu::launch_permute<double, double>((int)pd->n, 1, d.perm.p, 1, y, pd->n, d.w2.p, pd->n, st);
     pgpu::launch_spmv((int)pd->n, pd->csr_nnz, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha, d.w1.p, beta, d.w2.p, st);

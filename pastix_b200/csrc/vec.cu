@@ -111,11 +111,18 @@ __global__ void k_cast(int64_t n, const TS *__restrict__ src, TD *__restrict__ d
         dst[i] = (TD)src[i];
 }
 
-// G[e] = alpha * l[row[e]] * x[col[e]] for the stored entries e of the matrix
+// G[e] = alpha * l[row[e]] * x[col[e]] for the stored entries e of the matrix;
+// with symmetric storage an off-diagonal entry stands for a_ij and a_ji and
+// collects both terms.
 __global__ void k_sampled(int64_t nnz, const int *__restrict__ erow, const int *__restrict__ ecol, double alpha,
-                          const double *__restrict__ l, const double *__restrict__ x, double *__restrict__ G) {
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x)
-        G[e] = alpha * l[erow[e]] * x[ecol[e]];
+                          const double *__restrict__ l, const double *__restrict__ x, double *__restrict__ G,
+                          int sym) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x) {
+        const int i = erow[e], j = ecol[e];
+        double v = l[i] * x[j];
+        if (sym && i != j) v += l[j] * x[i];
+        G[e] = alpha * v;
+    }
 }
 
 // ------------------------------ launchers ---------------------------------
@@ -164,9 +171,9 @@ void launch_cast(int64_t n, const TS *src, TD *dst, cudaStream_t st) {
     k_cast<TS, TD><<<nblk(n), 256, 0, st>>>(n, src, dst);
 }
 void launch_sampled(int64_t nnz, const int *erow, const int *ecol, double alpha, const double *l, const double *x,
-                    double *G, cudaStream_t st) {
+                    double *G, int sym, cudaStream_t st) {
     if (nnz <= 0) return;
-    k_sampled<<<nblk(nnz), 256, 0, st>>>(nnz, erow, ecol, alpha, l, x, G);
+    k_sampled<<<nblk(nnz), 256, 0, st>>>(nnz, erow, ecol, alpha, l, x, G, sym);
 }
 
 template void launch_permute<double, double>(int, int, const int64_t *, int, const double *, int64_t, double *,

@@ -283,8 +283,15 @@ def stream_ptr(pd: Data) -> int:
     return int(p)
 
 
+def _torch_stream():
+    import torch
+    return torch.cuda.current_stream()
+
+
 def numfact_device(pd: Data, values) -> None:
-    """Numerical factorization from a CUDA float64 tensor of the spm values."""
+    """Numerical factorization from a CUDA float64 tensor of the spm values
+    (the caller's stream is synchronised first: the library works on its own stream)."""
+    _torch_stream().synchronize()
     _check("pgpu_numfact_device", _lib.load().pgpu_numfact_device(pd.ptr, C.c_void_p(values.data_ptr())))
 
 
@@ -294,7 +301,8 @@ def solve_device(pd: Data, B, transposed: bool = False) -> None:
     nrhs = 1 if B.dim() == 1 else B.shape[1]
     ld = n if B.dim() == 1 else B.stride(1)
     fn = _lib.load().pgpu_solve_transposed_device if transposed else _lib.load().pgpu_solve_device
-    _check("pgpu_solve_device", fn(pd.ptr, nrhs, C.c_void_p(B.data_ptr()), ld, None))
+    _check("pgpu_solve_device", fn(pd.ptr, nrhs, C.c_void_p(B.data_ptr()), ld,
+                                   C.c_void_p(_torch_stream().cuda_stream)))
 
 
 def solve_refine_device(pd: Data, B, X) -> None:
@@ -303,6 +311,7 @@ def solve_refine_device(pd: Data, B, X) -> None:
     nrhs = 1 if B.dim() == 1 else B.shape[1]
     ldb = n if B.dim() == 1 else B.stride(1)
     ldx = n if X.dim() == 1 else X.stride(1)
+    _torch_stream().synchronize()
     _check("pgpu_solve_refine_device",
            _lib.load().pgpu_solve_refine_device(pd.ptr, nrhs, C.c_void_p(B.data_ptr()), ldb,
                                                 C.c_void_p(X.data_ptr()), ldx))
@@ -310,7 +319,8 @@ def solve_refine_device(pd: Data, B, X) -> None:
 
 def spmv_device(pd: Data, alpha: float, x, beta: float, y) -> None:
     _check("pgpu_spmv_device", _lib.load().pgpu_spmv_device(pd.ptr, alpha, C.c_void_p(x.data_ptr()), beta,
-                                                            C.c_void_p(y.data_ptr()), None))
+                                                            C.c_void_p(y.data_ptr()),
+                                                            C.c_void_p(_torch_stream().cuda_stream)))
 
 
 def profile(pd: Data, enable: bool) -> None:

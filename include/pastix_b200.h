@@ -248,6 +248,19 @@ typedef struct pgpu_solver_info_s {
 /* Fills *info after pastix_task_analyze; returns PASTIX_ERR_BADPARAMETER before it. */
 int pgpu_solver_info(const pastix_data_t *pastix_data, pgpu_solver_info_t *info);
 
+/* Imports an analysis made elsewhere -- the SolverMatrix of the reference's own
+ * pastix_task_analyze -- for the pattern of `spm`: the permutation (permtab[v]
+ * = new index of vertex v) and the block symbolic structure as plain arrays
+ * (cblk k: columns cb_fcol[k]..cb_lcol[k], bloks cb_fblok[k]..cb_fblok[k+1]-1
+ * (bloknbr ends the last cblk), diagonal blok first; blok b: rows
+ * bk_frow[b]..bk_lrow[b] facing cblk bk_fcblk[b]).  Stands for
+ * pastix_subtask_order + symbfact + reordering + blend (blend/solver.h:141-279
+ * gives the fields).  IPARM_FACTORIZATION must be set before the call. */
+int pgpu_set_symbol(pastix_data_t *pastix_data, const spmatrix_t *spm, const pastix_int_t *permtab,
+                    pastix_int_t cblknbr, const pastix_int_t *cb_fcol, const pastix_int_t *cb_lcol,
+                    const pastix_int_t *cb_fblok, pastix_int_t bloknbr, const pastix_int_t *bk_frow,
+                    const pastix_int_t *bk_lrow, const pastix_int_t *bk_fcblk);
+
 /* Copies the factor panels to host memory in the library's layout (per cblk a
  * column-major stride x width panel at cb_coef[k]).  L and U are coefnbr
  * elements each, of the factorization's arithmetic (double, or float under

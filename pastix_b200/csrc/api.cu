@@ -1839,3 +1839,57 @@ extern "C" int pgpu_profile_get(pastix_data_t *pd, double *ms, long long *launch
     }
     return PASTIX_SUCCESS;
 }
+
+// ---------------------------------------------------------------------------
+// Import of an analysis computed elsewhere (the reference's own
+// pastix_task_analyze): the ordering and the block symbolic structure of its
+// SolverMatrix, taken as plain arrays.  Replaces pastix_subtask_order /
+// symbfact / reordering / blend for the given spm pattern.
+// ---------------------------------------------------------------------------
+extern "C" int pgpu_set_symbol(pastix_data_t *pd, const spmatrix_t *spm, const pastix_int_t *permtab,
+                               pastix_int_t cblknbr, const pastix_int_t *cb_fcol, const pastix_int_t *cb_lcol,
+                               const pastix_int_t *cb_fblok, pastix_int_t bloknbr, const pastix_int_t *bk_frow,
+                               const pastix_int_t *bk_lrow, const pastix_int_t *bk_fcblk) {
+    if (!pd || !spm || !permtab || cblknbr < 1 || bloknbr < cblknbr || !cb_fcol || !cb_lcol || !cb_fblok || !bk_frow ||
+        !bk_lrow || !bk_fcblk)
+        return PASTIX_ERR_BADPARAMETER;
+    // pattern (and graph) as in pastix_subtask_order, with the given permutation
+    pastix_order_t ord;
+    memset(&ord, 0, sizeof(ord));
+    ord.vertnbr = spm->n;
+    ord.permtab = const_cast<pastix_int_t *>(permtab);
+    std::vector<pastix_int_t> rang{0, spm->n}, tree{-1};
+    ord.cblknbr = 1;
+    ord.rangtab = rang.data();
+    ord.treetab = tree.data();
+    pastix_int_t saved = pd->iparm[IPARM_ORDERING];
+    pd->iparm[IPARM_ORDERING] = PastixOrderPersonal;
+    int rc = pastix_subtask_order(pd, spm, &ord);
+    pd->iparm[IPARM_ORDERING] = saved;
+    if (rc) return rc;
+    pgpu::Symbol &sy = pd->symbol;
+    sy = pgpu::Symbol{};
+    sy.nodenbr = spm->n;
+    sy.cblktab.resize(cblknbr + 1);
+    for (pastix_int_t k = 0; k < cblknbr; k++) sy.cblktab[k] = pgpu::SymCblk{cb_fcol[k], cb_lcol[k], cb_fblok[k]};
+    sy.cblktab[cblknbr] = pgpu::SymCblk{spm->n, spm->n - 1, bloknbr};
+    sy.bloktab.resize(bloknbr);
+    for (pastix_int_t k = 0; k < cblknbr; k++) {
+        pastix_int_t be = (k + 1 < cblknbr) ? cb_fblok[k + 1] : bloknbr;
+        if (cb_fblok[k] < 0 || be > bloknbr || be <= cb_fblok[k]) return PASTIX_ERR_BADPARAMETER;
+        for (pastix_int_t b = cb_fblok[k]; b < be; b++)
+            sy.bloktab[b] = pgpu::SymBlok{bk_frow[b], bk_lrow[b], k, bk_fcblk[b]};
+    }
+    std::string err = pgpu::symbol_check(sy);
+    if (!err.empty()) { perr("pgpu_set_symbol: structure check failed: %s", err.c_str()); return PASTIX_ERR_BADPARAMETER; }
+    pd->factotype = (int)pd->iparm[IPARM_FACTORIZATION];
+    int fk = fact_kind(pd);
+    pgpu::solver_build(pd->solver, sy, fk);
+    rc = build_maps_and_lists(pd);
+    if (rc) return rc;
+    pd->dparm[DPARM_FACT_THFLOPS] = pd->solver.thflops;
+    pd->iparm[IPARM_NNZEROS] = pd->solver.nnzl * (fk == pgpu::FACT_GETRF ? 2 : 1);
+    pd->steps = STEP_INIT | STEP_ORDERING | STEP_SYMBFACT | STEP_ANALYSE;
+    pd->dev.ready = false;
+    return PASTIX_SUCCESS;
+}

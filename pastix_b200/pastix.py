@@ -184,6 +184,17 @@ def analyze_grid(pd: Data, spm: spmatrix, nx: int, ny: int, nz: int) -> None:
     subtask_blend(pd)
 
 
+def set_symbol(pd: Data, spm: spmatrix, permtab, cb_fcol, cb_lcol, cb_fblok, bk_frow, bk_lrow, bk_fcblk) -> None:
+    """pgpu_set_symbol: use an ordering + block symbolic structure computed
+    elsewhere (e.g. exported from the reference's SolverMatrix)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.int64) for a in (permtab, cb_fcol, cb_lcol, cb_fblok, bk_frow, bk_lrow,
+                                                               bk_fcblk)]
+    pd._keep = arrs
+    p = [a.ctypes.data_as(PINT) for a in arrs]
+    _check("pgpu_set_symbol", _lib.load().pgpu_set_symbol(pd.ptr, spm.pointer(), p[0], len(arrs[1]), p[1], p[2], p[3],
+                                                           len(arrs[4]), p[4], p[5], p[6]))
+
+
 def task_numfact(pd: Data, spm: spmatrix) -> None:
     _check("pastix_task_numfact", _lib.load().pastix_task_numfact(pd.ptr, spm.pointer()))
 

@@ -81,11 +81,12 @@ def test_split_widths(lib):
     # the 144-column top separator was cut into pieces of 6..12 columns
     top = np.where(info["cb_lcol"] == 12 ** 3 - 1)[0][0]
     assert 6 <= w[top] <= 12
-    # every piece of a split separator carries a dense blok facing each later piece
-    for k in range(info["cblknbr"] - 1):
-        if info["cb_lcol"][k] + 1 == info["cb_fcol"][k + 1] and w[k] >= 6:
-            pass
-    assert info["coefnbr"] > 0
+    # every piece of the split top separator carries one dense blok facing each later piece
+    pieces = [k for k in range(info["cblknbr"]) if info["cb_fcol"][k] >= 12 ** 3 - 144]
+    for i, k in enumerate(pieces):
+        fb = info["cb_fblok"][k]
+        faced = list(info["bk_fcblk"][fb + 1: fb + len(pieces) - i])
+        assert faced == pieces[i + 1:]
 
 
 def _sum1d(info, fact):
@@ -157,3 +158,26 @@ def test_builtin_ordering_on_fixture(lib):
     info = px.solver_info(pd)
     assert info["n"] == n and info["cblknbr"] > 1
     assert sorted(info["permtab"].tolist()) == list(range(n))
+
+
+def test_import_external_symbol(lib):
+    """pgpu_set_symbol takes the structure of an analysis made elsewhere; the
+    resulting solver layout equals the one from the library's own analysis."""
+    A = gen.laplacian7(9, 8, 7)
+    pd, S, info = analyse(A, (9, 8, 7), "POTRF")
+    ip, dp = px.initParam()
+    ip[px.iparm.factorization] = px.factotype.POTRF
+    pd2 = px.init(ip, dp)
+    px.set_symbol(pd2, S, info["permtab"], info["cb_fcol"], info["cb_lcol"], info["cb_fblok"][:-1],
+                  info["bk_frow"], info["bk_lrow"], info["bk_fcblk"])
+    info2 = px.solver_info(pd2)
+    for key in ("cb_fcol", "cb_lcol", "cb_fblok", "cb_stride", "cb_coef", "bk_frow", "bk_lrow", "bk_fcblk",
+                "bk_rowoff", "permtab", "cb_level"):
+        assert np.array_equal(info[key], info2[key]), key
+    assert info2["thflops"] == info["thflops"]
+    # a structure that misses a facing cblk is rejected
+    bad = info["bk_fcblk"].copy()
+    bad[info["cb_fblok"][0] + 1] = 0
+    with pytest.raises(px.PastixError):
+        px.set_symbol(pd2, S, info["permtab"], info["cb_fcol"], info["cb_lcol"], info["cb_fblok"][:-1],
+                      info["bk_frow"], info["bk_lrow"], bad)

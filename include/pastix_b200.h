@@ -305,6 +305,21 @@ void *pgpu_stream(pastix_data_t *pastix_data);
 int pgpu_solve_refine_device(pastix_data_t *pastix_data, pastix_int_t nrhs, const double *B, pastix_int_t ldb,
                              double *X, pastix_int_t ldx);
 
+/* pgpu_solve_device without any allocation, for callers that cannot allocate
+ * device memory when they solve.  No counterpart in the reference.  Its work
+ * vectors live in one fixed array in the library's module memory: n * nrhs may
+ * not exceed PGPU_STATIC_SOLVE_ELEMS (12 bytes per element, 12 MiB in all);
+ * larger calls return PASTIX_ERR_BADPARAMETER and touch nothing.  The first
+ * call on a device sets up that device (looks the array up, creates one
+ * event): make it before any stream capture.  The array is shared by every
+ * pastix_data_t of the process on that device, so calls that overlap in time
+ * (two host threads, or two streams without ordering between them) race on
+ * it.  Not available while pgpu_profile timing is on.  Same arguments and
+ * stream semantics as pgpu_solve_device (A X = B). */
+#define PGPU_STATIC_SOLVE_ELEMS 1048576
+int pgpu_solve_device_static(pastix_data_t *pastix_data, pastix_int_t nrhs, double *B, pastix_int_t ldb,
+                             void *stream);
+
 /* Launch accounting.  pgpu_profile(pd, 1) resets the counters and times every
  * launch with CUDA events on the library stream; pgpu_profile(pd, 0) resets
  * and only counts.  pgpu_profile_get returns, per kernel class (fill, panel,

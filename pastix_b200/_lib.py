@@ -31,6 +31,7 @@ EXPORTS = [
     "pgpu_solver_info", "pgpu_get_coeftab", "pgpu_solve_device", "pgpu_solve_transposed_device",
     "pgpu_numfact_device", "pgpu_sampled_outer", "pgpu_spmv_device", "pgpu_device_status",
     "pgpu_stream", "pgpu_solve_refine_device", "pgpu_profile", "pgpu_profile_get", "pgpu_set_symbol",
+    "pgpu_solve_device_static",
 ]
 
 # kernel classes of pgpu_profile_get, in order
@@ -114,6 +115,7 @@ def load() -> C.CDLL:
         "pgpu_solver_info": (C.c_int, [P, C.POINTER(pgpu_solver_info_t)]),
         "pgpu_get_coeftab": (C.c_int, [P, VP, VP]),
         "pgpu_solve_device": (C.c_int, [P, pastix_int_t, VP, pastix_int_t, VP]),
+        "pgpu_solve_device_static": (C.c_int, [P, pastix_int_t, VP, pastix_int_t, VP]),
         "pgpu_solve_transposed_device": (C.c_int, [P, pastix_int_t, VP, pastix_int_t, VP]),
         "pgpu_numfact_device": (C.c_int, [P, VP]),
         "pgpu_sampled_outer": (C.c_int, [P, C.c_double, VP, VP, VP, VP]),

@@ -21,6 +21,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1891,5 +1892,96 @@ extern "C" int pgpu_set_symbol(pastix_data_t *pd, const spmatrix_t *spm, const p
     pd->iparm[IPARM_NNZEROS] = pd->solver.nnzl * (fk == pgpu::FACT_GETRF ? 2 : 1);
     pd->steps = STEP_INIT | STEP_ORDERING | STEP_SYMBFACT | STEP_ANALYSE;
     pd->dev.ready = false;
+    return PASTIX_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Device solve with no allocation.  Some callers cannot allocate device
+// memory at call time: code running inside a region that must not
+// synchronize (cudaMalloc / cudaFree serialize against every stream of the
+// device), or an application that reserves the whole heap up front.  This
+// variant of pgpu_solve_device takes its permuted work vector (and the float
+// copy of the mixed-precision path) from a fixed array in the module's global
+// memory instead of the grow-only work areas of pgpu_solve_device.  The first
+// call on a device looks the array's address up and creates the ordering
+// event; later calls on that device only launch kernels.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kStaticElems = PGPU_STATIC_SOLVE_ELEMS;
+// kStaticElems FP64 elements followed by kStaticElems FP32 elements.  Nothing
+// in it has to start at zero: every element a call reads is written earlier in
+// the same call (the permute fills the FP64 part, the cast the FP32 part).
+static __device__ __align__(256) unsigned char g_static_solve[kStaticElems * (sizeof(double) + sizeof(float))];
+
+constexpr int kMaxDevices = 64;
+struct StaticSolveSlot {
+    bool ready = false;
+    unsigned char *base = nullptr;  // address of g_static_solve in this device's context
+    cudaEvent_t ev = nullptr;       // orders the library stream with the caller's stream
+};
+static StaticSolveSlot g_static_slots[kMaxDevices];
+static std::mutex g_static_mutex;
+
+// Set-up of the device current on this thread.
+static int static_solve_setup(int dev, StaticSolveSlot **out) {
+    if (dev < 0 || dev >= kMaxDevices) return PASTIX_ERR_BADPARAMETER;
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    StaticSolveSlot &s = g_static_slots[dev];
+    if (!s.ready) {
+        void *p = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&p, g_static_solve));
+        CUDA_TRY(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming));
+        s.base = static_cast<unsigned char *>(p);
+        s.ready = true;
+    }
+    *out = &s;
+    return PASTIX_SUCCESS;
+}
+}  // namespace
+
+extern "C" int pgpu_solve_device_static(pastix_data_t *pd, pastix_int_t nrhs, double *B, pastix_int_t ldb,
+                                        void *stream) {
+    int rc = check_numfact(pd, "pgpu_solve_device_static");
+    if (rc) return rc;
+    if (nrhs < 1 || ldb < pd->n || !B) return PASTIX_ERR_BADPARAMETER;
+    const size_t need = (size_t)pd->n * (size_t)nrhs;
+    if (need > kStaticElems) {
+        perr("pgpu_solve_device_static: n * nrhs = %zu exceeds the fixed work array of %zu elements "
+             "(use pgpu_solve_device)", need, kStaticElems);
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    if (pd->prof_on) {  // timed launch accounting creates events and grows a host list
+        perr("pgpu_solve_device_static: not available while pgpu_profile timing is enabled");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    Device &d = pd->dev;
+    CUDA_TRY(cudaSetDevice(d.dev));
+    StaticSolveSlot *slot = nullptr;
+    rc = static_solve_setup(d.dev, &slot);
+    if (rc) return rc;
+    double *Y = reinterpret_cast<double *>(slot->base);
+    float *Yf = reinterpret_cast<float *>(slot->base + kStaticElems * sizeof(double));
+    const idx_t n = pd->n;
+    cudaStream_t user = (cudaStream_t)stream;
+    if (user != d.stream) {
+        CUDA_TRY(cudaEventRecord(slot->ev, user));
+        CUDA_TRY(cudaStreamWaitEvent(d.stream, slot->ev, 0));
+    }
+    pgpu::launch_permute<double, double>((int)n, (int)nrhs, d.perm.p, 1, B, ldb, Y, n, d.stream);
+    if (!pd->mixed) {
+        solve_perm<double>(pd, 0, Y, (int)n, (int)nrhs);
+    } else {
+        for (int j = 0; j < nrhs; j++)
+            pgpu::launch_cast<double, float>(n, Y + (size_t)j * n, Yf + (size_t)j * n, d.stream);
+        solve_perm<float>(pd, 0, Yf, (int)n, (int)nrhs);
+        for (int j = 0; j < nrhs; j++)
+            pgpu::launch_cast<float, double>(n, Yf + (size_t)j * n, Y + (size_t)j * n, d.stream);
+    }
+    pgpu::launch_permute<double, double>((int)n, (int)nrhs, d.perm.p, 0, Y, n, B, ldb, d.stream);
+    if (user != d.stream) {
+        CUDA_TRY(cudaEventRecord(slot->ev, d.stream));
+        CUDA_TRY(cudaStreamWaitEvent(user, slot->ev, 0));
+    }
+    CUDA_TRY(cudaGetLastError());
     return PASTIX_SUCCESS;
 }

@@ -37,9 +37,10 @@ void launch_fill_coef(int64_t, const double *, const int64_t *, const int64_t *,
 template <typename T, int F>
 void launch_panel_small(const DevStruct &, const int *, int, size_t, T *, T *, const FactParams &, cudaStream_t);
 template <typename T, int F>
-void launch_diag_large(const DevStruct &, const int *, int, size_t, T *, T *, T *, const FactParams &, cudaStream_t);
+void launch_diag_large(const DevStruct &, const int *, int, int, size_t, T *, T *, T *, const FactParams &,
+                       cudaStream_t);
 template <typename T, int F>
-void launch_trsm(const DevStruct &, const RowTile *, int, size_t, T *, T *, const T *, cudaStream_t);
+void launch_trsm(const DevStruct &, const RowTile *, int, int, size_t, T *, T *, const T *, cudaStream_t);
 template <typename T, int F>
 void launch_update(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);
 template <typename T, int F>
@@ -137,6 +138,8 @@ struct LevelLists {
     int cb0, cb1;           // all cblks of the level (solve diag)
     int st0, st1;           // solve row tiles
     int maxnc;
+    int trsm_maxnc;         // widest cblk with TRSM tiles
+    int diag_maxnc;         // widest cblk of the large list
     size_t small_smem_elems, diag_smem_elems, trsm_smem_elems;
 };
 
@@ -661,6 +664,8 @@ static int build_maps_and_lists(pastix_data_t *pd) {
         L.cb0 = (int)pd->level_cblks.size();
         L.st0 = (int)pd->solve_tiles.size();
         L.maxnc = 1;
+        L.trsm_maxnc = 0;
+        L.diag_maxnc = 0;
         L.small_smem_elems = L.diag_smem_elems = L.trsm_smem_elems = 0;
         for (idx_t p = sv.lvl_ptr[l]; p < sv.lvl_ptr[l + 1]; p++) {
             idx_t k = sv.lvl_cblk[p];
@@ -673,11 +678,13 @@ static int build_maps_and_lists(pastix_data_t *pd) {
             } else {
                 pd->large_list.push_back((int)k);
                 pd->cb_dinv[k] = pd->dinv_total;
+                L.diag_maxnc = std::max<int>(L.diag_maxnc, (int)nc);
                 pd->dinv_total += pgpu::dinv_elems((int)nc, fk);
                 L.diag_smem_elems = std::max<size_t>(L.diag_smem_elems, (size_t)pgpu::diag_smem_elems((int)nc, fk));
                 int bm = pgpu::trsm_tile_rows((int)nc);
                 for (idx_t r = nc; r < st; r += bm) pd->trsm_tiles.push_back(pgpu::RowTile{(int)k, (int)r});
                 if (st > nc) L.trsm_smem_elems = std::max<size_t>(L.trsm_smem_elems, (size_t)pgpu::trsm_smem_elems((int)nc));
+                if (st > nc) L.trsm_maxnc = std::max<int>(L.trsm_maxnc, (int)nc);
             }
             for (idx_t r = nc; r < st; r += SR) pd->solve_tiles.push_back(pgpu::RowTile{(int)k, (int)r});
         }
@@ -883,11 +890,11 @@ static int run_factor(pastix_data_t *pd, double criterion) {
                                            lv.small_smem_elems * sizeof(T), L, U, fp, st);
         });
         launch_cls(pd, PC_DIAG_LARGE, lv.large1 - lv.large0, [&] {
-            pgpu::launch_diag_large<T, F>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0,
+            pgpu::launch_diag_large<T, F>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0, lv.diag_maxnc,
                                           lv.diag_smem_elems * sizeof(T), L, U, Dinv, fp, st);
         });
         launch_cls(pd, PC_TRSM, lv.trsm1 - lv.trsm0, [&] {
-            pgpu::launch_trsm<T, F>(d.ds, d.trsm_tiles.p + lv.trsm0, lv.trsm1 - lv.trsm0,
+            pgpu::launch_trsm<T, F>(d.ds, d.trsm_tiles.p + lv.trsm0, lv.trsm1 - lv.trsm0, lv.trsm_maxnc,
                                     lv.trsm_smem_elems * sizeof(T), L, U, Dinv, st);
         });
         launch_cls(pd, PC_UPDATE, lv.upd1 - lv.upd0, [&] {

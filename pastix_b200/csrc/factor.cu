@@ -824,6 +824,482 @@ __global__ void __launch_bounds__(256) k_update_dmma(DevStruct s, const UpdTile 
 }
 
 // ---------------------------------------------------------------------------
+// Off-diagonal TRSM on FP64 tensor cores (DMMA m8n8k4), X T = A for a tile of
+// 32 panel rows of a wide cblk, T the upper triangular factor of the diagonal
+// block (L^T for POTRF, D L^T for SYTRF, U and L^T for the two GETRF sides),
+// as cpucblk_ztrsmsp (kernels/core_ztrsmsp.c:356).  The whole 32 x nc tile
+// stays in registers as 8 x 8 accumulator fragments: warp w owns the column
+// fragments w, w + 8, w + 16, ... (nc <= TD_MAXNC).  Column block j (32
+// columns) is solved with the inverted diagonal sub-block Z = T_jj^{-1} from
+// k_diag_large plus one residual correction, X_j = X0 + (A_j - X0 T_jj) Z
+// with X0 = A_j Z, then subtracted from the fragments to its right with T's
+// rows of block j read straight from the (L2-resident) diagonal block.
+// Storage may be FP32 (mixed precision); the arithmetic is FP64 throughout.
+// ---------------------------------------------------------------------------
+constexpr int TD_Q = 6;                 // column fragments per warp
+constexpr int TD_MAXNC = 8 * TD_Q * 8;  // 384 columns
+constexpr int TD_LDS = 36;              // shared row stride (doubles): 2 wavefronts per fragment load
+
+// T(a, b) of the upper triangular factor, a <= b < nc (callers guarantee it).
+template <typename T, int FACT>
+__device__ __forceinline__ double trsm_tval(const T *D, int st, int a, int b, int side) {
+    if (FACT == FACT_POTRF) return (double)D[b + (size_t)a * st];
+    if (FACT == FACT_SYTRF) {
+        const double da = (double)D[a + (size_t)a * st];
+        return (a == b) ? da : da * (double)D[b + (size_t)a * st];
+    }
+    if (side == 0) return (double)D[a + (size_t)b * st];
+    return (a == b) ? 1.0 : (double)D[b + (size_t)a * st];
+}
+
+template <typename T, int FACT>
+__global__ void __launch_bounds__(256, 1) k_trsm_dmma(DevStruct s, const RowTile *__restrict__ tiles, T *L, T *U,
+                                                       const T *__restrict__ dinv) {
+    __shared__ double As[32 * TD_LDS], Xs[32 * TD_LDS], Rs[32 * TD_LDS];
+    const RowTile tl = tiles[blockIdx.x];
+    const int side = blockIdx.y;
+    const int k = tl.cblk;
+    const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+    const int st = s.cb_stride[k];
+    const int rows = min(32, st - tl.r0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const T *D = L + s.cb_coef[k];
+    T *A = ((FACT == FACT_GETRF && side == 1) ? U : L) + s.cb_coef[k] + tl.r0;
+    const int nzb = (nc + 31) / 32;
+    const int ncf = (nc + 7) / 8;
+    const T *gZ = dinv + s.cb_dinv[k] + (size_t)(side ? nzb : 0) * 1024;
+
+    double acc[4][TD_Q][2];
+#pragma unroll
+    for (int q = 0; q < TD_Q; q++) {
+        const int c0 = 8 * (warp + 8 * q) + 2 * t4;
+#pragma unroll
+        for (int rf = 0; rf < 4; rf++) {
+            const int r = 8 * rf + g;
+#pragma unroll
+            for (int e = 0; e < 2; e++)
+                acc[rf][q][e] = (r < rows && c0 + e < nc) ? (double)A[r + (size_t)(c0 + e) * st] : 0.0;
+        }
+    }
+    const int orf = warp >> 1, ocf = 2 * (warp & 1);  // this warp's fragments of the 32 x 32 block solve
+    for (int j = 0; j < nzb; j++) {
+        const int jb = 32 * j;
+        // i. the owners of block j hand their fragments over to shared memory
+#pragma unroll
+        for (int q = 0; q < TD_Q; q++) {
+            const int cf = warp + 8 * q;
+            if ((cf >> 2) == j) {
+                const int cc = 8 * (cf & 3) + 2 * t4;
+#pragma unroll
+                for (int rf = 0; rf < 4; rf++) {
+                    As[(8 * rf + g) * TD_LDS + cc] = acc[rf][q][0];
+                    As[(8 * rf + g) * TD_LDS + cc + 1] = acc[rf][q][1];
+                }
+            }
+        }
+        __syncthreads();
+        const T *Zj = gZ + (size_t)j * 1024;
+        double x0[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+        // ii-a. X0 = A_j Z
+#pragma unroll
+        for (int ks = 0; ks < 8; ks++) {
+            const double a = As[(8 * orf + g) * TD_LDS + 4 * ks + t4];
+#pragma unroll
+            for (int c = 0; c < 2; c++)
+                dmma884(x0[c][0], x0[c][1], a, (double)Zj[(4 * ks + t4) * 32 + 8 * (ocf + c) + g]);
+        }
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            Xs[(8 * orf + g) * TD_LDS + 8 * (ocf + c) + 2 * t4] = x0[c][0];
+            Xs[(8 * orf + g) * TD_LDS + 8 * (ocf + c) + 2 * t4 + 1] = x0[c][1];
+        }
+        __syncthreads();
+        // ii-b. R = A_j - X0 T_jj
+        double rr[2][2];
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            rr[c][0] = As[(8 * orf + g) * TD_LDS + 8 * (ocf + c) + 2 * t4];
+            rr[c][1] = As[(8 * orf + g) * TD_LDS + 8 * (ocf + c) + 2 * t4 + 1];
+        }
+#pragma unroll
+        for (int ks = 0; ks < 8; ks++) {
+            const double a = -Xs[(8 * orf + g) * TD_LDS + 4 * ks + t4];
+            const int ta = jb + 4 * ks + t4;
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const int tb = jb + 8 * (ocf + c) + g;
+                const double b = (ta <= tb && tb < nc) ? trsm_tval<T, FACT>(D, st, ta, tb, side) : 0.0;
+                dmma884(rr[c][0], rr[c][1], a, b);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            Rs[(8 * orf + g) * TD_LDS + 8 * (ocf + c) + 2 * t4] = rr[c][0];
+            Rs[(8 * orf + g) * TD_LDS + 8 * (ocf + c) + 2 * t4 + 1] = rr[c][1];
+        }
+        __syncthreads();
+        // ii-c. X_j = X0 + R Z, to shared memory and to the panel
+#pragma unroll
+        for (int ks = 0; ks < 8; ks++) {
+            const double a = Rs[(8 * orf + g) * TD_LDS + 4 * ks + t4];
+#pragma unroll
+            for (int c = 0; c < 2; c++)
+                dmma884(x0[c][0], x0[c][1], a, (double)Zj[(4 * ks + t4) * 32 + 8 * (ocf + c) + g]);
+        }
+        {
+            const int r = 8 * orf + g;
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int cc = 8 * (ocf + c) + 2 * t4 + e;
+                    Xs[r * TD_LDS + cc] = x0[c][e];
+                    if (r < rows && jb + cc < nc) A[r + (size_t)(jb + cc) * st] = (T)x0[c][e];
+                }
+            }
+        }
+        __syncthreads();
+        // iii. fragments right of block j: acc -= X_j T(block j rows, their columns)
+        if (4 * j + 4 < ncf) {
+#pragma unroll 2
+            for (int ks = 0; ks < 8; ks++) {
+                const int ta = jb + 4 * ks + t4;
+                double a[4];
+#pragma unroll
+                for (int rf = 0; rf < 4; rf++) a[rf] = -Xs[(8 * rf + g) * TD_LDS + 4 * ks + t4];
+                double b[TD_Q];
+#pragma unroll
+                for (int q = 0; q < TD_Q; q++) {
+                    const int cf = warp + 8 * q;
+                    const int tb = 8 * cf + g;
+                    b[q] = (cf >= 4 * j + 4 && ta < nc && tb < nc) ? trsm_tval<T, FACT>(D, st, ta, tb, side) : 0.0;
+                }
+#pragma unroll
+                for (int q = 0; q < TD_Q; q++) {
+                    const int cf = warp + 8 * q;
+                    if (cf >= 4 * j + 4 && cf < ncf) {
+#pragma unroll
+                        for (int rf = 0; rf < 4; rf++) dmma884(acc[rf][q][0], acc[rf][q][1], a[rf], b[q]);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Diagonal block of a wide cblk on FP64 tensor cores (nc <= DG_MAXNC).  Right
+// looking by 32-column panels, as core_zpotrfsp / core_zgetrfsp /
+// core_zsytrfsp block their diagonal factorization:
+//   1. the (nc - jb) x 32 panel is staged in shared memory (FP64, row major);
+//   2. one warp factors its 32 x 32 top block in registers with static
+//      pivoting; one or two warps invert the triangular factor(s) (kept in
+//      `dinv` for the TRSM and the solve);
+//   3. the rows below (and GETRF's U strip) are solved 8 rows per warp with
+//      X = X0 + (A - X0 T) Z, X0 = A Z, on DMMA m8n8k4;
+//   4. the trailing block is updated from global memory in 16 x 16 blocks, the
+//      lower triangle for the symmetric kinds.
+// Storage may be FP32 (mixed precision); the arithmetic is FP64.
+// ---------------------------------------------------------------------------
+constexpr int DG_LD = 36;      // shared row stride (doubles): 2 wavefronts per fragment access
+constexpr int DG_MAXNC = 384;
+
+__host__ __device__ inline long long diag_dmma_smem_bytes(int nc) { return (long long)nc * DG_LD * 8; }
+
+// T_jj(a, b), a <= b, of the factored top block W (row major, ld DG_LD).
+template <int FACT>
+__device__ __forceinline__ double dg_t(const double *W, int a, int b, int side) {
+    if (FACT == FACT_POTRF) return W[b * DG_LD + a];
+    if (FACT == FACT_SYTRF) return (a == b) ? W[a * DG_LD + a] : W[a * DG_LD + a] * W[b * DG_LD + a];
+    if (side == 0) return W[a * DG_LD + b];
+    return (a == b) ? 1.0 : W[b * DG_LD + a];
+}
+
+// One warp: Z = T_jj^{-1} of the nb x nb leading block (identity beyond), to
+// shared memory (row major, ld DG_LD) and to `gZ` (32 x 32 row major).  Lane j
+// forms column j by back substitution.
+template <typename T, int FACT>
+__device__ __forceinline__ void dg_inverse(const double *W, int nb, int side, double *Z, T *gZ) {
+    const int lane = threadIdx.x & 31;
+    const double rl = (lane < nb) ? 1.0 / dg_t<FACT>(W, lane, lane, side) : 1.0;
+    double z[32];
+#pragma unroll
+    for (int i = 31; i >= 0; i--) {
+        double acc = 0.0;
+#pragma unroll
+        for (int kk = i + 1; kk < 32; kk++)
+            if (kk < nb) acc += dg_t<FACT>(W, i, kk, side) * z[kk];
+        const double ri = __shfl_sync(0xffffffffu, rl, i);
+        z[i] = (i > lane) ? 0.0 : ((i == lane) ? rl : -acc * ri);
+    }
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+        Z[i * DG_LD + lane] = z[i];
+        gZ[i * 32 + lane] = (T)z[i];
+    }
+}
+
+// CTA-wide transfer of a rows x cols region in 8 x 4 sub-tiles: lane (g, t4)
+// moves element (8 rb + g, 4 cb + t4), UNR sub-tiles in flight per warp, so
+// both a column-major global side and a row-major (ld DG_LD) shared side are
+// accessed without waste.
+template <int UNR, typename LoadF, typename StoreF>
+__device__ __forceinline__ void dg_copy(int rows, int cols, LoadF ld, StoreF stf) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int nrb = (rows + 7) >> 3, tot = nrb * ((cols + 3) >> 2);
+    for (int i0 = warp; i0 < tot; i0 += nw * UNR) {
+        double v[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; u++) {
+            const int i = i0 + u * nw;
+            const int r = 8 * (i % nrb) + g, c = 4 * (i / nrb) + t4;
+            v[u] = (i < tot && r < rows && c < cols) ? ld(r, c) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; u++) {
+            const int i = i0 + u * nw;
+            const int r = 8 * (i % nrb) + g, c = 4 * (i / nrb) + t4;
+            if (i < tot && r < rows && c < cols) stf(r, c, v[u]);
+        }
+    }
+}
+
+// One warp: X T = A for an 8 x 32 row fragment.  a_at(row, col) reads A,
+// t_at(a, b) reads T (zero outside its upper nb x nb part), Z = T^{-1} in
+// shared memory, Sw an 8 x DG_LD scratch of this warp; store(row, col, x).
+template <typename AF, typename TF, typename SF>
+__device__ __forceinline__ void dg_solve8(AF a_at, TF t_at, const double *Z, double *Sw, SF store) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
+    double x[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+    for (int ks = 0; ks < 8; ks++) {
+        const double a = a_at(g, 4 * ks + t4);
+#pragma unroll
+        for (int cf = 0; cf < 4; cf++) dmma884(x[cf][0], x[cf][1], a, Z[(4 * ks + t4) * DG_LD + 8 * cf + g]);
+    }
+#pragma unroll
+    for (int cf = 0; cf < 4; cf++) {
+        Sw[g * DG_LD + 8 * cf + 2 * t4] = x[cf][0];
+        Sw[g * DG_LD + 8 * cf + 2 * t4 + 1] = x[cf][1];
+    }
+    __syncwarp();
+    double r[4][2];
+#pragma unroll
+    for (int cf = 0; cf < 4; cf++) {
+        r[cf][0] = a_at(g, 8 * cf + 2 * t4);
+        r[cf][1] = a_at(g, 8 * cf + 2 * t4 + 1);
+    }
+#pragma unroll
+    for (int ks = 0; ks < 8; ks++) {
+        const double a = -Sw[g * DG_LD + 4 * ks + t4];
+#pragma unroll
+        for (int cf = 0; cf < 4; cf++) dmma884(r[cf][0], r[cf][1], a, t_at(4 * ks + t4, 8 * cf + g));
+    }
+    __syncwarp();
+#pragma unroll
+    for (int cf = 0; cf < 4; cf++) {
+        Sw[g * DG_LD + 8 * cf + 2 * t4] = r[cf][0];
+        Sw[g * DG_LD + 8 * cf + 2 * t4 + 1] = r[cf][1];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int ks = 0; ks < 8; ks++) {
+        const double a = Sw[g * DG_LD + 4 * ks + t4];
+#pragma unroll
+        for (int cf = 0; cf < 4; cf++) dmma884(x[cf][0], x[cf][1], a, Z[(4 * ks + t4) * DG_LD + 8 * cf + g]);
+    }
+#pragma unroll
+    for (int cf = 0; cf < 4; cf++) {
+        store(g, 8 * cf + 2 * t4, x[cf][0]);
+        store(g, 8 * cf + 2 * t4 + 1, x[cf][1]);
+    }
+    __syncwarp();
+}
+
+template <typename T, int FACT>
+__global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__restrict__ list, T *L, T *U, T *dinv,
+                                                       FactParams fp) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *W = reinterpret_cast<double *>(smem_raw);  // (nc - jb) x 32 panel, row major, ld DG_LD
+    __shared__ double Z0[32 * DG_LD], Z1[32 * DG_LD];
+    __shared__ double Sx[8][8 * DG_LD];
+    __shared__ double dsh[32];
+    __shared__ int npiv;
+    const int k = list[blockIdx.x];
+    const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+    const int st = s.cb_stride[k];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
+    T *A = L + s.cb_coef[k];
+    T *gZ = dinv + s.cb_dinv[k];
+    const int nzb = (nc + 31) / 32;
+    if (tid == 0) npiv = 0;
+    if (FACT == FACT_GETRF) {  // L_kk += (U^T)_kk^T : the full diagonal block
+        const T *Ut = U + s.cb_coef[k];
+        batched_copy<8, T>(
+            nc * nc, [&](int e) { int i = e % nc, j = e / nc; return A[i + (size_t)j * st] + Ut[j + (size_t)i * st]; },
+            [&](int e, T v) { int i = e % nc, j = e / nc; A[i + (size_t)j * st] = v; });
+    }
+    __syncthreads();
+    for (int jb = 0; jb < nc; jb += 32) {
+        const int nb = min(32, nc - jb), m = nc - jb, t = m - nb;
+        T *Ap = A + jb + (size_t)jb * st;  // top-left corner of the panel
+        dg_copy<4>(
+            m, 32, [&](int r, int c) { return (c < nb) ? (double)Ap[r + (size_t)c * st] : 0.0; },
+            [&](int r, int c, double v) { W[r * DG_LD + c] = v; });
+        __syncthreads();
+        // 2. factor the top block (warp 0), one row per lane in registers
+        if (warp == 0) {
+            double r[32];
+#pragma unroll
+            for (int j = 0; j < 32; j++)
+                r[j] = (lane < nb && j < nb) ? W[lane * DG_LD + j] : (lane == j ? 1.0 : 0.0);
+            int np = 0;
+#pragma unroll
+            for (int c = 0; c < 32; c++) {
+                if (c < nb) {
+                    const double d = static_pivot<double, FACT>(__shfl_sync(0xffffffffu, r[c], c), fp.criterion, np);
+                    const double inv = 1.0 / d;
+                    const double u = r[c];
+                    if (lane == c) r[c] = d;
+                    else if (lane > c) r[c] *= inv;
+#pragma unroll
+                    for (int j = c + 1; j < 32; j++) {
+                        if (j < nb) {
+                            if (FACT == FACT_POTRF) {
+                                const double ljc = __shfl_sync(0xffffffffu, r[c], j);
+                                if (lane >= j) r[j] -= r[c] * ljc;
+                            } else if (FACT == FACT_SYTRF) {
+                                const double ujc = __shfl_sync(0xffffffffu, u, j);
+                                if (lane >= j) r[j] -= r[c] * ujc;
+                            } else {
+                                const double ucj = __shfl_sync(0xffffffffu, r[j], c);
+                                if (lane > c) r[j] -= r[c] * ucj;
+                            }
+                        }
+                    }
+                }
+            }
+            if (lane < nb)
+#pragma unroll
+                for (int j = 0; j < 32; j++)
+                    if (j < nb) W[lane * DG_LD + j] = r[j];
+            if (lane == 0 && np) npiv += np;
+        }
+        __syncthreads();
+        if (warp == 0) dg_inverse<T, FACT>(W, nb, 0, Z0, gZ + (size_t)(jb / 32) * 1024);
+        if (FACT == FACT_GETRF && warp == 1) dg_inverse<T, FACT>(W, nb, 1, Z1, gZ + (size_t)(nzb + jb / 32) * 1024);
+        if (FACT == FACT_SYTRF && tid < 32) dsh[tid] = (tid < nb) ? W[tid * DG_LD + tid] : 0.0;
+        __syncthreads();
+        // 3. rows below the block (and the U strip of GETRF), 8 rows per warp
+        const int nrf = (t + 7) / 8;
+        for (int i = warp; i < nrf; i += 8) {
+            const int r0 = 32 + 8 * i;
+            dg_solve8(
+                [&](int row, int col) { return (r0 + row < m) ? W[(r0 + row) * DG_LD + col] : 0.0; },
+                [&](int a, int b) { return (a <= b && b < nb) ? dg_t<FACT>(W, a, b, 0) : 0.0; }, Z0, Sx[warp],
+                [&](int row, int col, double v) {
+                    if (r0 + row < m) W[(r0 + row) * DG_LD + col] = v;
+                });
+        }
+        if (FACT == FACT_GETRF) {  // U12^T (t x 32, columns of the panel's upper part) X L11^T = U12^T
+            for (int i = warp; i < nrf; i += 8) {
+                const int q0 = 32 + 8 * i;
+                dg_solve8(
+                    [&](int row, int col) {
+                        return (q0 + row < m) ? (double)Ap[col + (size_t)(q0 + row) * st] : 0.0;
+                    },
+                    [&](int a, int b) { return (a <= b && b < nb) ? dg_t<FACT>(W, a, b, 1) : 0.0; }, Z1, Sx[warp],
+                    [&](int row, int col, double v) {
+                        if (q0 + row < m) Ap[col + (size_t)(q0 + row) * st] = (T)v;
+                    });
+            }
+        }
+        __syncthreads();
+        dg_copy<4>(
+            m, nb, [&](int r, int c) { return W[r * DG_LD + c]; },
+            [&](int r, int c, double v) { Ap[r + (size_t)c * st] = (T)v; });
+        // 4. trailing update A22 -= L21 B^T in 16 x 16 blocks (B = L21, L21 D or U12^T)
+        if (t > 0) {
+            T *C = Ap + 32 + (size_t)32 * st;
+            const int nbk = (t + 15) / 16;
+            const int tot = (FACT == FACT_GETRF) ? nbk * nbk : nbk * (nbk + 1) / 2;
+            for (int id = warp; id < tot; id += 8) {
+                int bi, bj;
+                if (FACT == FACT_GETRF) {
+                    bi = id % nbk;
+                    bj = id / nbk;
+                } else {
+                    bi = (int)((sqrt(8.0 * id + 1.0) - 1.0) * 0.5);
+                    while (bi * (bi + 1) / 2 > id) bi--;
+                    while ((bi + 1) * (bi + 2) / 2 <= id) bi++;
+                    bj = id - bi * (bi + 1) / 2;
+                }
+                double c[2][2][2];
+#pragma unroll
+                for (int rf = 0; rf < 2; rf++)
+#pragma unroll
+                    for (int cf = 0; cf < 2; cf++)
+#pragma unroll
+                        for (int e = 0; e < 2; e++) {
+                            const int r = 16 * bi + 8 * rf + g, q = 16 * bj + 8 * cf + 2 * t4 + e;
+                            const bool ok = r < t && q < t && (FACT == FACT_GETRF || r >= q);
+                            c[rf][cf][e] = ok ? (double)C[r + (size_t)q * st] : 0.0;
+                        }
+#pragma unroll
+                for (int ks = 0; ks < 8; ks++) {
+                    const int kk = 4 * ks + t4;
+                    double a[2], b[2];
+#pragma unroll
+                    for (int rf = 0; rf < 2; rf++) {
+                        const int r = 16 * bi + 8 * rf + g;
+                        a[rf] = (r < t) ? -W[(32 + r) * DG_LD + kk] : 0.0;
+                    }
+#pragma unroll
+                    for (int cf = 0; cf < 2; cf++) {
+                        const int q = 16 * bj + 8 * cf + g;
+                        if (FACT == FACT_GETRF) b[cf] = (q < t) ? (double)Ap[kk + (size_t)(32 + q) * st] : 0.0;
+                        else if (FACT == FACT_SYTRF) b[cf] = (q < t) ? W[(32 + q) * DG_LD + kk] * dsh[kk] : 0.0;
+                        else b[cf] = (q < t) ? W[(32 + q) * DG_LD + kk] : 0.0;
+                    }
+#pragma unroll
+                    for (int rf = 0; rf < 2; rf++)
+#pragma unroll
+                        for (int cf = 0; cf < 2; cf++) dmma884(c[rf][cf][0], c[rf][cf][1], a[rf], b[cf]);
+                }
+#pragma unroll
+                for (int rf = 0; rf < 2; rf++)
+#pragma unroll
+                    for (int cf = 0; cf < 2; cf++)
+#pragma unroll
+                        for (int e = 0; e < 2; e++) {
+                            const int r = 16 * bi + 8 * rf + g, q = 16 * bj + 8 * cf + 2 * t4 + e;
+                            if (r < t && q < t && (FACT == FACT_GETRF || r >= q)) C[r + (size_t)q * st] = (T)c[rf][cf][e];
+                        }
+            }
+        }
+        __syncthreads();
+    }
+    if (FACT == FACT_SYTRF) {  // upper part of the diagonal block holds D L^T
+        batched_copy<8, T>(
+            nc * nc,
+            [&](int e) {
+                int i = e % nc, j = e / nc;
+                return (i < j) ? A[i + (size_t)i * st] * A[j + (size_t)i * st] : T(0);
+            },
+            [&](int e, T v) { int i = e % nc, j = e / nc; if (i < j) A[i + (size_t)j * st] = v; });
+    }
+    if (FACT == FACT_GETRF) {  // (U^T)_kk = (L\U)_kk^T
+        T *Ut = U + s.cb_coef[k];
+        batched_copy<8, T>(
+            nc * nc, [&](int e) { int i = e % nc, j = e / nc; return A[i + (size_t)j * st]; },
+            [&](int e, T v) { int i = e % nc, j = e / nc; Ut[j + (size_t)i * st] = v; });
+    }
+    if (tid == 0 && npiv) atomicAdd(fp.nbpivots, npiv);
+}
+
+// ---------------------------------------------------------------------------
 // Host launch wrappers (called from the driver with level lists in device memory)
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -842,18 +1318,24 @@ void launch_panel_small(const DevStruct &s, const int *list, int count, size_t s
 }
 
 template <typename T, int FACT>
-void launch_diag_large(const DevStruct &s, const int *list, int count, size_t smem, T *L, T *U, T *dinv,
+void launch_diag_large(const DevStruct &s, const int *list, int count, int maxnc, size_t smem, T *L, T *U, T *dinv,
                        const FactParams &fp, cudaStream_t st) {
     if (count <= 0) return;
-    k_diag_large<T, FACT><<<count, 256, smem, st>>>(s, list, L, U, dinv, fp);
+    if (maxnc <= DG_MAXNC)
+        k_diag_dmma<T, FACT><<<count, 256, (size_t)diag_dmma_smem_bytes(maxnc), st>>>(s, list, L, U, dinv, fp);
+    else
+        k_diag_large<T, FACT><<<count, 256, smem, st>>>(s, list, L, U, dinv, fp);
 }
 
 template <typename T, int FACT>
-void launch_trsm(const DevStruct &s, const RowTile *tiles, int count, size_t smem, T *L, T *U, const T *dinv,
-                 cudaStream_t st) {
+void launch_trsm(const DevStruct &s, const RowTile *tiles, int count, int maxnc, size_t smem, T *L, T *U,
+                 const T *dinv, cudaStream_t st) {
     if (count <= 0) return;
     dim3 grid(count, FACT == FACT_GETRF ? 2 : 1);
-    k_trsm<T, FACT><<<grid, 256, smem, st>>>(s, tiles, L, U, dinv);
+    if (maxnc <= TD_MAXNC)
+        k_trsm_dmma<T, FACT><<<grid, 256, 0, st>>>(s, tiles, L, U, dinv);
+    else
+        k_trsm<T, FACT><<<grid, 256, smem, st>>>(s, tiles, L, U, dinv);
 }
 
 template <typename T, int FACT>
@@ -893,6 +1375,7 @@ cudaError_t set_smem_attrs(size_t, size_t, size_t) {
     if ((e = opt_in_smem(k_panel_small<T, FACT>)) != cudaSuccess) return e;
     if ((e = opt_in_smem(k_diag_large<T, FACT>)) != cudaSuccess) return e;
     if ((e = opt_in_smem(k_trsm<T, FACT>)) != cudaSuccess) return e;
+    if ((e = opt_in_smem(k_diag_dmma<T, FACT>)) != cudaSuccess) return e;
     if constexpr (sizeof(T) == 8) {
         if ((e = opt_in_smem(k_update_dmma<FACT>)) != cudaSuccess) return e;
     }
@@ -902,9 +1385,9 @@ cudaError_t set_smem_attrs(size_t, size_t, size_t) {
 #define PGPU_INST_FACT(T, F)                                                                                     \
     template void launch_panel_small<T, F>(const DevStruct &, const int *, int, size_t, T *, T *,                \
                                            const FactParams &, cudaStream_t);                                    \
-    template void launch_diag_large<T, F>(const DevStruct &, const int *, int, size_t, T *, T *, T *,            \
+    template void launch_diag_large<T, F>(const DevStruct &, const int *, int, int, size_t, T *, T *, T *,       \
                                           const FactParams &, cudaStream_t);                                     \
-    template void launch_trsm<T, F>(const DevStruct &, const RowTile *, int, size_t, T *, T *, const T *,        \
+    template void launch_trsm<T, F>(const DevStruct &, const RowTile *, int, int, size_t, T *, T *, const T *,   \
                                     cudaStream_t);                                                               \
     template void launch_update<T, F>(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);          \
     template void launch_update_big<T, F>(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);      \

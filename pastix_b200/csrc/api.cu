@@ -45,6 +45,8 @@ template <typename T, int F>
 void launch_update(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);
 template <typename T, int F>
 void launch_update_big(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);
+template <int F>
+void launch_update_tc(const DevStruct &, const UpdTile *, int, float *, float *, int *, cudaStream_t);
 template <typename T, int F>
 cudaError_t set_smem_attrs(size_t, size_t, size_t);
 // solve.cu
@@ -135,6 +137,7 @@ struct LevelLists {
     int trsm0, trsm1;       // k_trsm row tiles
     int upd0, upd1;         // k_update tiles (64 x 64)
     int updb0, updb1;       // big update tiles (128 x 64): DMMA for FP64
+    int updt0, updt1;       // the same tasks in 128 x 128 tiles: tcgen05 for FP32
     int cb0, cb1;           // all cblks of the level (solve diag)
     int st0, st1;           // solve row tiles
     int maxnc;
@@ -153,7 +156,7 @@ struct Device {
     DBuf<pgpu::TaskDev> tasks;
     DBuf<int> small_list, large_list, level_cblks;
     DBuf<pgpu::RowTile> trsm_tiles, solve_tiles;
-    DBuf<pgpu::UpdTile> upd_tiles, upd_big_tiles;
+    DBuf<pgpu::UpdTile> upd_tiles, upd_big_tiles, upd_tc_tiles;
     // matrix
     DBuf<double> vals, csr_val;
     DBuf<int64_t> lmap, umap, csr_src, perm;
@@ -200,7 +203,7 @@ struct pastix_data_s {
     // host copies of the launch lists
     std::vector<int> small_list, large_list, level_cblks;
     std::vector<pgpu::RowTile> trsm_tiles, solve_tiles;
-    std::vector<pgpu::UpdTile> upd_tiles, upd_big_tiles;
+    std::vector<pgpu::UpdTile> upd_tiles, upd_big_tiles, upd_tc_tiles;
     std::vector<pgpu::TaskDev> tasks;
     std::vector<int64_t> cb_dinv;
     int64_t dinv_total = 0;
@@ -627,6 +630,7 @@ static int build_maps_and_lists(pastix_data_t *pd) {
     pd->levels.assign(sv.nlevels, LevelLists{});
     pd->small_list.clear(); pd->large_list.clear(); pd->level_cblks.clear();
     pd->trsm_tiles.clear(); pd->solve_tiles.clear(); pd->upd_tiles.clear(); pd->upd_big_tiles.clear();
+    pd->upd_tc_tiles.clear();
     // exclusive tasks: dst targeted by a single source in the level
     pd->tasks.resize(sv.tasks.size());
     {
@@ -695,6 +699,7 @@ static int build_maps_and_lists(pastix_data_t *pd) {
         L.st1 = (int)pd->solve_tiles.size();
         L.upd0 = (int)pd->upd_tiles.size();
         L.updb0 = (int)pd->upd_big_tiles.size();
+        L.updt0 = (int)pd->upd_tc_tiles.size();
         for (idx_t t = sv.lvl_task_ptr[l]; t < sv.lvl_task_ptr[l + 1]; t++) {
             const auto &tk = sv.tasks[t];
             const idx_t K = sv.cb_lcol[tk.src] - sv.cb_fcol[tk.src] + 1;
@@ -711,10 +716,20 @@ static int build_maps_and_lists(pastix_data_t *pd) {
                         if (fk != pgpu::FACT_GETRF && (a + 1) * BM <= c * BN) continue;
                         list.push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
                     }
+                if (big) {  // 128 x 128 tiles of the tcgen05 kernel (FP32 factors)
+                    const idx_t TB = 128;
+                    const idx_t mt2 = (M + TB - 1) / TB, nt2 = (tk.n + TB - 1) / TB;
+                    for (idx_t a = 0; a < mt2; a++)
+                        for (idx_t c = 0; c < nt2; c++) {
+                            if (fk != pgpu::FACT_GETRF && (a + 1) * TB <= c * TB) continue;
+                            pd->upd_tc_tiles.push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
+                        }
+                }
             }
         }
         L.upd1 = (int)pd->upd_tiles.size();
         L.updb1 = (int)pd->upd_big_tiles.size();
+        L.updt1 = (int)pd->upd_tc_tiles.size();
     }
     return PASTIX_SUCCESS;
 }
@@ -832,6 +847,7 @@ static int device_setup(pastix_data_t *pd) {
     CUDA_TRY(d.solve_tiles.upload(pd->solve_tiles, st));
     CUDA_TRY(d.upd_tiles.upload(pd->upd_tiles, st));
     CUDA_TRY(d.upd_big_tiles.upload(pd->upd_big_tiles, st));
+    CUDA_TRY(d.upd_tc_tiles.upload(pd->upd_tc_tiles, st));
     CUDA_TRY(d.lmap.upload(pd->lmap, st));
     if (!pd->umap.empty()) CUDA_TRY(d.umap.upload(pd->umap, st));
     else d.umap.reset();
@@ -900,9 +916,16 @@ static int run_factor(pastix_data_t *pd, double criterion) {
         launch_cls(pd, PC_UPDATE, lv.upd1 - lv.upd0, [&] {
             pgpu::launch_update<T, F>(d.ds, d.upd_tiles.p + lv.upd0, lv.upd1 - lv.upd0, L, U, st);
         });
-        launch_cls(pd, PC_UPDATE_BIG, lv.updb1 - lv.updb0, [&] {
-            pgpu::launch_update_big<T, F>(d.ds, d.upd_big_tiles.p + lv.updb0, lv.updb1 - lv.updb0, L, U, st);
-        });
+        if constexpr (sizeof(T) == 4) {
+            launch_cls(pd, PC_UPDATE_BIG, lv.updt1 - lv.updt0, [&] {
+                pgpu::launch_update_tc<F>(d.ds, d.upd_tc_tiles.p + lv.updt0, lv.updt1 - lv.updt0, L, U,
+                                          d.counters.p + 1, st);
+            });
+        } else {
+            launch_cls(pd, PC_UPDATE_BIG, lv.updb1 - lv.updb0, [&] {
+                pgpu::launch_update_big<T, F>(d.ds, d.upd_big_tiles.p + lv.updb0, lv.updb1 - lv.updb0, L, U, st);
+            });
+        }
     }
     CUDA_TRY(cudaGetLastError());
     return PASTIX_SUCCESS;

@@ -21,6 +21,8 @@
 // keeping its sign (GETRF, SYTRF), and counted.
 #include "device.cuh"
 
+#include <cuda_bf16.h>
+
 #include <algorithm>
 
 namespace pgpu {
@@ -1300,6 +1302,262 @@ __global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__
 }
 
 // ---------------------------------------------------------------------------
+// FP32 update GEMM with fused scatter-add on the 5th-generation tensor cores
+// (tcgen05.mma kind::f16, accumulator in tensor memory).  Each FP32 operand
+// is split into three BF16 terms a = a0 + a1 + a2 (24 significant bits) and
+// the tile product is accumulated in FP32 from the six terms a_i b_j with
+// i + j <= 2; the three dropped terms are below 2^-24 of the product.
+// Tile 128 x 128 (N narrowed to the task's blok height, rounded up to 16),
+// K by blocks of 64: all 256 threads stage a block (coalesced FP32 loads,
+// split, 16-byte stores in the no-swizzle K-major canonical layout) while the
+// tensor cores work on the previous block; one thread issues the MMAs and a
+// tcgen05.commit per block to that stage's mbarrier.  The epilogue reads the
+// accumulator with tcgen05.ld (one tile row per thread) and scatters it into
+// the facing panel like k_update (core_zgemmsp_2d2d semantics).  Every wait
+// is bounded; on expiry the kernel records PGPU_STATUS_TIMEOUT and returns.
+// ---------------------------------------------------------------------------
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 64;
+constexpr int TC_PIECE = TC_BM * TC_BK * 2;  // bytes of one BF16 operand term (128 rows x 64)
+constexpr int TC_STAGE = 6 * TC_PIECE;       // A0 A1 A2 B0 B1 B2
+constexpr size_t TC_SMEM = 2 * (size_t)TC_STAGE;
+constexpr int TC_SPIN = 1 << 20;             // try_wait rounds before giving up
+constexpr int PGPU_STATUS_TIMEOUT = 3;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared memory matrix descriptor: K-major, no swizzle; core matrices of
+// 8 rows x 16 bytes, the next 8 K elements 128 bytes on (LBO), the next 8 rows
+// 1024 bytes on (SBO); descriptor version 1.
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46);
+}
+// Instruction descriptor: BF16 x BF16 -> FP32, both operands K-major, M = 128, N = n.
+__device__ __forceinline__ uint32_t tc_idesc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+}
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+        "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Bounded wait for the completion of the phase of `bar` with parity `parity`.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (int it = 0; it < TC_SPIN; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
+}
+// a = t0 + t1 + t2 in BF16 (round to nearest at each step), as 16-bit patterns.
+__device__ __forceinline__ void split_bf16x3(float a, uint32_t &t0, uint32_t &t1, uint32_t &t2) {
+    const __nv_bfloat16 h0 = __float2bfloat16_rn(a);
+    float r = a - __bfloat162float(h0);
+    const __nv_bfloat16 h1 = __float2bfloat16_rn(r);
+    r -= __bfloat162float(h1);
+    const __nv_bfloat16 h2 = __float2bfloat16_rn(r);
+    t0 = __bfloat16_as_ushort(h0);
+    t1 = __bfloat16_as_ushort(h1);
+    t2 = __bfloat16_as_ushort(h2);
+}
+
+template <int FACT>
+__global__ void __launch_bounds__(256, 1) k_update_tc(DevStruct s, const UpdTile *__restrict__ tiles, float *L,
+                                                       float *U, int *status) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_sh;
+    __shared__ int rt[TC_BM];
+    __shared__ int ct[TC_BN];
+    const UpdTile tl = tiles[blockIdx.x];
+    const TaskDev tk = s.tasks[tl.task];
+    const int k = tk.src, f = tk.dst;
+    const int K = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+    const int st = s.cb_stride[k];
+    const int shift = tl.side ? tk.n : 0;
+    const int M = tk.m - shift;
+    const int arow = tk.row0 + shift + tl.mt * TC_BM;
+    const int brow = tk.row0 + tl.nt * TC_BN;
+    const int mrows = min(TC_BM, M - tl.mt * TC_BM);
+    const int ncols = min(TC_BN, tk.n - tl.nt * TC_BN);
+    const int nmma = (ncols + 15) & ~15;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const float *Ap = ((FACT == FACT_GETRF && tl.side == 1) ? U : L) + s.cb_coef[k];
+    const float *Bp = ((FACT == FACT_GETRF && tl.side == 0) ? U : L) + s.cb_coef[k];
+    const float *Dk = L + s.cb_coef[k];
+    float *Cp = ((FACT == FACT_GETRF && tl.side == 1) ? U : L) + s.cb_coef[f];
+    const int stf = s.cb_stride[f];
+    if (*(volatile int *)status != 0) return;  // an earlier tile gave up: leave the tensor cores alone
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
+                     "r"(TC_BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    const int *ridx = s.rowidx + s.cb_rowidx[k];
+    if (tid < TC_BM) {
+        int r = -1;
+        if (tid < mrows) {
+            const int g = ridx[arow + tid];
+            int lo = s.cb_fblok[f], hi = s.cb_fblok[f + 1] - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s.bk_frow[mid] <= g) lo = mid;
+                else hi = mid - 1;
+            }
+            r = s.bk_rowoff[lo] + (g - s.bk_frow[lo]);
+        }
+        rt[tid] = r;
+    } else if (tid - TC_BM < TC_BN) {
+        const int c = tid - TC_BM;
+        ct[c] = (c < ncols) ? (ridx[brow + c] - s.cb_fcol[f]) : -1;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_sh;
+    const uint32_t sbase = smem_u32(smem_raw);
+    const uint32_t idesc = tc_idesc(nmma);
+    const int nkb = (K + TC_BK - 1) / TC_BK;
+    int aborted = 0, committed = 0;
+
+    for (int kb = 0; kb < nkb; kb++) {
+        const int sidx = kb & 1;
+        const int late = (kb >= 2 && !mbar_wait(&mbar[sidx], ((kb - 2) >> 1) & 1));
+        // stage K block kb: items (operand, row, 8-column chunk), 8 loads each
+        unsigned char *sp = smem_raw + sidx * TC_STAGE;
+        const int k0 = kb * TC_BK;
+#pragma unroll 2
+        for (int u = 0; u < 8; u++) {
+            const int item = tid + u * 256;
+            const int isB = item >> 10;
+            const int r = item & 127, kc = (item >> 7) & 7;
+            const bool valid = isB ? (r < ncols) : (r < mrows);
+            const float *src = isB ? (Bp + brow + r) : (Ap + arow + r);
+            float v[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int kk = k0 + 8 * kc + j;
+                v[j] = (valid && kk < K) ? src[(size_t)kk * st] : 0.f;
+            }
+            if (FACT == FACT_SYTRF && isB) {
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const int kk = k0 + 8 * kc + j;
+                    if (kk < K) v[j] *= Dk[kk + (size_t)kk * st];
+                }
+            }
+            uint32_t w[3][4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                uint32_t a0, a1, a2, b0, b1, b2;
+                split_bf16x3(v[2 * j], a0, a1, a2);
+                split_bf16x3(v[2 * j + 1], b0, b1, b2);
+                w[0][j] = a0 | (b0 << 16);
+                w[1][j] = a1 | (b1 << 16);
+                w[2][j] = a2 | (b2 << 16);
+            }
+            const int off = (3 * isB) * TC_PIECE + (r >> 3) * 1024 + kc * 128 + (r & 7) * 16;
+#pragma unroll
+            for (int p = 0; p < 3; p++)
+                *reinterpret_cast<uint4 *>(sp + off + p * TC_PIECE) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (__syncthreads_or(late)) {
+            aborted = 1;
+            break;
+        }
+        committed = kb + 1;
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t st0 = sbase + sidx * TC_STAGE;
+#pragma unroll
+            for (int ks = 0; ks < TC_BK / 16; ks++) {
+#pragma unroll
+                for (int p = 0; p < 6; p++) {
+                    const int pa = (p == 2 || p == 4) ? 1 : (p == 5 ? 2 : 0);
+                    const int pb = (p == 1 || p == 4) ? 1 : (p == 3 ? 2 : 0);
+                    tc_mma(tmem, tc_desc(st0 + pa * TC_PIECE + ks * 256), tc_desc(st0 + (3 + pb) * TC_PIECE + ks * 256),
+                           idesc, (kb | ks | p) != 0);
+                }
+            }
+            tc_commit(&mbar[sidx]);
+        }
+    }
+    // all MMAs issued so far have completed once the last commit's phase has
+    if (committed > 0 && !mbar_wait(&mbar[(committed - 1) & 1], ((committed - 1) >> 1) & 1)) aborted = 1;
+    aborted = __syncthreads_or(aborted);
+    tc_fence_after();
+    if (aborted) {
+        if (tid == 0) atomicExch(status, PGPU_STATUS_TIMEOUT);
+    } else {
+        // epilogue: warp w reads accumulator lanes 32 (w % 4) .. + 31, columns 64 (w / 4) .. + 63
+        const int sub = warp & 3, half = warp >> 2;
+        const int row = 32 * sub + lane;
+        const int rr = rt[row];
+        const uint32_t taddr = tmem + ((uint32_t)(32 * sub) << 16) + 64 * half;
+#pragma unroll 1
+        for (int c0 = 0; c0 < 64; c0 += 16) {
+            if (64 * half + c0 >= ncols) break;
+            float v[16];
+            tmem_ld16(taddr + c0, v);
+            if (rr < 0) continue;
+            float *dst[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                const int cc = ct[64 * half + c0 + j];
+                dst[j] = (cc < 0) ? nullptr : Cp + rr + (size_t)cc * stf;
+            }
+            if (tk.excl) {
+                float old[16];
+#pragma unroll
+                for (int j = 0; j < 16; j++) old[j] = dst[j] ? *dst[j] : 0.f;
+#pragma unroll
+                for (int j = 0; j < 16; j++)
+                    if (dst[j]) *dst[j] = old[j] - v[j];
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; j++)
+                    if (dst[j]) atomicAdd(dst[j], -v[j]);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
+}
+
+// ---------------------------------------------------------------------------
 // Host launch wrappers (called from the driver with level lists in device memory)
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -1354,6 +1612,14 @@ void launch_update_big(const DevStruct &s, const UpdTile *tiles, int count, T *L
         k_update<T, FACT, 128, 64, 16, 8, 4><<<count, 256, 0, st>>>(s, tiles, L, U);
 }
 
+// FP32 updates of 128 x 128 tiles on tcgen05 (split BF16 terms)
+template <int FACT>
+void launch_update_tc(const DevStruct &s, const UpdTile *tiles, int count, float *L, float *U, int *status,
+                      cudaStream_t st) {
+    if (count <= 0) return;
+    k_update_tc<FACT><<<count, 256, TC_SMEM, st>>>(s, tiles, L, U, status);
+}
+
 // Opt every kernel with dynamic shared memory into the largest size the
 // device allows next to its static shared memory.
 template <typename K>
@@ -1378,6 +1644,8 @@ cudaError_t set_smem_attrs(size_t, size_t, size_t) {
     if ((e = opt_in_smem(k_diag_dmma<T, FACT>)) != cudaSuccess) return e;
     if constexpr (sizeof(T) == 8) {
         if ((e = opt_in_smem(k_update_dmma<FACT>)) != cudaSuccess) return e;
+    } else {
+        if ((e = opt_in_smem(k_update_tc<FACT>)) != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
@@ -1399,6 +1667,12 @@ PGPU_INST_FACT(double, FACT_GETRF)
 PGPU_INST_FACT(float, FACT_POTRF)
 PGPU_INST_FACT(float, FACT_SYTRF)
 PGPU_INST_FACT(float, FACT_GETRF)
+template void launch_update_tc<FACT_POTRF>(const DevStruct &, const UpdTile *, int, float *, float *, int *,
+                                           cudaStream_t);
+template void launch_update_tc<FACT_SYTRF>(const DevStruct &, const UpdTile *, int, float *, float *, int *,
+                                           cudaStream_t);
+template void launch_update_tc<FACT_GETRF>(const DevStruct &, const UpdTile *, int, float *, float *, int *,
+                                           cudaStream_t);
 template void launch_fill_coef<double>(int64_t, const double *, const int64_t *, const int64_t *, double *,
                                        double *, cudaStream_t);
 template void launch_fill_coef<float>(int64_t, const double *, const int64_t *, const int64_t *, float *,

@@ -75,3 +75,30 @@ def test_solve(lib, name, fact, small, nrhs):
     px.task_solve(pd, S, x)
     for j in range(nrhs):
         assert backward_error(Af, x[:, j], b[:, j]) < 1e-14
+
+
+# FP32 factors (IPARM_MIXED): every update runs in FP32 (tcgen05 tiles with
+# split BF16 terms for the big tasks, SIMT for the rest), so the factor must
+# agree with the FP64 oracle to FP32 accuracy.  A BF16-only product would
+# miss this bar by two orders of magnitude.
+MIXED_CASES = [("lap20", "POTRF", False), ("cd64", "GETRF", True), ("lap20", "SYTRF", False)]
+
+
+@pytest.mark.parametrize("name,fact,small", MIXED_CASES)
+def test_fp32_factor_accuracy(lib, oracle_mod, name, fact, small):
+    A, grid, _ = gen.workload(name, small=small)
+    pd, S, info = analyse(A, grid, fact, mixed=True)
+    px.task_numfact(pd, S)
+    Lg, Ug = px.get_coeftab(pd, with_u=(fact == "GETRF"))
+    assert Lg.dtype == np.float32
+    sym = oracle_mod.Symbol(info)
+    Ap = oracle_mod.permuted_full(S.full(), info["permtab"])
+    L2, U2, npiv = oracle_mod.factor(sym, Ap, fact, oracle_mod.criterion(Ap))
+    Lo = oracle_mod.to_panels(sym, L2)
+    keep = _mask_compare(fact, info)
+    rel = np.linalg.norm((Lg.astype(np.float64) - Lo)[keep]) / np.linalg.norm(Lo[keep])
+    assert rel < 2e-6, rel
+    if fact == "GETRF":
+        Uo = oracle_mod.to_panels(sym, U2)
+        relu = np.linalg.norm(Ug.astype(np.float64) - Uo) / np.linalg.norm(Uo)
+        assert relu < 2e-6, relu

@@ -209,13 +209,12 @@ def run_b200(args, ws, rank, local):
                              npiv=int(ip[px.iparm.static_pivoting]), launches=launches / args.steps,
                              analyze_s=t_an, clocks=clocks, thflops=info["thflops"])
         # profiled pass (per-class device times) for the roofline of the dominant kernel
-        if mode == "fp64":
-            px.profile(pd, True)
-            step()
-            prof = px.profile_get(pd)
-            px.profile(pd, False)
-            results[mode]["profile"] = prof
-            results[mode]["info"] = {k: info[k] for k in ("cb_lcol", "cb_fcol", "cb_stride", "coefnbr")}
+        px.profile(pd, True)
+        step()
+        prof = px.profile_get(pd)
+        px.profile(pd, False)
+        results[mode]["profile"] = prof
+        results[mode]["info"] = {k: info[k] for k in ("cb_lcol", "cb_fcol", "cb_stride", "coefnbr")}
         if mode == "mixed":
             # e2e through the C ABI with host buffers
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -277,7 +276,7 @@ def run_cpu_baseline(args, sample_small: bool):
                 berr=backward_error(Af, x, b), iters=it)
 
 
-def run_probe(s: int) -> int:
+def run_probe(s: int, mixed: bool = False) -> int:
     import torch
     from pastix_b200 import gen
     from pastix_b200 import pastix as px
@@ -286,6 +285,7 @@ def run_probe(s: int) -> int:
     ip, dp = px.initParam()
     ip[px.iparm.factorization] = px.factotype.POTRF
     ip[px.iparm.refinement] = px.refine.CG
+    ip[px.iparm.mixed] = 1 if mixed else 0
     pd = px.init(ip, dp)
     S = spmatrix(A, mtxtype.Symmetric)
     px.analyze_grid(pd, S, s, s, s)
@@ -312,9 +312,10 @@ def main():
     ap.add_argument("--probe", type=int, default=0,
                     help="profiling case: analysis of an N^3 Laplacian then two LL^T FP64 "
                          "factor + solve + CG passes, no timing (used for ncu captures)")
+    ap.add_argument("--probe-mixed", action="store_true", help="the --probe case with FP32 factors")
     args = ap.parse_args()
     if args.probe:
-        return run_probe(args.probe)
+        return run_probe(args.probe, args.probe_mixed)
     args.warmup = max(args.warmup, 3)
 
     ws, rank, local = (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
@@ -383,6 +384,7 @@ def main():
                                     "peaks file)",
                      "launches": upd_launch, "ms_total": upd_ms, "algorithmic_flops": uflops},
         "profile_ms": {k: v[0] for k, v in prof.items() if v[1]},
+        "profile_ms_fp32": {k: v[0] for k, v in mixed["profile"].items() if v[1]},
         "clocks": mixed["clocks"],
         "gpu_launches": int(res[best]["launches"]),
         "e2e": {"value": mixed["e2e"], "unit": "s", "h2d_bytes_per_step": mixed["h2d"],

@@ -324,7 +324,7 @@ int pgpu_solve_device_static(pastix_data_t *pastix_data, pastix_int_t nrhs, doub
  * launch with CUDA events on the library stream; pgpu_profile(pd, 0) resets
  * and only counts.  pgpu_profile_get returns, per kernel class (fill, panel,
  * diag, trsm, update, fwd diag, fwd update, bwd update, bwd diag, spmv, vec,
- * big update tiles),
+ * big update tiles, BF16 split of FP32 panels),
  * the summed device milliseconds and the launch counts. */
 int pgpu_profile(pastix_data_t *pastix_data, int enable);
 int pgpu_profile_get(pastix_data_t *pastix_data, double *ms, long long *launches, int nclass);

@@ -36,7 +36,7 @@ EXPORTS = [
 
 # kernel classes of pgpu_profile_get, in order
 PROFILE_CLASSES = ["fill", "panel_small", "diag_large", "trsm", "update", "fwd_diag", "fwd_update",
-                   "bwd_update", "bwd_diag", "spmv", "vec", "update_big"]
+                   "bwd_update", "bwd_diag", "spmv", "vec", "update_big", "split"]
 
 
 class spmatrix_t(C.Structure):

@@ -46,7 +46,11 @@ void launch_update(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream
 template <typename T, int F>
 void launch_update_big(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);
 template <int F>
-void launch_update_tc(const DevStruct &, const UpdTile *, int, float *, float *, int *, cudaStream_t);
+void launch_update_tc(const DevStruct &, const UpdTile *, int, float *, float *, const unsigned char *,
+                      const unsigned char *, const int64_t *, int *, cudaStream_t);
+void launch_split(const DevStruct &, const SplitSlab *, int, const float *, const float *, const int64_t *,
+                  unsigned char *, int, cudaStream_t);
+long long split_image_bytes(int nc, int st);
 template <typename T, int F>
 cudaError_t set_smem_attrs(size_t, size_t, size_t);
 // solve.cu
@@ -89,7 +93,7 @@ using pgpu::idx_t;
 // kernel classes for launch accounting (pgpu_profile_get)
 enum : int {
     PC_FILL = 0, PC_PANEL_SMALL, PC_DIAG_LARGE, PC_TRSM, PC_UPDATE, PC_FWD_DIAG, PC_FWD_UPDATE, PC_BWD_UPDATE,
-    PC_BWD_DIAG, PC_SPMV, PC_VEC, PC_UPDATE_BIG, PGPU_NCLASS
+    PC_BWD_DIAG, PC_SPMV, PC_VEC, PC_UPDATE_BIG, PC_SPLIT, PGPU_NCLASS
 };
 
 // ---------------------------------------------------------------------------
@@ -137,7 +141,8 @@ struct LevelLists {
     int trsm0, trsm1;       // k_trsm row tiles
     int upd0, upd1;         // k_update tiles (64 x 64)
     int updb0, updb1;       // big update tiles (128 x 64): DMMA for FP64
-    int updt0, updt1;       // the same tasks in 128 x 128 tiles: tcgen05 for FP32
+    int updt0, updt1;       // the same tasks in 128-row aligned windows: tcgen05 for FP32
+    int spl0, spl1;         // 128-row slabs of the level's cblks split into BF16 terms (FP32)
     int cb0, cb1;           // all cblks of the level (solve diag)
     int st0, st1;           // solve row tiles
     int maxnc;
@@ -152,7 +157,9 @@ struct Device {
     cudaStream_t stream = nullptr;
     // structure
     DBuf<int> cb_fcol, cb_lcol, cb_stride, cb_fblok, bk_frow, bk_lrow, bk_rowoff, bk_fcblk, rowidx;
-    DBuf<int64_t> cb_coef, cb_rowidx, cb_dinv;
+    DBuf<int64_t> cb_coef, cb_rowidx, cb_dinv, sp_off;
+    DBuf<pgpu::SplitSlab> split_slabs;
+    DBuf<unsigned char> img0, img1;  // BF16 images of the FP32 panels (tcgen05 operands)
     DBuf<pgpu::TaskDev> tasks;
     DBuf<int> small_list, large_list, level_cblks;
     DBuf<pgpu::RowTile> trsm_tiles, solve_tiles;
@@ -206,6 +213,9 @@ struct pastix_data_s {
     std::vector<pgpu::UpdTile> upd_tiles, upd_big_tiles, upd_tc_tiles;
     std::vector<pgpu::TaskDev> tasks;
     std::vector<int64_t> cb_dinv;
+    std::vector<int64_t> sp_off;             // byte offset of each cblk's BF16 image (-1: none)
+    int64_t split_total = 0;
+    std::vector<pgpu::SplitSlab> split_slabs;
     int64_t dinv_total = 0;
     int factotype = PastixFactPOTRF;
     int mixed = 0;
@@ -660,6 +670,19 @@ static int build_maps_and_lists(pastix_data_t *pd) {
     const int SR = pgpu::solve_rows_per_tile();
     pd->cb_dinv.assign(sv.cblknbr, -1);
     pd->dinv_total = 0;
+    // BF16 images for the tcgen05 updates (FP32 factors): sources of big tasks
+    pd->sp_off.assign(sv.cblknbr, -1);
+    pd->split_total = 0;
+    pd->split_slabs.clear();
+    for (const auto &tk : sv.tasks) {
+        const idx_t K = sv.cb_lcol[tk.src] - sv.cb_fcol[tk.src] + 1;
+        if (tk.n >= 32 && K >= 32 && pd->sp_off[tk.src] < 0) pd->sp_off[tk.src] = 0;
+    }
+    for (idx_t k = 0; k < sv.cblknbr; k++) {
+        if (pd->sp_off[k] < 0) continue;
+        pd->sp_off[k] = pd->split_total;
+        pd->split_total += pgpu::split_image_bytes((int)(sv.cb_lcol[k] - sv.cb_fcol[k] + 1), (int)sv.cb_stride[k]);
+    }
     for (idx_t l = 0; l < sv.nlevels; l++) {
         LevelLists &L = pd->levels[l];
         L.small0 = (int)pd->small_list.size();
@@ -692,6 +715,13 @@ static int build_maps_and_lists(pastix_data_t *pd) {
             }
             for (idx_t r = nc; r < st; r += SR) pd->solve_tiles.push_back(pgpu::RowTile{(int)k, (int)r});
         }
+        L.spl0 = (int)pd->split_slabs.size();
+        for (idx_t p = sv.lvl_ptr[l]; p < sv.lvl_ptr[l + 1]; p++) {
+            idx_t k = sv.lvl_cblk[p];
+            if (pd->sp_off[k] < 0) continue;
+            for (idx_t r = 0; r < sv.cb_stride[k]; r += 128) pd->split_slabs.push_back(pgpu::SplitSlab{(int)k, (int)r});
+        }
+        L.spl1 = (int)pd->split_slabs.size();
         L.small1 = (int)pd->small_list.size();
         L.large1 = (int)pd->large_list.size();
         L.trsm1 = (int)pd->trsm_tiles.size();
@@ -716,9 +746,10 @@ static int build_maps_and_lists(pastix_data_t *pd) {
                         if (fk != pgpu::FACT_GETRF && (a + 1) * BM <= c * BN) continue;
                         list.push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
                     }
-                if (big) {  // 128 x 128 tiles of the tcgen05 kernel (FP32 factors)
+                if (big) {  // tcgen05 tiles (FP32 factors): 128-row windows aligned to groups of 8 rows
                     const idx_t TB = 128;
-                    const idx_t mt2 = (M + TB - 1) / TB, nt2 = (tk.n + TB - 1) / TB;
+                    const idx_t ra = tk.row0 + (side ? tk.n : 0);
+                    const idx_t mt2 = (ra % 8 + M + TB - 1) / TB, nt2 = (tk.row0 % 8 + tk.n + TB - 1) / TB;
                     for (idx_t a = 0; a < mt2; a++)
                         for (idx_t c = 0; c < nt2; c++) {
                             if (fk != pgpu::FACT_GETRF && (a + 1) * TB <= c * TB) continue;
@@ -848,6 +879,8 @@ static int device_setup(pastix_data_t *pd) {
     CUDA_TRY(d.upd_tiles.upload(pd->upd_tiles, st));
     CUDA_TRY(d.upd_big_tiles.upload(pd->upd_big_tiles, st));
     CUDA_TRY(d.upd_tc_tiles.upload(pd->upd_tc_tiles, st));
+    CUDA_TRY(d.sp_off.upload(pd->sp_off, st));
+    if (!pd->split_slabs.empty()) CUDA_TRY(d.split_slabs.upload(pd->split_slabs, st));
     CUDA_TRY(d.lmap.upload(pd->lmap, st));
     if (!pd->umap.empty()) CUDA_TRY(d.umap.upload(pd->umap, st));
     else d.umap.reset();
@@ -917,9 +950,16 @@ static int run_factor(pastix_data_t *pd, double criterion) {
             pgpu::launch_update<T, F>(d.ds, d.upd_tiles.p + lv.upd0, lv.upd1 - lv.upd0, L, U, st);
         });
         if constexpr (sizeof(T) == 4) {
+            launch_cls(pd, PC_SPLIT, lv.spl1 - lv.spl0, [&] {
+                const pgpu::SplitSlab *sl = d.split_slabs.p + lv.spl0;
+                const int cnt = lv.spl1 - lv.spl0;
+                pgpu::launch_split(d.ds, sl, cnt, L, L, d.sp_off.p, d.img0.p, 0, st);
+                if (F == pgpu::FACT_SYTRF) pgpu::launch_split(d.ds, sl, cnt, L, L, d.sp_off.p, d.img1.p, 1, st);
+                if (F == pgpu::FACT_GETRF) pgpu::launch_split(d.ds, sl, cnt, U, L, d.sp_off.p, d.img1.p, 0, st);
+            });
             launch_cls(pd, PC_UPDATE_BIG, lv.updt1 - lv.updt0, [&] {
-                pgpu::launch_update_tc<F>(d.ds, d.upd_tc_tiles.p + lv.updt0, lv.updt1 - lv.updt0, L, U,
-                                          d.counters.p + 1, st);
+                pgpu::launch_update_tc<F>(d.ds, d.upd_tc_tiles.p + lv.updt0, lv.updt1 - lv.updt0, L, U, d.img0.p,
+                                          d.img1.p, d.sp_off.p, d.counters.p + 1, st);
             });
         } else {
             launch_cls(pd, PC_UPDATE_BIG, lv.updb1 - lv.updb0, [&] {
@@ -1016,6 +1056,22 @@ extern "C" int pastix_subtask_bcsc2ctab(pastix_data_t *pd) {
     const size_t dbytes = (size_t)std::max<int64_t>(1, pd->dinv_total) * fs;
     if (d.dinv.n != dbytes) CUDA_TRY(d.dinv.alloc(dbytes));
     d.fltsize = fs;
+    if (pd->mixed && pd->split_total > 0) {  // BF16 images: padding must read as zero, so clear on (re)allocation
+        const size_t sb = (size_t)pd->split_total;
+        const int nimg = (fk == pgpu::FACT_POTRF) ? 1 : 2;
+        if (d.img0.n != sb) {
+            CUDA_TRY(d.img0.alloc(sb));
+            CUDA_TRY(cudaMemsetAsync(d.img0.p, 0, sb, d.stream));
+        }
+        if (nimg == 2 && d.img1.n != sb) {
+            CUDA_TRY(d.img1.alloc(sb));
+            CUDA_TRY(cudaMemsetAsync(d.img1.p, 0, sb, d.stream));
+        }
+        if (nimg == 1) d.img1.reset();
+    } else {
+        d.img0.reset();
+        d.img1.reset();
+    }
     CUDA_TRY(cudaMemsetAsync(d.Lc.p, 0, bytes, d.stream));
     if (d.Uc.p) CUDA_TRY(cudaMemsetAsync(d.Uc.p, 0, bytes, d.stream));
     const int64_t *um = d.Uc.p ? d.umap.p : nullptr;

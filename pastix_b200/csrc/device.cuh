@@ -48,6 +48,12 @@ struct RowTile {
     int r0;           // first panel row of the tile (>= width: below the diagonal block)
 };
 
+// A slab of 128 panel rows of one cblk, split into BF16 terms by k_split.
+struct SplitSlab {
+    int cblk;
+    int r0;
+};
+
 struct DevStruct {
     int n;
     int cblknbr;

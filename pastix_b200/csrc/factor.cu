@@ -1303,34 +1303,51 @@ __global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__
 
 // ---------------------------------------------------------------------------
 // FP32 update GEMM with fused scatter-add on the 5th-generation tensor cores
-// (tcgen05.mma kind::f16, accumulator in tensor memory).  Each FP32 operand
-// is split into three BF16 terms a = a0 + a1 + a2 (24 significant bits) and
-// the tile product is accumulated in FP32 from the six terms a_i b_j with
-// i + j <= 2; the three dropped terms are below 2^-24 of the product.
-// Tile 128 x 128 (N narrowed to the task's blok height, rounded up to 16),
-// K by blocks of 64: all 256 threads stage a block (coalesced FP32 loads,
-// split, 16-byte stores in the no-swizzle K-major canonical layout) while the
-// tensor cores work on the previous block; one thread issues the MMAs and a
-// tcgen05.commit per block to that stage's mbarrier.  The epilogue reads the
+// (tcgen05.mma kind::f16, FP32 accumulator in tensor memory).
+//
+// Operands.  Each FP32 panel value is split once into three BF16 terms
+// a = a0 + a1 + a2 (24 significant bits) by k_split, right after its level's
+// TRSM, into an image laid out exactly as the tensor cores read shared memory
+// (K-major, no swizzle, core matrices of 8 rows x 16 bytes).  The product of a
+// tile is accumulated from the six terms a_i b_j with i + j <= 2; the dropped
+// terms are below 2^-24 of the product.
+//
+// Image of cblk k (bytes from sp_off[k]): term p, K block kb of 32 columns,
+// row group g of 8 panel rows at ((p * nkb + kb) * ng + g) * 512; inside the
+// 512 bytes, column chunk c (8 columns) at 128 c, row r at 16 r, column j at
+// 2 j.  ng = ceil(stride / 8) + 16 so that a window of 16 row groups from any
+// row group of the panel stays inside the (zero padded) image.
+//
+// Tiles.  A task's A rows and B rows are covered by 128-row windows aligned to
+// row groups; rows and columns outside the task are masked in the epilogue.
+// Per K block one thread issues six bulk copies (three terms of A and of B)
+// onto the stage's mbarrier, one thread issues the twelve MMAs and commits
+// them to the stage's "empty" mbarrier; four stages.  The epilogue reads the
 // accumulator with tcgen05.ld (one tile row per thread) and scatters it into
-// the facing panel like k_update (core_zgemmsp_2d2d semantics).  Every wait
+// the facing panel (core_zgemmsp_2d2d semantics, like k_update).  Every wait
 // is bounded; on expiry the kernel records PGPU_STATUS_TIMEOUT and returns.
 // ---------------------------------------------------------------------------
-constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 64;
-constexpr int TC_PIECE = TC_BM * TC_BK * 2;  // bytes of one BF16 operand term (128 rows x 64)
-constexpr int TC_STAGE = 6 * TC_PIECE;       // A0 A1 A2 B0 B1 B2
-constexpr size_t TC_SMEM = 2 * (size_t)TC_STAGE;
-constexpr int TC_SPIN = 1 << 20;             // try_wait rounds before giving up
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32, TC_STAGES = 4;
+constexpr int TC_GROUP = 512;                       // bytes of 8 rows x 32 columns of one term
+constexpr int TC_PIECE = (TC_BM / 8) * TC_GROUP;    // one term of a 128-row operand block
+constexpr int TC_STAGE = 6 * TC_PIECE;              // A0 A1 A2 B0 B1 B2
+constexpr size_t TC_SMEM = (size_t)TC_STAGES * TC_STAGE;
+constexpr int TC_SPIN = 1 << 20;                    // try_wait rounds before giving up
 constexpr int PGPU_STATUS_TIMEOUT = 3;
+
+__host__ __device__ inline int split_nkb(int nc) { return (nc + TC_BK - 1) / TC_BK; }
+__host__ __device__ inline int split_ng(int st) { return (st + 7) / 8 + 16; }
+__host__ __device__ inline long long split_bytes(int nc, int st) {
+    return 3LL * split_nkb(nc) * split_ng(st) * TC_GROUP;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Shared memory matrix descriptor: K-major, no swizzle; core matrices of
-// 8 rows x 16 bytes, the next 8 K elements 128 bytes on (LBO), the next 8 rows
-// 1024 bytes on (SBO); descriptor version 1.
+// Shared memory matrix descriptor: K-major, no swizzle; the next 8 K elements
+// 128 bytes on (LBO), the next 8 rows TC_GROUP bytes on (SBO); version 1.
 __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
-           (1ull << 46);
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
+           ((uint64_t)(TC_GROUP >> 4) << 32) | (1ull << 46);
 }
 // Instruction descriptor: BF16 x BF16 -> FP32, both operands K-major, M = 128, N = n.
 __device__ __forceinline__ uint32_t tc_idesc(int n) {
@@ -1348,6 +1365,9 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar) {
 }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
 // Bounded wait for the completion of the phase of `bar` with parity `parity`.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     const uint32_t a = smem_u32(bar);
@@ -1362,6 +1382,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
         if (done) return true;
     }
     return false;
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Bulk copy global -> shared (this GPU's memory, no multicast), completion on `bar`.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
     uint32_t r[16];
@@ -1386,11 +1416,61 @@ __device__ __forceinline__ void split_bf16x3(float a, uint32_t &t0, uint32_t &t1
     t2 = __bfloat16_as_ushort(h2);
 }
 
+// Split 128-row slabs of FP32 panels into their BF16 image.  `scale` multiplies
+// column c by the diagonal entry D[c][c] of the panel (the L D operand of LDL^T).
+__global__ void __launch_bounds__(256) k_split(DevStruct s, const SplitSlab *__restrict__ slabs, const float *P,
+                                               const float *Dp, const int64_t *__restrict__ sp_off,
+                                               unsigned char *img, int scale) {
+    const SplitSlab sl = slabs[blockIdx.x];
+    const int k = sl.cblk;
+    const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+    const int st = s.cb_stride[k];
+    const int nkb = split_nkb(nc), ng = split_ng(st);
+    const float *A = P + s.cb_coef[k];
+    const float *D = Dp + s.cb_coef[k];
+    unsigned char *out = img + sp_off[k];
+    const int rows = min(128, 8 * ((st + 7) / 8) - sl.r0);  // whole row groups of the panel
+    const int nch = 4 * nkb;                                 // 8-column chunks
+    const int items = 128 * nch;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int r = it & 127, ch = it >> 7;
+        if (r >= rows) continue;
+        const int pr = sl.r0 + r;
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int c = 8 * ch + j;
+            v[j] = (pr < st && c < nc) ? A[pr + (size_t)c * st] : 0.f;
+            if (scale && pr < st && c < nc) v[j] *= D[c + (size_t)c * st];
+        }
+        uint32_t w[3][4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            uint32_t a0, a1, a2, b0, b1, b2;
+            split_bf16x3(v[2 * j], a0, a1, a2);
+            split_bf16x3(v[2 * j + 1], b0, b1, b2);
+            w[0][j] = a0 | (b0 << 16);
+            w[1][j] = a1 | (b1 << 16);
+            w[2][j] = a2 | (b2 << 16);
+        }
+        const size_t base = (size_t)(ch >> 2) * ng * TC_GROUP + (size_t)(pr >> 3) * TC_GROUP + (ch & 3) * 128 +
+                            (pr & 7) * 16;
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+            *reinterpret_cast<uint4 *>(out + base + (size_t)p * nkb * ng * TC_GROUP) =
+                make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
+    }
+}
+
+// imgA / imgB: the BF16 images holding the A and B operands of this kind
+// (POTRF: L, L; SYTRF: L, L D; GETRF: L and U, swapped on the U side).
 template <int FACT>
-__global__ void __launch_bounds__(256, 1) k_update_tc(DevStruct s, const UpdTile *__restrict__ tiles, float *L,
-                                                       float *U, int *status) {
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t mbar[2];
+__global__ void __launch_bounds__(128, 1) k_update_tc(DevStruct s, const UpdTile *__restrict__ tiles, float *L,
+                                                       float *U, const unsigned char *img0,
+                                                       const unsigned char *img1, const int64_t *__restrict__ sp_off,
+                                                       int *status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES], done;
     __shared__ uint32_t tmem_sh;
     __shared__ int rt[TC_BM];
     __shared__ int ct[TC_BN];
@@ -1399,36 +1479,55 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(DevStruct s, const UpdTile
     const int k = tk.src, f = tk.dst;
     const int K = s.cb_lcol[k] - s.cb_fcol[k] + 1;
     const int st = s.cb_stride[k];
-    const int shift = tl.side ? tk.n : 0;
-    const int M = tk.m - shift;
-    const int arow = tk.row0 + shift + tl.mt * TC_BM;
-    const int brow = tk.row0 + tl.nt * TC_BN;
-    const int mrows = min(TC_BM, M - tl.mt * TC_BM);
-    const int ncols = min(TC_BN, tk.n - tl.nt * TC_BN);
-    const int nmma = (ncols + 15) & ~15;
+    const int nkb = split_nkb(K), ng = split_ng(st);
+    const int ra = tk.row0 + (tl.side ? tk.n : 0);  // first A row of the task
+    const int rend = tk.row0 + tk.m;                // end of the A rows
+    const int rb = tk.row0, rbe = tk.row0 + tk.n;   // B rows
+    const int ga = (ra >> 3) + 16 * tl.mt, gb = (rb >> 3) + 16 * tl.nt;
+    const int nbrows = min(TC_BN, rbe - 8 * gb);
+    const int nmma = (nbrows + 15) & ~15;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const float *Ap = ((FACT == FACT_GETRF && tl.side == 1) ? U : L) + s.cb_coef[k];
-    const float *Bp = ((FACT == FACT_GETRF && tl.side == 0) ? U : L) + s.cb_coef[k];
-    const float *Dk = L + s.cb_coef[k];
-    float *Cp = ((FACT == FACT_GETRF && tl.side == 1) ? U : L) + s.cb_coef[f];
+    const bool swap = (FACT == FACT_GETRF && tl.side == 1);
+    const unsigned char *iA = (swap ? img1 : img0) + sp_off[k];
+    const unsigned char *iB = ((FACT == FACT_POTRF) ? img0 : (swap ? img0 : img1)) + sp_off[k];
+    float *Cp = (swap ? U : L) + s.cb_coef[f];
     const int stf = s.cb_stride[f];
-    if (*(volatile int *)status != 0) return;  // an earlier tile gave up: leave the tensor cores alone
+    const size_t term = (size_t)nkb * ng * TC_GROUP;  // bytes between the three terms
+    if (*(volatile int *)status != 0) return;         // an earlier tile gave up: leave the tensor cores alone
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
                      "r"(TC_BN));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
+    const uint32_t bbytes = (uint32_t)(nmma / 8) * TC_GROUP;
+    auto produce = [&](int kb) {
+        const int sidx = kb % TC_STAGES;
+        unsigned char *sp = smem_raw + (size_t)sidx * TC_STAGE;
+        mbar_expect_tx(&full[sidx], 3u * TC_PIECE + 3u * bbytes);
+#pragma unroll
+        for (int p = 0; p < 3; p++) {
+            bulk_g2s(sp + p * TC_PIECE, iA + p * term + ((size_t)kb * ng + ga) * TC_GROUP, TC_PIECE, &full[sidx]);
+            bulk_g2s(sp + (3 + p) * TC_PIECE, iB + p * term + ((size_t)kb * ng + gb) * TC_GROUP, bbytes,
+                     &full[sidx]);
+        }
+    };
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+        for (int i = 0; i < TC_STAGES; i++) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(&done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int kb = 0; kb < min(nkb, TC_STAGES); kb++) produce(kb);
     }
+    // target rows and columns in the facing panel (-1: outside the task)
     const int *ridx = s.rowidx + s.cb_rowidx[k];
-    if (tid < TC_BM) {
+    {
+        const int pr = 8 * ga + tid;
         int r = -1;
-        if (tid < mrows) {
-            const int g = ridx[arow + tid];
+        if (pr >= ra && pr < rend) {
+            const int g = ridx[pr];
             int lo = s.cb_fblok[f], hi = s.cb_fblok[f + 1] - 1;
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
@@ -1438,67 +1537,31 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(DevStruct s, const UpdTile
             r = s.bk_rowoff[lo] + (g - s.bk_frow[lo]);
         }
         rt[tid] = r;
-    } else if (tid - TC_BM < TC_BN) {
-        const int c = tid - TC_BM;
-        ct[c] = (c < ncols) ? (ridx[brow + c] - s.cb_fcol[f]) : -1;
+        const int pc = 8 * gb + tid;
+        ct[tid] = (pc >= rb && pc < rbe) ? (ridx[pc] - s.cb_fcol[f]) : -1;
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_sh;
-    const uint32_t sbase = smem_u32(smem_raw);
-    const uint32_t idesc = tc_idesc(nmma);
-    const int nkb = (K + TC_BK - 1) / TC_BK;
-    int aborted = 0, committed = 0;
-
-    for (int kb = 0; kb < nkb; kb++) {
-        const int sidx = kb & 1;
-        const int late = (kb >= 2 && !mbar_wait(&mbar[sidx], ((kb - 2) >> 1) & 1));
-        // stage K block kb: items (operand, row, 8-column chunk), 8 loads each
-        unsigned char *sp = smem_raw + sidx * TC_STAGE;
-        const int k0 = kb * TC_BK;
-#pragma unroll 2
-        for (int u = 0; u < 8; u++) {
-            const int item = tid + u * 256;
-            const int isB = item >> 10;
-            const int r = item & 127, kc = (item >> 7) & 7;
-            const bool valid = isB ? (r < ncols) : (r < mrows);
-            const float *src = isB ? (Bp + brow + r) : (Ap + arow + r);
-            float v[8];
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const int kk = k0 + 8 * kc + j;
-                v[j] = (valid && kk < K) ? src[(size_t)kk * st] : 0.f;
+    int late = 0;
+    if (tid == 0) {  // producer: the remaining K blocks, each once its stage is released
+        for (int kb = TC_STAGES; kb < nkb; kb++) {
+            if (!mbar_wait(&empty[kb % TC_STAGES], ((kb / TC_STAGES) - 1) & 1)) {
+                late = 1;
+                break;
             }
-            if (FACT == FACT_SYTRF && isB) {
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const int kk = k0 + 8 * kc + j;
-                    if (kk < K) v[j] *= Dk[kk + (size_t)kk * st];
-                }
-            }
-            uint32_t w[3][4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                uint32_t a0, a1, a2, b0, b1, b2;
-                split_bf16x3(v[2 * j], a0, a1, a2);
-                split_bf16x3(v[2 * j + 1], b0, b1, b2);
-                w[0][j] = a0 | (b0 << 16);
-                w[1][j] = a1 | (b1 << 16);
-                w[2][j] = a2 | (b2 << 16);
-            }
-            const int off = (3 * isB) * TC_PIECE + (r >> 3) * 1024 + kc * 128 + (r & 7) * 16;
-#pragma unroll
-            for (int p = 0; p < 3; p++)
-                *reinterpret_cast<uint4 *>(sp + off + p * TC_PIECE) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
+            produce(kb);
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (__syncthreads_or(late)) {
-            aborted = 1;
-            break;
-        }
-        committed = kb + 1;
-        if (tid == 0) {
+    } else if (tid == 32) {  // MMA issuer
+        const uint32_t idesc = tc_idesc(nmma);
+        const uint32_t sbase = smem_u32(smem_raw);
+        for (int kb = 0; kb < nkb; kb++) {
+            const int sidx = kb % TC_STAGES;
+            if (!mbar_wait(&full[sidx], (kb / TC_STAGES) & 1)) {
+                late = 1;
+                break;
+            }
             tc_fence_after();
             const uint32_t st0 = sbase + sidx * TC_STAGE;
 #pragma unroll
@@ -1507,35 +1570,34 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(DevStruct s, const UpdTile
                 for (int p = 0; p < 6; p++) {
                     const int pa = (p == 2 || p == 4) ? 1 : (p == 5 ? 2 : 0);
                     const int pb = (p == 1 || p == 4) ? 1 : (p == 3 ? 2 : 0);
-                    tc_mma(tmem, tc_desc(st0 + pa * TC_PIECE + ks * 256), tc_desc(st0 + (3 + pb) * TC_PIECE + ks * 256),
-                           idesc, (kb | ks | p) != 0);
+                    tc_mma(tmem, tc_desc(st0 + pa * TC_PIECE + ks * 256),
+                           tc_desc(st0 + (3 + pb) * TC_PIECE + ks * 256), idesc, (kb | ks | p) != 0);
                 }
             }
-            tc_commit(&mbar[sidx]);
+            tc_commit(&empty[sidx]);
         }
+        if (!late) tc_commit(&done);
     }
-    // all MMAs issued so far have completed once the last commit's phase has
-    if (committed > 0 && !mbar_wait(&mbar[(committed - 1) & 1], ((committed - 1) >> 1) & 1)) aborted = 1;
-    aborted = __syncthreads_or(aborted);
+    __syncwarp();
+    if (!mbar_wait(&done, 0)) late = 1;
+    const int aborted = __syncthreads_or(late);
     tc_fence_after();
     if (aborted) {
         if (tid == 0) atomicExch(status, PGPU_STATUS_TIMEOUT);
     } else {
-        // epilogue: warp w reads accumulator lanes 32 (w % 4) .. + 31, columns 64 (w / 4) .. + 63
-        const int sub = warp & 3, half = warp >> 2;
-        const int row = 32 * sub + lane;
+        // epilogue: warp w reads accumulator lanes 32 w .. 32 w + 31, one tile row per thread
+        const int row = 32 * warp + lane;
         const int rr = rt[row];
-        const uint32_t taddr = tmem + ((uint32_t)(32 * sub) << 16) + 64 * half;
+        const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
 #pragma unroll 1
-        for (int c0 = 0; c0 < 64; c0 += 16) {
-            if (64 * half + c0 >= ncols) break;
+        for (int c0 = 0; c0 < nmma; c0 += 16) {
             float v[16];
             tmem_ld16(taddr + c0, v);
             if (rr < 0) continue;
             float *dst[16];
 #pragma unroll
             for (int j = 0; j < 16; j++) {
-                const int cc = ct[64 * half + c0 + j];
+                const int cc = ct[c0 + j];
                 dst[j] = (cc < 0) ? nullptr : Cp + rr + (size_t)cc * stf;
             }
             if (tk.excl) {
@@ -1612,13 +1674,22 @@ void launch_update_big(const DevStruct &s, const UpdTile *tiles, int count, T *L
         k_update<T, FACT, 128, 64, 16, 8, 4><<<count, 256, 0, st>>>(s, tiles, L, U);
 }
 
-// FP32 updates of 128 x 128 tiles on tcgen05 (split BF16 terms)
+// FP32 updates of 128 x 128 tiles on tcgen05 from the split BF16 images
 template <int FACT>
-void launch_update_tc(const DevStruct &s, const UpdTile *tiles, int count, float *L, float *U, int *status,
+void launch_update_tc(const DevStruct &s, const UpdTile *tiles, int count, float *L, float *U,
+                      const unsigned char *img0, const unsigned char *img1, const int64_t *sp_off, int *status,
                       cudaStream_t st) {
     if (count <= 0) return;
-    k_update_tc<FACT><<<count, 256, TC_SMEM, st>>>(s, tiles, L, U, status);
+    k_update_tc<FACT><<<count, 128, TC_SMEM, st>>>(s, tiles, L, U, img0, img1, sp_off, status);
 }
+
+void launch_split(const DevStruct &s, const SplitSlab *slabs, int count, const float *P, const float *D,
+                  const int64_t *sp_off, unsigned char *img, int scale, cudaStream_t st) {
+    if (count <= 0) return;
+    k_split<<<count, 256, 0, st>>>(s, slabs, P, D, sp_off, img, scale);
+}
+
+long long split_image_bytes(int nc, int st) { return split_bytes(nc, st); }
 
 // Opt every kernel with dynamic shared memory into the largest size the
 // device allows next to its static shared memory.
@@ -1667,11 +1738,14 @@ PGPU_INST_FACT(double, FACT_GETRF)
 PGPU_INST_FACT(float, FACT_POTRF)
 PGPU_INST_FACT(float, FACT_SYTRF)
 PGPU_INST_FACT(float, FACT_GETRF)
-template void launch_update_tc<FACT_POTRF>(const DevStruct &, const UpdTile *, int, float *, float *, int *,
+template void launch_update_tc<FACT_POTRF>(const DevStruct &, const UpdTile *, int, float *, float *,
+                                           const unsigned char *, const unsigned char *, const int64_t *, int *,
                                            cudaStream_t);
-template void launch_update_tc<FACT_SYTRF>(const DevStruct &, const UpdTile *, int, float *, float *, int *,
+template void launch_update_tc<FACT_SYTRF>(const DevStruct &, const UpdTile *, int, float *, float *,
+                                           const unsigned char *, const unsigned char *, const int64_t *, int *,
                                            cudaStream_t);
-template void launch_update_tc<FACT_GETRF>(const DevStruct &, const UpdTile *, int, float *, float *, int *,
+template void launch_update_tc<FACT_GETRF>(const DevStruct &, const UpdTile *, int, float *, float *,
+                                           const unsigned char *, const unsigned char *, const int64_t *, int *,
                                            cudaStream_t);
 template void launch_fill_coef<double>(int64_t, const double *, const int64_t *, const int64_t *, double *,
                                        double *, cudaStream_t);

@@ -1312,23 +1312,26 @@ __global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__
 // tile is accumulated from the six terms a_i b_j with i + j <= 2; the dropped
 // terms are below 2^-24 of the product.
 //
-// Image of cblk k (bytes from sp_off[k]): term p, K block kb of 32 columns,
-// row group g of 8 panel rows at ((p * nkb + kb) * ng + g) * 512; inside the
-// 512 bytes, column chunk c (8 columns) at 128 c, row r at 16 r, column j at
-// 2 j.  ng = ceil(stride / 8) + 16 so that a window of 16 row groups from any
-// row group of the panel stays inside the (zero padded) image.
+// Image of cblk k (bytes from sp_off[k]): term p, K block kb of TC_BK
+// columns, row group g of 8 panel rows at ((p * nkb + kb) * ng + g) * TC_GROUP;
+// inside a group, column chunk c (8 columns) at 128 c, row r at 16 r, column j
+// at 2 j.  ng = ceil(stride / 8) + 16 so that a window of 16 row groups from
+// any row group of the panel stays inside the (zero padded) image.
 //
 // Tiles.  A task's A rows and B rows are covered by 128-row windows aligned to
 // row groups; rows and columns outside the task are masked in the epilogue.
 // Per K block one thread issues six bulk copies (three terms of A and of B)
-// onto the stage's mbarrier, one thread issues the twelve MMAs and commits
-// them to the stage's "empty" mbarrier; four stages.  The epilogue reads the
+// onto the stage's mbarrier, one thread issues the six MMAs per 16 columns and
+// commits them to the stage's "empty" mbarrier.  Two stages of 24 KB keep four
+// CTAs (and their 128-column accumulators, all of tensor memory) on an SM, so
+// one tile's epilogue overlaps the others' MMAs.  The epilogue reads the
 // accumulator with tcgen05.ld (one tile row per thread) and scatters it into
 // the facing panel (core_zgemmsp_2d2d semantics, like k_update).  Every wait
 // is bounded; on expiry the kernel records PGPU_STATUS_TIMEOUT and returns.
 // ---------------------------------------------------------------------------
-constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32, TC_STAGES = 4;
-constexpr int TC_GROUP = 512;                       // bytes of 8 rows x 32 columns of one term
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 16, TC_STAGES = 2;
+constexpr int TC_CH = TC_BK / 8;                    // 8-column chunks per K block
+constexpr int TC_GROUP = 128 * TC_CH;               // bytes of 8 rows x TC_BK columns of one term
 constexpr int TC_PIECE = (TC_BM / 8) * TC_GROUP;    // one term of a 128-row operand block
 constexpr int TC_STAGE = 6 * TC_PIECE;              // A0 A1 A2 B0 B1 B2
 constexpr size_t TC_SMEM = (size_t)TC_STAGES * TC_STAGE;
@@ -1430,7 +1433,7 @@ __global__ void __launch_bounds__(256) k_split(DevStruct s, const SplitSlab *__r
     const float *D = Dp + s.cb_coef[k];
     unsigned char *out = img + sp_off[k];
     const int rows = min(128, 8 * ((st + 7) / 8) - sl.r0);  // whole row groups of the panel
-    const int nch = 4 * nkb;                                 // 8-column chunks
+    const int nch = TC_CH * nkb;                             // 8-column chunks
     const int items = 128 * nch;
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
         const int r = it & 127, ch = it >> 7;
@@ -1453,8 +1456,8 @@ __global__ void __launch_bounds__(256) k_split(DevStruct s, const SplitSlab *__r
             w[1][j] = a1 | (b1 << 16);
             w[2][j] = a2 | (b2 << 16);
         }
-        const size_t base = (size_t)(ch >> 2) * ng * TC_GROUP + (size_t)(pr >> 3) * TC_GROUP + (ch & 3) * 128 +
-                            (pr & 7) * 16;
+        const size_t base = (size_t)(ch / TC_CH) * ng * TC_GROUP + (size_t)(pr >> 3) * TC_GROUP +
+                            (ch % TC_CH) * 128 + (pr & 7) * 16;
 #pragma unroll
         for (int p = 0; p < 3; p++)
             *reinterpret_cast<uint4 *>(out + base + (size_t)p * nkb * ng * TC_GROUP) =
@@ -1465,7 +1468,7 @@ __global__ void __launch_bounds__(256) k_split(DevStruct s, const SplitSlab *__r
 // imgA / imgB: the BF16 images holding the A and B operands of this kind
 // (POTRF: L, L; SYTRF: L, L D; GETRF: L and U, swapped on the U side).
 template <int FACT>
-__global__ void __launch_bounds__(128, 1) k_update_tc(DevStruct s, const UpdTile *__restrict__ tiles, float *L,
+__global__ void __launch_bounds__(128, 4) k_update_tc(DevStruct s, const UpdTile *__restrict__ tiles, float *L,
                                                        float *U, const unsigned char *img0,
                                                        const unsigned char *img1, const int64_t *__restrict__ sp_off,
                                                        int *status) {

@@ -108,6 +108,7 @@ enum : int {
 namespace {
 
 constexpr idx_t SMALL_PANEL_ELEMS = 4096;  // st*nc below which a cblk is factored in one CTA's smem
+constexpr idx_t TC_MIN_K = 32;             // FP32 factors: tasks whose source is this wide go to tcgen05
 
 template <typename X>
 struct DBuf {  // owning device buffer
@@ -139,7 +140,8 @@ struct LevelLists {
     int small0, small1;     // k_panel_small cblks
     int large0, large1;     // k_diag_large cblks
     int trsm0, trsm1;       // k_trsm row tiles
-    int upd0, upd1;         // k_update tiles (64 x 64)
+    int upd0, upd1;         // k_update tiles (64 x 64), FP64 factors
+    int upds0, upds1;       // k_update tiles (64 x 64), FP32 factors (tasks the tcgen05 kernel does not take)
     int updb0, updb1;       // big update tiles (128 x 64): DMMA for FP64
     int updt0, updt1;       // the same tasks in 128-row aligned windows: tcgen05 for FP32
     int spl0, spl1;         // 128-row slabs of the level's cblks split into BF16 terms (FP32)
@@ -163,7 +165,7 @@ struct Device {
     DBuf<pgpu::TaskDev> tasks;
     DBuf<int> small_list, large_list, level_cblks;
     DBuf<pgpu::RowTile> trsm_tiles, solve_tiles;
-    DBuf<pgpu::UpdTile> upd_tiles, upd_big_tiles, upd_tc_tiles;
+    DBuf<pgpu::UpdTile> upd_tiles, upd_big_tiles, upd_tc_tiles, upd_tiles32;
     // matrix
     DBuf<double> vals, csr_val;
     DBuf<int64_t> lmap, umap, csr_src, perm;
@@ -210,7 +212,7 @@ struct pastix_data_s {
     // host copies of the launch lists
     std::vector<int> small_list, large_list, level_cblks;
     std::vector<pgpu::RowTile> trsm_tiles, solve_tiles;
-    std::vector<pgpu::UpdTile> upd_tiles, upd_big_tiles, upd_tc_tiles;
+    std::vector<pgpu::UpdTile> upd_tiles, upd_big_tiles, upd_tc_tiles, upd_tiles32;
     std::vector<pgpu::TaskDev> tasks;
     std::vector<int64_t> cb_dinv;
     std::vector<int64_t> sp_off;             // byte offset of each cblk's BF16 image (-1: none)
@@ -641,6 +643,7 @@ static int build_maps_and_lists(pastix_data_t *pd) {
     pd->small_list.clear(); pd->large_list.clear(); pd->level_cblks.clear();
     pd->trsm_tiles.clear(); pd->solve_tiles.clear(); pd->upd_tiles.clear(); pd->upd_big_tiles.clear();
     pd->upd_tc_tiles.clear();
+    pd->upd_tiles32.clear();
     // exclusive tasks: dst targeted by a single source in the level
     pd->tasks.resize(sv.tasks.size());
     {
@@ -676,7 +679,7 @@ static int build_maps_and_lists(pastix_data_t *pd) {
     pd->split_slabs.clear();
     for (const auto &tk : sv.tasks) {
         const idx_t K = sv.cb_lcol[tk.src] - sv.cb_fcol[tk.src] + 1;
-        if (tk.n >= 32 && K >= 32 && pd->sp_off[tk.src] < 0) pd->sp_off[tk.src] = 0;
+        if (K >= TC_MIN_K && pd->sp_off[tk.src] < 0) pd->sp_off[tk.src] = 0;
     }
     for (idx_t k = 0; k < sv.cblknbr; k++) {
         if (pd->sp_off[k] < 0) continue;
@@ -730,10 +733,12 @@ static int build_maps_and_lists(pastix_data_t *pd) {
         L.upd0 = (int)pd->upd_tiles.size();
         L.updb0 = (int)pd->upd_big_tiles.size();
         L.updt0 = (int)pd->upd_tc_tiles.size();
+        L.upds0 = (int)pd->upd_tiles32.size();
         for (idx_t t = sv.lvl_task_ptr[l]; t < sv.lvl_task_ptr[l + 1]; t++) {
             const auto &tk = sv.tasks[t];
             const idx_t K = sv.cb_lcol[tk.src] - sv.cb_fcol[tk.src] + 1;
-            const bool big = tk.n >= 32 && K >= 32;
+            const bool big = tk.n >= 32 && K >= 32;       // FP64: DMMA tiles
+            const bool tc = K >= TC_MIN_K;                // FP32: tcgen05 tiles
             const idx_t BM = big ? 128 : 64, BN = 64;
             auto &list = big ? pd->upd_big_tiles : pd->upd_tiles;
             for (int side = 0; side < (fk == pgpu::FACT_GETRF ? 2 : 1); side++) {
@@ -746,7 +751,15 @@ static int build_maps_and_lists(pastix_data_t *pd) {
                         if (fk != pgpu::FACT_GETRF && (a + 1) * BM <= c * BN) continue;
                         list.push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
                     }
-                if (big) {  // tcgen05 tiles (FP32 factors): 128-row windows aligned to groups of 8 rows
+                if (!tc) {  // FP32 tasks with a narrow source: SIMT 64 x 64 tiles
+                    const idx_t mt3 = (M + 63) / 64, nt3 = (tk.n + 63) / 64;
+                    for (idx_t a = 0; a < mt3; a++)
+                        for (idx_t c = 0; c < nt3; c++) {
+                            if (fk != pgpu::FACT_GETRF && (a + 1) * 64 <= c * 64) continue;
+                            pd->upd_tiles32.push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
+                        }
+                }
+                if (tc) {  // tcgen05 tiles (FP32 factors): 128-row windows aligned to groups of 8 rows
                     const idx_t TB = 128;
                     const idx_t ra = tk.row0 + (side ? tk.n : 0);
                     const idx_t mt2 = (ra % 8 + M + TB - 1) / TB, nt2 = (tk.row0 % 8 + tk.n + TB - 1) / TB;
@@ -761,6 +774,7 @@ static int build_maps_and_lists(pastix_data_t *pd) {
         L.upd1 = (int)pd->upd_tiles.size();
         L.updb1 = (int)pd->upd_big_tiles.size();
         L.updt1 = (int)pd->upd_tc_tiles.size();
+        L.upds1 = (int)pd->upd_tiles32.size();
     }
     return PASTIX_SUCCESS;
 }
@@ -879,6 +893,7 @@ static int device_setup(pastix_data_t *pd) {
     CUDA_TRY(d.upd_tiles.upload(pd->upd_tiles, st));
     CUDA_TRY(d.upd_big_tiles.upload(pd->upd_big_tiles, st));
     CUDA_TRY(d.upd_tc_tiles.upload(pd->upd_tc_tiles, st));
+    CUDA_TRY(d.upd_tiles32.upload(pd->upd_tiles32, st));
     CUDA_TRY(d.sp_off.upload(pd->sp_off, st));
     if (!pd->split_slabs.empty()) CUDA_TRY(d.split_slabs.upload(pd->split_slabs, st));
     CUDA_TRY(d.lmap.upload(pd->lmap, st));
@@ -946,9 +961,15 @@ static int run_factor(pastix_data_t *pd, double criterion) {
             pgpu::launch_trsm<T, F>(d.ds, d.trsm_tiles.p + lv.trsm0, lv.trsm1 - lv.trsm0, lv.trsm_maxnc,
                                     lv.trsm_smem_elems * sizeof(T), L, U, Dinv, st);
         });
-        launch_cls(pd, PC_UPDATE, lv.upd1 - lv.upd0, [&] {
-            pgpu::launch_update<T, F>(d.ds, d.upd_tiles.p + lv.upd0, lv.upd1 - lv.upd0, L, U, st);
-        });
+        if constexpr (sizeof(T) == 8) {
+            launch_cls(pd, PC_UPDATE, lv.upd1 - lv.upd0, [&] {
+                pgpu::launch_update<T, F>(d.ds, d.upd_tiles.p + lv.upd0, lv.upd1 - lv.upd0, L, U, st);
+            });
+        } else {
+            launch_cls(pd, PC_UPDATE, lv.upds1 - lv.upds0, [&] {
+                pgpu::launch_update<T, F>(d.ds, d.upd_tiles32.p + lv.upds0, lv.upds1 - lv.upds0, L, U, st);
+            });
+        }
         if constexpr (sizeof(T) == 4) {
             launch_cls(pd, PC_SPLIT, lv.spl1 - lv.spl0, [&] {
                 const pgpu::SplitSlab *sl = d.split_slabs.p + lv.spl0;

@@ -173,11 +173,25 @@ __global__ void __launch_bounds__(256) k_fwd_diag_inv(DevStruct s, const int *__
             if (i < nb && j < nr) y[jb + i + j * nc] = yb[e];
         }
         __syncthreads();
-        for (int e = tid; e < (nc - jb - nb) * nr; e += nt) {
-            int i = jb + nb + e % (nc - jb - nb), j = e / (nc - jb - nb);
-            T acc = T(0);
-            for (int c = 0; c < nb; c++) acc += D[i + (size_t)(jb + c) * st] * y[jb + c + j * nc];
-            y[i + j * nc] -= acc;
+        // rows below inside the diagonal block (the block is full when rows remain):
+        // one row per thread, its 32 panel entries loaded together
+        for (int r = jb + 32 + tid; r < nc; r += nt) {
+            T p[32];
+#pragma unroll
+            for (int c = 0; c < 32; c++) p[c] = D[r + (size_t)(jb + c) * st];
+            T acc[RC];
+#pragma unroll
+            for (int j = 0; j < RC; j++) acc[j] = T(0);
+#pragma unroll
+            for (int c = 0; c < 32; c++) {
+                const T pc = p[c];
+#pragma unroll
+                for (int j = 0; j < RC; j++) acc[j] += pc * yb[c + j * 32];
+                asm volatile("" ::: "memory");  // keeps the compiler from hoisting all shared loads ahead
+            }
+#pragma unroll
+            for (int j = 0; j < RC; j++)
+                if (j < nr) y[r + j * nc] -= acc[j];
         }
         __syncthreads();
     }
@@ -187,6 +201,9 @@ __global__ void __launch_bounds__(256) k_fwd_diag_inv(DevStruct s, const int *__
     }
 }
 
+// Backward, right looking inside the diagonal block: once x_j is final its
+// contribution P[block j, c]^T x_j is removed from every earlier column c, one
+// warp per column (coalesced 32-row reads, shuffle reductions).
 template <typename T, int RC>
 __global__ void __launch_bounds__(256) k_bwd_diag_inv(DevStruct s, const int *__restrict__ list, const T *P,
                                                        const T *__restrict__ dinv, int zside, int scaled,
@@ -205,27 +222,24 @@ __global__ void __launch_bounds__(256) k_bwd_diag_inv(DevStruct s, const int *__
     const T *Dl = Ldiag + s.cb_coef[k];
     const int nzb = (nc + 31) / 32;
     const T *gZ = dinv + s.cb_dinv[k] + (size_t)(zside ? nzb : 0) * 1024;
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     for (int e = tid; e < nc * nr; e += nt) {
         int i = e % nc, j = e / nc;
         y[i + j * nc] = Y[(fc + i) + (size_t)(j0 + j) * ldy];
     }
     __syncthreads();
-    const int nblk = (nc + 31) / 32;
-    for (int b = nblk - 1; b >= 0; b--) {
+    for (int b = nzb - 1; b >= 0; b--) {
         const int jb = b * 32;
         const int nb = min(32, nc - jb);
-        const int below = nc - jb - nb;
         for (int e = tid; e < 1024; e += nt) Z[(e >> 5) * 33 + (e & 31)] = gZ[(size_t)b * 1024 + e];
-        for (int e = tid; e < 32 * RC; e += nt) {  // yb = S (x_j - P[below, j]^T x[below])
+        for (int e = tid; e < 32 * RC; e += nt) {  // yb = S x_j (contributions of later blocks already removed)
             int i = e & 31, j = e >> 5;
-            T acc = T(0);
+            T v = T(0);
             if (i < nb && j < nr) {
-                acc = y[jb + i + j * nc];
-                for (int r = 0; r < below; r++) acc -= D[(jb + nb + r) + (size_t)(jb + i) * st] * y[jb + nb + r + j * nc];
-                if (scaled) acc *= Dl[(jb + i) + (size_t)(jb + i) * st];
+                v = y[jb + i + j * nc];
+                if (scaled) v *= Dl[(jb + i) + (size_t)(jb + i) * st];
             }
-            yb[e] = acc;
+            yb[e] = v;
         }
         __syncthreads();
         for (int e = tid; e < 32 * RC; e += nt) {  // x_j = Z yb
@@ -234,6 +248,25 @@ __global__ void __launch_bounds__(256) k_bwd_diag_inv(DevStruct s, const int *__
                 T acc = T(0);
                 for (int c = i; c < nb; c++) acc += Z[i * 33 + c] * yb[c + j * 32];
                 y[jb + i + j * nc] = acc;
+            }
+        }
+        __syncthreads();
+        for (int c0 = 8 * warp; c0 < jb; c0 += nt / 4) {  // x_c -= P[block j, c]^T x_j, 8 columns per warp
+            T p[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                p[u] = (lane < nb && c0 + u < jb) ? D[(jb + lane) + (size_t)(c0 + u) * st] : T(0);
+#pragma unroll
+            for (int j = 0; j < RC; j++) {
+                if (j >= nr) break;
+                const T xv = (lane < nb) ? y[jb + lane + j * nc] : T(0);
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    T v = p[u] * xv;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    if (lane == 0 && c0 + u < jb) y[c0 + u + j * nc] -= v;
+                }
             }
         }
         __syncthreads();

@@ -50,12 +50,19 @@ __global__ void __launch_bounds__(256) k_fwd_diag(DevStruct s, const int *__rest
         {
             const int lane = tid & 31, warp = tid >> 5;
             const T rd = (!unit && lane < nb) ? T(1) / D[(jb + lane) + (size_t)(jb + lane) * st] : T(1);
+            T drow[32];  // row jb + lane of the block, loaded before the dependent sweep
+#pragma unroll
+            for (int c = 0; c < 32; c++)
+                drow[c] = (c < lane && lane < nb) ? D[(jb + lane) + (size_t)(jb + c) * st] : T(0);
             for (int j = warp; j < nr; j += nt / 32) {
                 T v = (lane < nb) ? y[jb + lane + j * nc] : T(0);
-                for (int c = 0; c < nb; c++) {
-                    if (lane == c) v *= rd;
-                    T vc = __shfl_sync(0xffffffffu, v, c);
-                    if (lane > c && lane < nb) v -= D[(jb + lane) + (size_t)(jb + c) * st] * vc;
+#pragma unroll
+                for (int c = 0; c < 32; c++) {
+                    if (c < nb) {
+                        if (lane == c) v *= rd;
+                        const T vc = __shfl_sync(0xffffffffu, v, c);
+                        v -= drow[c] * vc;
+                    }
                 }
                 if (lane < nb) y[jb + lane + j * nc] = v;
             }
@@ -99,12 +106,19 @@ __global__ void __launch_bounds__(256) k_bwd_diag(DevStruct s, const int *__rest
         {
             const int lane = tid & 31, warp = tid >> 5;
             const T rd = (!unit && lane < nb) ? T(1) / D[(jb + lane) + (size_t)(jb + lane) * st] : T(1);
+            T dcol[32];  // column jb + lane of the block, loaded before the dependent sweep
+#pragma unroll
+            for (int c = 0; c < 32; c++)
+                dcol[c] = (lane < c && c < nb) ? D[(jb + c) + (size_t)(jb + lane) * st] : T(0);
             for (int j = warp; j < nr; j += nt / 32) {
                 T v = (lane < nb) ? y[jb + lane + j * nc] : T(0);
-                for (int c = nb - 1; c >= 0; c--) {
-                    if (lane == c) v *= rd;
-                    T vc = __shfl_sync(0xffffffffu, v, c);
-                    if (lane < c) v -= D[(jb + c) + (size_t)(jb + lane) * st] * vc;
+#pragma unroll
+                for (int c = 31; c >= 0; c--) {
+                    if (c < nb) {
+                        if (lane == c) v *= rd;
+                        const T vc = __shfl_sync(0xffffffffu, v, c);
+                        v -= dcol[c] * vc;
+                    }
                 }
                 if (lane < nb) y[jb + lane + j * nc] = v;
             }

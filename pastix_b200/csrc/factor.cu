@@ -1006,6 +1006,7 @@ __global__ void __launch_bounds__(256, 1) k_trsm_dmma(DevStruct s, const RowTile
 // ---------------------------------------------------------------------------
 constexpr int DG_LD = 36;      // shared row stride (doubles): 2 wavefronts per fragment access
 constexpr int DG_MAXNC = 384;
+constexpr int DG_NBLK = 2;     // trailing-update blocks in flight per warp
 
 __host__ __device__ inline long long diag_dmma_smem_bytes(int nc) { return (long long)nc * DG_LD * 8; }
 
@@ -1227,58 +1228,73 @@ __global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__
             T *C = Ap + 32 + (size_t)32 * st;
             const int nbk = (t + 15) / 16;
             const int tot = (FACT == FACT_GETRF) ? nbk * nbk : nbk * (nbk + 1) / 2;
-            for (int id = warp; id < tot; id += 8) {
-                int bi, bj;
-                if (FACT == FACT_GETRF) {
-                    bi = id % nbk;
-                    bj = id / nbk;
-                } else {
-                    bi = (int)((sqrt(8.0 * id + 1.0) - 1.0) * 0.5);
-                    while (bi * (bi + 1) / 2 > id) bi--;
-                    while ((bi + 1) * (bi + 2) / 2 <= id) bi++;
-                    bj = id - bi * (bi + 1) / 2;
-                }
-                double c[2][2][2];
+            // each warp keeps DG_NBLK blocks in flight: their C loads are issued together
+            constexpr int NB = DG_NBLK;
+            for (int id0 = warp; id0 < tot; id0 += 8 * NB) {
+                int bi[NB], bj[NB];
+                double c[NB][2][2][2];
 #pragma unroll
-                for (int rf = 0; rf < 2; rf++)
-#pragma unroll
-                    for (int cf = 0; cf < 2; cf++)
-#pragma unroll
-                        for (int e = 0; e < 2; e++) {
-                            const int r = 16 * bi + 8 * rf + g, q = 16 * bj + 8 * cf + 2 * t4 + e;
-                            const bool ok = r < t && q < t && (FACT == FACT_GETRF || r >= q);
-                            c[rf][cf][e] = ok ? (double)C[r + (size_t)q * st] : 0.0;
-                        }
-#pragma unroll
-                for (int ks = 0; ks < 8; ks++) {
-                    const int kk = 4 * ks + t4;
-                    double a[2], b[2];
-#pragma unroll
-                    for (int rf = 0; rf < 2; rf++) {
-                        const int r = 16 * bi + 8 * rf + g;
-                        a[rf] = (r < t) ? -W[(32 + r) * DG_LD + kk] : 0.0;
+                for (int u = 0; u < NB; u++) {
+                    const int id = id0 + 8 * u;
+                    if (FACT == FACT_GETRF) {
+                        bi[u] = id % nbk;
+                        bj[u] = id / nbk;
+                    } else {
+                        int x = (int)((sqrt(8.0 * id + 1.0) - 1.0) * 0.5);
+                        while (x * (x + 1) / 2 > id) x--;
+                        while ((x + 1) * (x + 2) / 2 <= id) x++;
+                        bi[u] = x;
+                        bj[u] = id - x * (x + 1) / 2;
                     }
-#pragma unroll
-                    for (int cf = 0; cf < 2; cf++) {
-                        const int q = 16 * bj + 8 * cf + g;
-                        if (FACT == FACT_GETRF) b[cf] = (q < t) ? (double)Ap[kk + (size_t)(32 + q) * st] : 0.0;
-                        else if (FACT == FACT_SYTRF) b[cf] = (q < t) ? W[(32 + q) * DG_LD + kk] * dsh[kk] : 0.0;
-                        else b[cf] = (q < t) ? W[(32 + q) * DG_LD + kk] : 0.0;
-                    }
+                    if (id >= tot) bi[u] = bj[u] = nbk;  // no block: every row and column masked
 #pragma unroll
                     for (int rf = 0; rf < 2; rf++)
 #pragma unroll
-                        for (int cf = 0; cf < 2; cf++) dmma884(c[rf][cf][0], c[rf][cf][1], a[rf], b[cf]);
+                        for (int cf = 0; cf < 2; cf++)
+#pragma unroll
+                            for (int e = 0; e < 2; e++) {
+                                const int r = 16 * bi[u] + 8 * rf + g, q = 16 * bj[u] + 8 * cf + 2 * t4 + e;
+                                const bool ok = r < t && q < t && (FACT == FACT_GETRF || r >= q);
+                                c[u][rf][cf][e] = ok ? (double)C[r + (size_t)q * st] : 0.0;
+                            }
                 }
 #pragma unroll
-                for (int rf = 0; rf < 2; rf++)
+                for (int ks = 0; ks < 8; ks++) {
+                    const int kk = 4 * ks + t4;
 #pragma unroll
-                    for (int cf = 0; cf < 2; cf++)
+                    for (int u = 0; u < NB; u++) {
+                        double a[2], b[2];
 #pragma unroll
-                        for (int e = 0; e < 2; e++) {
-                            const int r = 16 * bi + 8 * rf + g, q = 16 * bj + 8 * cf + 2 * t4 + e;
-                            if (r < t && q < t && (FACT == FACT_GETRF || r >= q)) C[r + (size_t)q * st] = (T)c[rf][cf][e];
+                        for (int rf = 0; rf < 2; rf++) {
+                            const int r = 16 * bi[u] + 8 * rf + g;
+                            a[rf] = (r < t) ? -W[(32 + r) * DG_LD + kk] : 0.0;
                         }
+#pragma unroll
+                        for (int cf = 0; cf < 2; cf++) {
+                            const int q = 16 * bj[u] + 8 * cf + g;
+                            if (FACT == FACT_GETRF) b[cf] = (q < t) ? (double)Ap[kk + (size_t)(32 + q) * st] : 0.0;
+                            else if (FACT == FACT_SYTRF) b[cf] = (q < t) ? W[(32 + q) * DG_LD + kk] * dsh[kk] : 0.0;
+                            else b[cf] = (q < t) ? W[(32 + q) * DG_LD + kk] : 0.0;
+                        }
+#pragma unroll
+                        for (int rf = 0; rf < 2; rf++)
+#pragma unroll
+                            for (int cf = 0; cf < 2; cf++)
+                                dmma884(c[u][rf][cf][0], c[u][rf][cf][1], a[rf], b[cf]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < NB; u++)
+#pragma unroll
+                    for (int rf = 0; rf < 2; rf++)
+#pragma unroll
+                        for (int cf = 0; cf < 2; cf++)
+#pragma unroll
+                            for (int e = 0; e < 2; e++) {
+                                const int r = 16 * bi[u] + 8 * rf + g, q = 16 * bj[u] + 8 * cf + 2 * t4 + e;
+                                if (r < t && q < t && (FACT == FACT_GETRF || r >= q))
+                                    C[r + (size_t)q * st] = (T)c[u][rf][cf][e];
+                            }
             }
         }
         __syncthreads();

@@ -21,6 +21,7 @@
 // keeping its sign (GETRF, SYTRF), and counted.
 #include "device.cuh"
 
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -1021,26 +1022,92 @@ __device__ __forceinline__ double dg_t(const double *W, int a, int b, int side) 
 
 // One warp: Z = T_jj^{-1} of the nb x nb leading block (identity beyond), to
 // shared memory (row major, ld DG_LD) and to `gZ` (32 x 32 row major).  Lane j
-// forms column j by back substitution.
+// forms column j by back substitution.  A full block (nb = 32, every block
+// but possibly a cblk's last) runs fully unrolled without guards, so its
+// broadcast reads of T are issued ahead of the dependent sums.  Kept out of
+// line: inlined into the large factorization kernels its 32-entry column
+// would be demoted to local memory.
 template <typename T, int FACT>
-__device__ __forceinline__ void dg_inverse(const double *W, int nb, int side, double *Z, T *gZ) {
+__device__ __noinline__ void dg_inverse(const double *W, int nb, int side, double *Z, T *gZ) {
     const int lane = threadIdx.x & 31;
     const double rl = (lane < nb) ? 1.0 / dg_t<FACT>(W, lane, lane, side) : 1.0;
-    double z[32];
+    if (nb == 32) {
+        double z[32];
 #pragma unroll
-    for (int i = 31; i >= 0; i--) {
+        for (int i = 31; i >= 0; i--) {
+            double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+            for (int kk = i + 1; kk < 32; kk++) {
+                if ((kk - i) & 1) a0 += dg_t<FACT>(W, i, kk, side) * z[kk];
+                else a1 += dg_t<FACT>(W, i, kk, side) * z[kk];
+            }
+            const double ri = __shfl_sync(0xffffffffu, rl, i);
+            z[i] = (i > lane) ? 0.0 : ((i == lane) ? rl : -(a0 + a1) * ri);
+        }
+#pragma unroll
+        for (int i = 0; i < 32; i++) {
+            Z[i * DG_LD + lane] = z[i];
+            gZ[i * 32 + lane] = (T)z[i];
+        }
+        return;
+    }
+    for (int i = 31; i >= 0; i--) {  // partial block: column kept in Z itself
         double acc = 0.0;
-#pragma unroll
-        for (int kk = i + 1; kk < 32; kk++)
-            if (kk < nb) acc += dg_t<FACT>(W, i, kk, side) * z[kk];
+        for (int kk = i + 1; kk < nb; kk++) acc += dg_t<FACT>(W, i, kk, side) * Z[kk * DG_LD + lane];
         const double ri = __shfl_sync(0xffffffffu, rl, i);
-        z[i] = (i > lane) ? 0.0 : ((i == lane) ? rl : -acc * ri);
+        Z[i * DG_LD + lane] = (i > lane) ? 0.0 : ((i == lane) ? rl : -acc * ri);
     }
+    for (int i = 0; i < 32; i++) gZ[i * 32 + lane] = (T)Z[i * DG_LD + lane];
+}
+
+// One warp: factor the nb x nb top block held row major in W (ld DG_LD) in
+// place, one row per lane in registers, with static pivoting; returns the
+// number of replaced pivots.  POTRF leaves L (lower), SYTRF L (unit, strictly
+// lower) and D on the diagonal, GETRF L (unit, strictly lower) and U.  The
+// column (or, for GETRF, the row) of each step reaches the other lanes through
+// the 32-entry shared vector Ls as broadcast reads: a dependent chain of warp
+// shuffles costs several times more per step.
+template <int FACT>
+__device__ __forceinline__ int dg_factor32(double *W, int nb, double crit, double *Ls) {
+    const int lane = threadIdx.x & 31;
+    double r[32];
 #pragma unroll
-    for (int i = 0; i < 32; i++) {
-        Z[i * DG_LD + lane] = z[i];
-        gZ[i * 32 + lane] = (T)z[i];
+    for (int j = 0; j < 32; j++) r[j] = (lane < nb && j < nb) ? W[lane * DG_LD + j] : (lane == j ? 1.0 : 0.0);
+    int np = 0;
+#pragma unroll
+    for (int c = 0; c < 32; c++) {
+        if (c < nb) {
+            const double d = static_pivot<double, FACT>(__shfl_sync(0xffffffffu, r[c], c), crit, np);
+            const double inv = 1.0 / d;
+            const double u = r[c];
+            if (lane == c) r[c] = d;
+            else if (lane > c) r[c] *= inv;
+            if (FACT == FACT_POTRF) Ls[lane] = r[c];
+            else if (FACT == FACT_SYTRF) Ls[lane] = u;
+            else if (lane == c) {
+#pragma unroll
+                for (int j = 0; j < 32; j++) Ls[j] = r[j];
+            }
+            __syncwarp();
+            // no j < nb guard: beyond nb both Ls and the padded lanes' entries are zero,
+            // and an unguarded loop lets the 31 broadcast reads issue back to back
+#pragma unroll
+            for (int j = c + 1; j < 32; j++) {
+                const double v = Ls[j];
+                if (FACT == FACT_GETRF) {
+                    if (lane > c) r[j] -= r[c] * v;
+                } else if (lane >= j) {
+                    r[j] -= r[c] * v;
+                }
+            }
+            __syncwarp();
+        }
     }
+    if (lane < nb)
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+            if (j < nb) W[lane * DG_LD + j] = r[j];
+    return np;
 }
 
 // CTA-wide transfer of a rows x cols region in 8 x 4 sub-tiles: lane (g, t4)
@@ -1128,7 +1195,7 @@ __global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__
     double *W = reinterpret_cast<double *>(smem_raw);  // (nc - jb) x 32 panel, row major, ld DG_LD
     __shared__ double Z0[32 * DG_LD], Z1[32 * DG_LD];
     __shared__ double Sx[8][8 * DG_LD];
-    __shared__ double dsh[32];
+    __shared__ double dsh[32], Ls[32];
     __shared__ int npiv;
     const int k = list[blockIdx.x];
     const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
@@ -1154,40 +1221,7 @@ __global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__
         __syncthreads();
         // 2. factor the top block (warp 0), one row per lane in registers
         if (warp == 0) {
-            double r[32];
-#pragma unroll
-            for (int j = 0; j < 32; j++)
-                r[j] = (lane < nb && j < nb) ? W[lane * DG_LD + j] : (lane == j ? 1.0 : 0.0);
-            int np = 0;
-#pragma unroll
-            for (int c = 0; c < 32; c++) {
-                if (c < nb) {
-                    const double d = static_pivot<double, FACT>(__shfl_sync(0xffffffffu, r[c], c), fp.criterion, np);
-                    const double inv = 1.0 / d;
-                    const double u = r[c];
-                    if (lane == c) r[c] = d;
-                    else if (lane > c) r[c] *= inv;
-#pragma unroll
-                    for (int j = c + 1; j < 32; j++) {
-                        if (j < nb) {
-                            if (FACT == FACT_POTRF) {
-                                const double ljc = __shfl_sync(0xffffffffu, r[c], j);
-                                if (lane >= j) r[j] -= r[c] * ljc;
-                            } else if (FACT == FACT_SYTRF) {
-                                const double ujc = __shfl_sync(0xffffffffu, u, j);
-                                if (lane >= j) r[j] -= r[c] * ujc;
-                            } else {
-                                const double ucj = __shfl_sync(0xffffffffu, r[j], c);
-                                if (lane > c) r[j] -= r[c] * ucj;
-                            }
-                        }
-                    }
-                }
-            }
-            if (lane < nb)
-#pragma unroll
-                for (int j = 0; j < 32; j++)
-                    if (j < nb) W[lane * DG_LD + j] = r[j];
+            const int np = dg_factor32<FACT>(W, nb, fp.criterion, Ls);
             if (lane == 0 && np) npiv += np;
         }
         __syncthreads();
@@ -1314,6 +1348,210 @@ __global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__
             nc * nc, [&](int e) { int i = e % nc, j = e / nc; return A[i + (size_t)j * st]; },
             [&](int e, T v) { int i = e % nc, j = e / nc; Ut[j + (size_t)i * st] = v; });
     }
+    if (tid == 0 && npiv) atomicAdd(fp.nbpivots, npiv);
+}
+
+// ---------------------------------------------------------------------------
+// Diagonal block of a wide cblk factored by a cluster of DC CTAs (one per SM)
+// that keeps the whole block in shared memory: 32-column panel p lives in the
+// shared memory of CTA p % DC (rows 32 p .. nc - 1, all rows for GETRF, FP64,
+// row major, ld DG_LD).  Step p: the owner factors panel p (top block in
+// registers, inverse, rows below by X = X0 + (A - X0 T) Z on DMMA) and writes
+// it out; after a cluster barrier every CTA updates its own panels q > p,
+// reading panel p from the owner's shared memory (distributed shared memory)
+// -- for GETRF first the U block U_pq = L_pp^{-1} A_pq, as in the right
+// looking core_zgetrfsp.  Nothing of the trailing matrix goes through global
+// memory, so the step is bound by the owner's factorization and the cluster
+// barrier rather than by L2 round trips.
+// ---------------------------------------------------------------------------
+constexpr int DC = 8;                      // CTAs per cluster
+constexpr int DC_MIN_NC = 96;              // narrower blocks stay on one CTA
+constexpr long long DC_MAX_SMEM = 180 * 1024;  // dynamic shared memory next to the static 46 KB
+
+__host__ __device__ inline int dc_lo(int p, int fact) { return fact == FACT_GETRF ? 0 : 32 * p; }
+// Shared memory (doubles) of the panels CTA `rank` owns for a block of width nc.
+__host__ __device__ inline long long dc_panel_doubles(int nc, int fact, int rank) {
+    const int np = (nc + 31) / 32;
+    long long n = 0;
+    for (int p = rank; p < np; p += DC) n += (long long)(nc - dc_lo(p, fact)) * DG_LD;
+    return n;
+}
+__host__ __device__ inline long long diag_cluster_smem_bytes(int nc, int fact) {
+    return 8 * dc_panel_doubles(nc, fact, 0);  // CTA 0 holds the most
+}
+
+template <typename T, int FACT>
+__global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
+    k_diag_cluster(DevStruct s, const int *__restrict__ list, T *L, T *U, T *dinv, FactParams fp) {
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *Wl = reinterpret_cast<double *>(smem_raw);  // this CTA's panels, one after the other
+    __shared__ double Zs[2][32 * DG_LD];                 // inverted top blocks of the last panel factored here
+    __shared__ double Sx[8][8 * DG_LD];
+    __shared__ double Tb[32 * DG_LD], Ls[32];            // the top block being factored
+    __shared__ int npiv;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int k = list[blockIdx.x / DC];
+    const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+    const int st = s.cb_stride[k];
+    const int np = (nc + 31) / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
+    T *A = L + s.cb_coef[k];
+    T *gZ = dinv + s.cb_dinv[k];
+    if (tid == 0) npiv = 0;
+    // panel p of CTA p % DC: its offset inside that CTA's shared memory
+    auto poff = [&](int p) {
+        long long off = 0;
+        for (int q = p % DC; q < p; q += DC) off += (long long)(nc - dc_lo(q, FACT)) * DG_LD;
+        return off;
+    };
+    auto panel = [&](int p) -> double * {  // generic pointer, local or in another CTA of the cluster
+        double *base = cluster.map_shared_rank(Wl, p % DC);
+        return base + poff(p);
+    };
+    // load this CTA's panels (GETRF: L_kk += (U^T)_kk^T on the way)
+    for (int p = rank; p < np; p += DC) {
+        const int lo = dc_lo(p, FACT), rows = nc - lo, nb = min(32, nc - 32 * p);
+        double *W = Wl + poff(p);
+        const T *Ut = U + s.cb_coef[k];
+        dg_copy<4>(
+            rows, 32,
+            [&](int r, int c) {
+                if (c >= nb) return 0.0;
+                const int i = lo + r, j = 32 * p + c;
+                double v = (double)A[i + (size_t)j * st];
+                if (FACT == FACT_GETRF) v += (double)Ut[j + (size_t)i * st];
+                return v;
+            },
+            [&](int r, int c, double v) { W[r * DG_LD + c] = v; });
+    }
+    __syncthreads();
+    for (int p = 0; p < np; p++) {
+        const int nb = min(32, nc - 32 * p);
+        const int lop = dc_lo(p, FACT);
+        if (p % DC == rank) {  // factor panel p
+            double *W = Wl + poff(p);
+            double *Wt = W + (32 * p - lop) * DG_LD;  // top block
+            for (int e = tid; e < nb * DG_LD; e += blockDim.x) Tb[e] = Wt[e];  // the panel has nb rows left at its top
+            __syncthreads();
+            if (warp == 0) {
+                const int n = dg_factor32<FACT>(Tb, nb, fp.criterion, Ls);
+                if (lane == 0 && n) npiv += n;
+            }
+            __syncthreads();
+            if (warp == 0) dg_inverse<T, FACT>(Tb, nb, 0, Zs[0], gZ + (size_t)p * 1024);
+            if (FACT == FACT_GETRF && warp == 1) dg_inverse<T, FACT>(Tb, nb, 1, Zs[1], gZ + (size_t)(np + p) * 1024);
+            for (int e = tid; e < nb * DG_LD; e += blockDim.x) Wt[e] = Tb[e];
+            __syncthreads();
+            const int r0 = 32 * p + 32;  // rows below the top block
+            const int nrf = (nc - r0 + 7) / 8;
+            for (int i = warp; i < nrf; i += 8) {
+                const int rb = r0 + 8 * i;
+                dg_solve8(
+                    [&](int row, int col) { return (rb + row < nc) ? W[(rb + row - lop) * DG_LD + col] : 0.0; },
+                    [&](int a, int b) { return (a <= b && b < nb) ? dg_t<FACT>(Tb, a, b, 0) : 0.0; }, Zs[0],
+                    Sx[warp],
+                    [&](int row, int col, double v) {
+                        if (rb + row < nc) W[(rb + row - lop) * DG_LD + col] = v;
+                    });
+            }
+        }
+        cluster.sync();  // panel p (and its inverted blocks) visible to the cluster
+        if (p + 1 == np) break;
+        const double *Wp = panel(p);
+        const double *Wpt = Wp + (32 * p - lop) * DG_LD;
+        const double *Zr = cluster.map_shared_rank(&Zs[0][0], p % DC);
+        for (int q = p + 1 + ((rank - (p + 1)) % DC + DC) % DC; q < np; q += DC) {
+            const int nbq = min(32, nc - 32 * q);
+            const int loq = dc_lo(q, FACT);
+            double *Wq = Wl + poff(q);
+            if (FACT == FACT_GETRF) {  // U_pq = L_pp^{-1} A_pq, as (U_pq)^T L_pp^T = (A_pq)^T, 8 columns per warp
+                double *Ab = Wq + (32 * p - loq) * DG_LD;  // rows 32 p .. 32 p + 31 of panel q
+                if (warp < 4) {
+                    const int c0 = 8 * warp;
+                    dg_solve8(
+                        [&](int row, int col) { return (c0 + row < nbq) ? Ab[col * DG_LD + c0 + row] : 0.0; },
+                        [&](int a, int b) { return (a <= b && b < nb) ? dg_t<FACT>(Wpt, a, b, 1) : 0.0; },
+                        Zr + 32 * DG_LD, Sx[warp],
+                        [&](int row, int col, double v) {
+                            if (c0 + row < nbq) Ab[col * DG_LD + c0 + row] = v;
+                        });
+                }
+                __syncthreads();
+            }
+            // B block of this update (32 x 32: k by the columns of panel q) staged locally
+            for (int e = tid; e < 1024; e += blockDim.x) {
+                const int kk = e >> 5, cc = e & 31;
+                double b = 0.0;
+                if (cc < nbq && kk < nb) {
+                    if (FACT == FACT_GETRF) b = Wq[(32 * p + kk - loq) * DG_LD + cc];
+                    else {
+                        b = Wp[(32 * q + cc - lop) * DG_LD + kk];
+                        if (FACT == FACT_SYTRF) b *= Wpt[kk * DG_LD + kk];
+                    }
+                }
+                Tb[kk * DG_LD + cc] = b;
+            }
+            __syncthreads();
+            // trailing rows of panel q: rows from 32 p + 32 (GETRF) or 32 q (lower part) to nc;
+            // the 8 remote A values of a row fragment are requested together
+            const int rs = (FACT == FACT_GETRF) ? 32 * p + 32 : 32 * q;
+            const int nrf = (nc - rs + 7) / 8;
+            for (int i = warp; i < nrf; i += 8) {
+                const int rb = rs + 8 * i;
+                const bool rowok = rb + g < nc;
+                double av[8];
+#pragma unroll
+                for (int ks = 0; ks < 8; ks++) av[ks] = rowok ? -Wp[(rb + g - lop) * DG_LD + 4 * ks + t4] : 0.0;
+                double c[4][2];
+#pragma unroll
+                for (int cf = 0; cf < 4; cf++)
+#pragma unroll
+                    for (int e = 0; e < 2; e++)
+                        c[cf][e] = rowok ? Wq[(rb + g - loq) * DG_LD + 8 * cf + 2 * t4 + e] : 0.0;
+#pragma unroll
+                for (int ks = 0; ks < 8; ks++)
+#pragma unroll
+                    for (int cf = 0; cf < 4; cf++)
+                        dmma884(c[cf][0], c[cf][1], av[ks], Tb[(4 * ks + t4) * DG_LD + 8 * cf + g]);
+#pragma unroll
+                for (int cf = 0; cf < 4; cf++)
+#pragma unroll
+                    for (int e = 0; e < 2; e++)
+                        if (rowok) Wq[(rb + g - loq) * DG_LD + 8 * cf + 2 * t4 + e] = c[cf][e];
+            }
+            __syncthreads();
+        }
+    }
+    // this CTA's panels are final: write them out
+    for (int p = rank; p < np; p += DC) {
+        const int lop = dc_lo(p, FACT), nb = min(32, nc - 32 * p);
+        const double *W = Wl + poff(p);
+        dg_copy<4>(
+            nc - lop, nb, [&](int r, int c) { return W[r * DG_LD + c]; },
+            [&](int r, int c, double v) { A[(lop + r) + (size_t)(32 * p + c) * st] = (T)v; });
+    }
+    __threadfence();
+    cluster.sync();  // all panels written; no CTA leaves while its shared memory may still be read
+    if (rank == 0) {
+        if (FACT == FACT_SYTRF) {  // upper part of the diagonal block holds D L^T
+            batched_copy<8, T>(
+                nc * nc,
+                [&](int e) {
+                    int i = e % nc, j = e / nc;
+                    return (i < j) ? A[i + (size_t)i * st] * A[j + (size_t)i * st] : T(0);
+                },
+                [&](int e, T v) { int i = e % nc, j = e / nc; if (i < j) A[i + (size_t)j * st] = v; });
+        }
+        if (FACT == FACT_GETRF) {  // (U^T)_kk = (L\U)_kk^T
+            T *Ut = U + s.cb_coef[k];
+            batched_copy<8, T>(
+                nc * nc, [&](int e) { int i = e % nc, j = e / nc; return A[i + (size_t)j * st]; },
+                [&](int e, T v) { int i = e % nc, j = e / nc; Ut[j + (size_t)i * st] = v; });
+        }
+    }
+    __syncthreads();
     if (tid == 0 && npiv) atomicAdd(fp.nbpivots, npiv);
 }
 
@@ -1660,7 +1898,17 @@ template <typename T, int FACT>
 void launch_diag_large(const DevStruct &s, const int *list, int count, int maxnc, size_t smem, T *L, T *U, T *dinv,
                        const FactParams &fp, cudaStream_t st) {
     if (count <= 0) return;
-    if (maxnc <= DG_MAXNC)
+    static int nsm = 0;
+    if (nsm == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            nsm = 1;
+    }
+    const long long csm = diag_cluster_smem_bytes(maxnc, FACT);
+    if (maxnc <= DG_MAXNC && maxnc >= DC_MIN_NC && (long long)count * DC <= nsm && csm <= DC_MAX_SMEM)
+        k_diag_cluster<T, FACT><<<count * DC, 256, (size_t)csm, st>>>(s, list, L, U, dinv, fp);
+    else if (maxnc <= DG_MAXNC)
         k_diag_dmma<T, FACT><<<count, 256, (size_t)diag_dmma_smem_bytes(maxnc), st>>>(s, list, L, U, dinv, fp);
     else
         k_diag_large<T, FACT><<<count, 256, smem, st>>>(s, list, L, U, dinv, fp);
@@ -1732,6 +1980,7 @@ cudaError_t set_smem_attrs(size_t, size_t, size_t) {
     if ((e = opt_in_smem(k_diag_large<T, FACT>)) != cudaSuccess) return e;
     if ((e = opt_in_smem(k_trsm<T, FACT>)) != cudaSuccess) return e;
     if ((e = opt_in_smem(k_diag_dmma<T, FACT>)) != cudaSuccess) return e;
+    if ((e = opt_in_smem(k_diag_cluster<T, FACT>)) != cudaSuccess) return e;
     if constexpr (sizeof(T) == 8) {
         if ((e = opt_in_smem(k_update_dmma<FACT>)) != cudaSuccess) return e;
     } else {

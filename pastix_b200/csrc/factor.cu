@@ -856,7 +856,7 @@ __device__ __forceinline__ double trsm_tval(const T *D, int st, int a, int b, in
 }
 
 template <typename T, int FACT>
-__global__ void __launch_bounds__(256, 1) k_trsm_dmma(DevStruct s, const RowTile *__restrict__ tiles, T *L, T *U,
+__global__ void __launch_bounds__(256, 2) k_trsm_dmma(DevStruct s, const RowTile *__restrict__ tiles, T *L, T *U,
                                                        const T *__restrict__ dinv) {
     __shared__ double As[32 * TD_LDS], Xs[32 * TD_LDS], Rs[32 * TD_LDS];
     const RowTile tl = tiles[blockIdx.x];
@@ -1067,8 +1067,9 @@ __device__ __noinline__ void dg_inverse(const double *W, int nb, int side, doubl
 // column (or, for GETRF, the row) of each step reaches the other lanes through
 // the 32-entry shared vector Ls as broadcast reads: a dependent chain of warp
 // shuffles costs several times more per step.
-template <int FACT>
-__device__ __forceinline__ int dg_factor32(double *W, int nb, double crit, double *Ls) {
+template <int FACT, bool FULL>
+__device__ __forceinline__ int dg_factor32_impl(double *W, int nbr, double crit, double *Ls) {
+    const int nb = FULL ? 32 : nbr;  // a full block compiles without any bound test
     const int lane = threadIdx.x & 31;
     double r[32];
 #pragma unroll
@@ -1108,6 +1109,10 @@ __device__ __forceinline__ int dg_factor32(double *W, int nb, double crit, doubl
         for (int j = 0; j < 32; j++)
             if (j < nb) W[lane * DG_LD + j] = r[j];
     return np;
+}
+template <int FACT>
+__device__ __forceinline__ int dg_factor32(double *W, int nb, double crit, double *Ls) {
+    return (nb == 32) ? dg_factor32_impl<FACT, true>(W, 32, crit, Ls) : dg_factor32_impl<FACT, false>(W, nb, crit, Ls);
 }
 
 // CTA-wide transfer of a rows x cols region in 8 x 4 sub-tiles: lane (g, t4)

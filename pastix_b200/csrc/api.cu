@@ -51,6 +51,15 @@ void launch_update_tc(const DevStruct &, const UpdTile *, int, float *, float *,
 void launch_split(const DevStruct &, const SplitSlab *, int, const float *, const float *, const int64_t *,
                   unsigned char *, int, cudaStream_t);
 long long split_image_bytes(int nc, int st);
+int trinv_max_blocks();
+template <int F>
+void launch_trinv(const DevStruct &, const int *, int, int, const float *, const float *, const float *,
+                  const int64_t *, float *, cudaStream_t);
+void launch_split_dense(const DenseSlab *, int, const float *, unsigned char *, cudaStream_t);
+template <int F>
+void launch_trsm_tc(const DevStruct &, const UpdTile *, int, float *, float *, const unsigned char *,
+                    const unsigned char *, const int64_t *, const unsigned char *, const int64_t *, int *,
+                    cudaStream_t);
 template <typename T, int F>
 cudaError_t set_smem_attrs(size_t, size_t, size_t);
 // solve.cu
@@ -145,6 +154,10 @@ struct LevelLists {
     int updb0, updb1;       // big update tiles (128 x 64): DMMA for FP64
     int updt0, updt1;       // the same tasks in 128-row aligned windows: tcgen05 for FP32
     int spl0, spl1;         // 128-row slabs of the level's cblks split into BF16 terms (FP32)
+    int tt0, tt1;           // FP32 TRSM as GEMM tiles (tcgen05), task = cblk
+    int ds0, ds1;           // 128-row slabs of the transposed triangular inverses
+    int tr32_0, tr32_1;     // FP32: DMMA TRSM tiles of the wide cblks the GEMM form does not take
+    int ti_maxnzb;          // 32-column blocks of the widest cblk with a triangular inverse
     int cb0, cb1;           // all cblks of the level (solve diag)
     int st0, st1;           // solve row tiles
     int maxnc;
@@ -161,6 +174,12 @@ struct Device {
     DBuf<int> cb_fcol, cb_lcol, cb_stride, cb_fblok, bk_frow, bk_lrow, bk_rowoff, bk_fcblk, rowidx;
     DBuf<int64_t> cb_coef, cb_rowidx, cb_dinv, sp_off;
     DBuf<pgpu::SplitSlab> split_slabs;
+    DBuf<int64_t> ti_off, ti_img;
+    DBuf<pgpu::DenseSlab> dense_slabs;
+    DBuf<pgpu::UpdTile> trsm_tc_tiles;
+    DBuf<pgpu::RowTile> trsm_tiles32;
+    DBuf<float> tinv;                // transposed triangular inverses (FP32 factors)
+    DBuf<unsigned char> timg;        // their BF16 images
     DBuf<unsigned char> img0, img1;  // BF16 images of the FP32 panels (tcgen05 operands)
     DBuf<pgpu::TaskDev> tasks;
     DBuf<int> small_list, large_list, level_cblks;
@@ -218,6 +237,11 @@ struct pastix_data_s {
     std::vector<int64_t> sp_off;             // byte offset of each cblk's BF16 image (-1: none)
     int64_t split_total = 0;
     std::vector<pgpu::SplitSlab> split_slabs;
+    std::vector<int64_t> ti_off, ti_img;     // per cblk: FP32 TRSM by GEMM (-1: DMMA TRSM)
+    int64_t tinv_total = 0, timg_total = 0;
+    std::vector<pgpu::DenseSlab> dense_slabs;
+    std::vector<pgpu::UpdTile> trsm_tc_tiles;
+    std::vector<pgpu::RowTile> trsm_tiles32;
     int64_t dinv_total = 0;
     int factotype = PastixFactPOTRF;
     int mixed = 0;
@@ -686,6 +710,23 @@ static int build_maps_and_lists(pastix_data_t *pd) {
         pd->sp_off[k] = pd->split_total;
         pd->split_total += pgpu::split_image_bytes((int)(sv.cb_lcol[k] - sv.cb_fcol[k] + 1), (int)sv.cb_stride[k]);
     }
+    // FP32 TRSM by GEMM with the triangular inverse: wide cblks with rows below and a BF16 image
+    pd->ti_off.assign(sv.cblknbr, -1);
+    pd->ti_img.assign(sv.cblknbr, -1);
+    pd->tinv_total = pd->timg_total = 0;
+    pd->dense_slabs.clear();
+    pd->trsm_tc_tiles.clear();
+    pd->trsm_tiles32.clear();
+    const int nsides = (fk == pgpu::FACT_GETRF) ? 2 : 1;
+    for (idx_t k = 0; k < sv.cblknbr; k++) {
+        const idx_t nc = sv.cb_lcol[k] - sv.cb_fcol[k] + 1, st = sv.cb_stride[k];
+        if (pd->sp_off[k] < 0 || st <= nc || st * nc <= SMALL_PANEL_ELEMS || nc > 32 * pgpu::trinv_max_blocks())
+            continue;
+        pd->ti_off[k] = pd->tinv_total;
+        pd->ti_img[k] = pd->timg_total;
+        pd->tinv_total += (int64_t)nsides * nc * nc;
+        pd->timg_total += (int64_t)nsides * pgpu::split_image_bytes((int)nc, (int)nc);
+    }
     for (idx_t l = 0; l < sv.nlevels; l++) {
         LevelLists &L = pd->levels[l];
         L.small0 = (int)pd->small_list.size();
@@ -725,6 +766,33 @@ static int build_maps_and_lists(pastix_data_t *pd) {
             for (idx_t r = 0; r < sv.cb_stride[k]; r += 128) pd->split_slabs.push_back(pgpu::SplitSlab{(int)k, (int)r});
         }
         L.spl1 = (int)pd->split_slabs.size();
+        L.tt0 = (int)pd->trsm_tc_tiles.size();
+        L.ds0 = (int)pd->dense_slabs.size();
+        L.tr32_0 = (int)pd->trsm_tiles32.size();
+        L.ti_maxnzb = 0;
+        for (idx_t p = sv.lvl_ptr[l]; p < sv.lvl_ptr[l + 1]; p++) {
+            idx_t k = sv.lvl_cblk[p];
+            const idx_t nc = sv.cb_lcol[k] - sv.cb_fcol[k] + 1, st = sv.cb_stride[k];
+            if (st * nc <= SMALL_PANEL_ELEMS || st <= nc) continue;
+            if (pd->ti_off[k] < 0) {
+                for (idx_t r = nc; r < st; r += pgpu::trsm_tile_rows((int)nc))
+                    pd->trsm_tiles32.push_back(pgpu::RowTile{(int)k, (int)r});
+                continue;
+            }
+            L.ti_maxnzb = std::max<int>(L.ti_maxnzb, (int)((nc + 31) / 32));
+            const idx_t mt = (nc % 8 + (st - nc) + 127) / 128, nt = (nc + 127) / 128;
+            for (int side = 0; side < nsides; side++) {
+                for (idx_t a = 0; a < mt; a++)
+                    for (idx_t c = 0; c < nt; c++) pd->trsm_tc_tiles.push_back(pgpu::UpdTile{(int)k, (int)a, (int)c, side});
+                const int64_t src = pd->ti_off[k] + (int64_t)side * nc * nc;
+                const int64_t img = pd->ti_img[k] + (int64_t)side * pgpu::split_image_bytes((int)nc, (int)nc);
+                for (idx_t r = 0; r < nc; r += 128)
+                    pd->dense_slabs.push_back(pgpu::DenseSlab{src, img, (int)nc, (int)nc, (int)nc, (int)r});
+            }
+        }
+        L.tt1 = (int)pd->trsm_tc_tiles.size();
+        L.ds1 = (int)pd->dense_slabs.size();
+        L.tr32_1 = (int)pd->trsm_tiles32.size();
         L.small1 = (int)pd->small_list.size();
         L.large1 = (int)pd->large_list.size();
         L.trsm1 = (int)pd->trsm_tiles.size();
@@ -895,6 +963,11 @@ static int device_setup(pastix_data_t *pd) {
     CUDA_TRY(d.upd_tc_tiles.upload(pd->upd_tc_tiles, st));
     CUDA_TRY(d.upd_tiles32.upload(pd->upd_tiles32, st));
     CUDA_TRY(d.sp_off.upload(pd->sp_off, st));
+    CUDA_TRY(d.ti_off.upload(pd->ti_off, st));
+    CUDA_TRY(d.ti_img.upload(pd->ti_img, st));
+    if (!pd->dense_slabs.empty()) CUDA_TRY(d.dense_slabs.upload(pd->dense_slabs, st));
+    if (!pd->trsm_tc_tiles.empty()) CUDA_TRY(d.trsm_tc_tiles.upload(pd->trsm_tc_tiles, st));
+    if (!pd->trsm_tiles32.empty()) CUDA_TRY(d.trsm_tiles32.upload(pd->trsm_tiles32, st));
     if (!pd->split_slabs.empty()) CUDA_TRY(d.split_slabs.upload(pd->split_slabs, st));
     CUDA_TRY(d.lmap.upload(pd->lmap, st));
     if (!pd->umap.empty()) CUDA_TRY(d.umap.upload(pd->umap, st));
@@ -957,10 +1030,29 @@ static int run_factor(pastix_data_t *pd, double criterion) {
             pgpu::launch_diag_large<T, F>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0, lv.diag_maxnc,
                                           lv.diag_smem_elems * sizeof(T), L, U, Dinv, fp, st);
         });
-        launch_cls(pd, PC_TRSM, lv.trsm1 - lv.trsm0, [&] {
-            pgpu::launch_trsm<T, F>(d.ds, d.trsm_tiles.p + lv.trsm0, lv.trsm1 - lv.trsm0, lv.trsm_maxnc,
-                                    lv.trsm_smem_elems * sizeof(T), L, U, Dinv, st);
-        });
+        if constexpr (sizeof(T) == 8) {
+            launch_cls(pd, PC_TRSM, lv.trsm1 - lv.trsm0, [&] {
+                pgpu::launch_trsm<T, F>(d.ds, d.trsm_tiles.p + lv.trsm0, lv.trsm1 - lv.trsm0, lv.trsm_maxnc,
+                                        lv.trsm_smem_elems * sizeof(T), L, U, Dinv, st);
+            });
+        } else {
+            // FP32: X = A T^{-1} on tcgen05 -- inverses, their images, the panels' images before the TRSM
+            launch_cls(pd, PC_TRSM, lv.tt1 - lv.tt0, [&] {
+                pgpu::launch_trinv<F>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0, lv.ti_maxnzb, L, U,
+                                      Dinv, d.ti_off.p, d.tinv.p, st);
+                pgpu::launch_split_dense(d.dense_slabs.p + lv.ds0, lv.ds1 - lv.ds0, d.tinv.p, d.timg.p, st);
+                const pgpu::SplitSlab *sl = d.split_slabs.p + lv.spl0;
+                const int cnt = lv.spl1 - lv.spl0;
+                pgpu::launch_split(d.ds, sl, cnt, L, L, d.sp_off.p, d.img0.p, 0, st);
+                if (F == pgpu::FACT_GETRF) pgpu::launch_split(d.ds, sl, cnt, U, L, d.sp_off.p, d.img1.p, 0, st);
+                pgpu::launch_trsm_tc<F>(d.ds, d.trsm_tc_tiles.p + lv.tt0, lv.tt1 - lv.tt0, L, U, d.img0.p, d.img1.p,
+                                        d.sp_off.p, d.timg.p, d.ti_img.p, d.counters.p + 1, st);
+            });
+            launch_cls(pd, PC_TRSM, lv.tr32_1 - lv.tr32_0, [&] {
+                pgpu::launch_trsm<T, F>(d.ds, d.trsm_tiles32.p + lv.tr32_0, lv.tr32_1 - lv.tr32_0, lv.trsm_maxnc,
+                                        lv.trsm_smem_elems * sizeof(T), L, U, Dinv, st);
+            });
+        }
         if constexpr (sizeof(T) == 8) {
             launch_cls(pd, PC_UPDATE, lv.upd1 - lv.upd0, [&] {
                 pgpu::launch_update<T, F>(d.ds, d.upd_tiles.p + lv.upd0, lv.upd1 - lv.upd0, L, U, st);
@@ -1089,9 +1181,20 @@ extern "C" int pastix_subtask_bcsc2ctab(pastix_data_t *pd) {
             CUDA_TRY(cudaMemsetAsync(d.img1.p, 0, sb, d.stream));
         }
         if (nimg == 1) d.img1.reset();
+        // triangular inverses: entries below their blocks are never written, so clear on (re)allocation
+        if (pd->tinv_total > 0 && d.tinv.n != (size_t)pd->tinv_total) {
+            CUDA_TRY(d.tinv.alloc((size_t)pd->tinv_total));
+            CUDA_TRY(cudaMemsetAsync(d.tinv.p, 0, (size_t)pd->tinv_total * sizeof(float), d.stream));
+        }
+        if (pd->timg_total > 0 && d.timg.n != (size_t)pd->timg_total) {
+            CUDA_TRY(d.timg.alloc((size_t)pd->timg_total));
+            CUDA_TRY(cudaMemsetAsync(d.timg.p, 0, (size_t)pd->timg_total, d.stream));
+        }
     } else {
         d.img0.reset();
         d.img1.reset();
+        d.tinv.reset();
+        d.timg.reset();
     }
     CUDA_TRY(cudaMemsetAsync(d.Lc.p, 0, bytes, d.stream));
     if (d.Uc.p) CUDA_TRY(cudaMemsetAsync(d.Uc.p, 0, bytes, d.stream));

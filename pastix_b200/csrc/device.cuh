@@ -54,6 +54,14 @@ struct SplitSlab {
     int r0;
 };
 
+// A slab of 128 rows of a dense column-major FP32 matrix split into its BF16
+// image by k_split_dense (the transposed triangular inverses of k_trinv).
+struct DenseSlab {
+    int64_t src;  // element offset of the matrix
+    int64_t img;  // byte offset of its image
+    int ld, rows, cols, r0;
+};
+
 struct DevStruct {
     int n;
     int cblknbr;

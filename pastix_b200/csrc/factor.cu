@@ -1724,54 +1724,40 @@ __global__ void __launch_bounds__(256) k_split(DevStruct s, const SplitSlab *__r
     }
 }
 
-// imgA / imgB: the BF16 images holding the A and B operands of this kind
-// (POTRF: L, L; SYTRF: L, L D; GETRF: L and U, swapped on the U side).
-template <int FACT>
-__global__ void __launch_bounds__(128, 4) k_update_tc(DevStruct s, const UpdTile *__restrict__ tiles, float *L,
-                                                       float *U, const unsigned char *img0,
-                                                       const unsigned char *img1, const int64_t *__restrict__ sp_off,
-                                                       int *status) {
+// One 128 x nmma tile on tcgen05: operands from two BF16 images (A rows from
+// row group ga of an image with ngA row groups, B rows from group gb of one
+// with ngB groups; nkb K blocks; `term*` bytes between the three terms).  All
+// 128 threads call it; `pro` runs once the first stages are in flight (the
+// caller's per-tile set-up), `epi(row, c0, v)` receives 16 accumulator
+// columns c0 .. c0 + 15 of tile row `row`.  Returns false when a bounded wait
+// expired (PGPU_STATUS_TIMEOUT recorded, no epilogue run).
+struct TcOperands {
+    const unsigned char *iA, *iB;
+    size_t termA, termB;
+    int ngA, ngB, nkb, ga, gb, nmma;
+};
+template <typename Pro, typename Epi>
+__device__ __forceinline__ bool tc_tile(const TcOperands &op, int *status, Pro pro, Epi epi) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES], done;
     __shared__ uint32_t tmem_sh;
-    __shared__ int rt[TC_BM];
-    __shared__ int ct[TC_BN];
-    const UpdTile tl = tiles[blockIdx.x];
-    const TaskDev tk = s.tasks[tl.task];
-    const int k = tk.src, f = tk.dst;
-    const int K = s.cb_lcol[k] - s.cb_fcol[k] + 1;
-    const int st = s.cb_stride[k];
-    const int nkb = split_nkb(K), ng = split_ng(st);
-    const int ra = tk.row0 + (tl.side ? tk.n : 0);  // first A row of the task
-    const int rend = tk.row0 + tk.m;                // end of the A rows
-    const int rb = tk.row0, rbe = tk.row0 + tk.n;   // B rows
-    const int ga = (ra >> 3) + 16 * tl.mt, gb = (rb >> 3) + 16 * tl.nt;
-    const int nbrows = min(TC_BN, rbe - 8 * gb);
-    const int nmma = (nbrows + 15) & ~15;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const bool swap = (FACT == FACT_GETRF && tl.side == 1);
-    const unsigned char *iA = (swap ? img1 : img0) + sp_off[k];
-    const unsigned char *iB = ((FACT == FACT_POTRF) ? img0 : (swap ? img0 : img1)) + sp_off[k];
-    float *Cp = (swap ? U : L) + s.cb_coef[f];
-    const int stf = s.cb_stride[f];
-    const size_t term = (size_t)nkb * ng * TC_GROUP;  // bytes between the three terms
-    if (*(volatile int *)status != 0) return;         // an earlier tile gave up: leave the tensor cores alone
-
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
                      "r"(TC_BN));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    const uint32_t bbytes = (uint32_t)(nmma / 8) * TC_GROUP;
+    const uint32_t bbytes = (uint32_t)(op.nmma / 8) * TC_GROUP;
     auto produce = [&](int kb) {
         const int sidx = kb % TC_STAGES;
         unsigned char *sp = smem_raw + (size_t)sidx * TC_STAGE;
         mbar_expect_tx(&full[sidx], 3u * TC_PIECE + 3u * bbytes);
 #pragma unroll
         for (int p = 0; p < 3; p++) {
-            bulk_g2s(sp + p * TC_PIECE, iA + p * term + ((size_t)kb * ng + ga) * TC_GROUP, TC_PIECE, &full[sidx]);
-            bulk_g2s(sp + (3 + p) * TC_PIECE, iB + p * term + ((size_t)kb * ng + gb) * TC_GROUP, bbytes,
+            bulk_g2s(sp + p * TC_PIECE, op.iA + p * op.termA + ((size_t)kb * op.ngA + op.ga) * TC_GROUP, TC_PIECE,
                      &full[sidx]);
+            bulk_g2s(sp + (3 + p) * TC_PIECE, op.iB + p * op.termB + ((size_t)kb * op.ngB + op.gb) * TC_GROUP,
+                     bbytes, &full[sidx]);
         }
     };
     if (tid == 0) {
@@ -1781,34 +1767,16 @@ __global__ void __launch_bounds__(128, 4) k_update_tc(DevStruct s, const UpdTile
         }
         mbar_init(&done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        for (int kb = 0; kb < min(nkb, TC_STAGES); kb++) produce(kb);
+        for (int kb = 0; kb < min(op.nkb, TC_STAGES); kb++) produce(kb);
     }
-    // target rows and columns in the facing panel (-1: outside the task)
-    const int *ridx = s.rowidx + s.cb_rowidx[k];
-    {
-        const int pr = 8 * ga + tid;
-        int r = -1;
-        if (pr >= ra && pr < rend) {
-            const int g = ridx[pr];
-            int lo = s.cb_fblok[f], hi = s.cb_fblok[f + 1] - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (s.bk_frow[mid] <= g) lo = mid;
-                else hi = mid - 1;
-            }
-            r = s.bk_rowoff[lo] + (g - s.bk_frow[lo]);
-        }
-        rt[tid] = r;
-        const int pc = 8 * gb + tid;
-        ct[tid] = (pc >= rb && pc < rbe) ? (ridx[pc] - s.cb_fcol[f]) : -1;
-    }
+    pro();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_sh;
     int late = 0;
     if (tid == 0) {  // producer: the remaining K blocks, each once its stage is released
-        for (int kb = TC_STAGES; kb < nkb; kb++) {
+        for (int kb = TC_STAGES; kb < op.nkb; kb++) {
             if (!mbar_wait(&empty[kb % TC_STAGES], ((kb / TC_STAGES) - 1) & 1)) {
                 late = 1;
                 break;
@@ -1816,9 +1784,9 @@ __global__ void __launch_bounds__(128, 4) k_update_tc(DevStruct s, const UpdTile
             produce(kb);
         }
     } else if (tid == 32) {  // MMA issuer
-        const uint32_t idesc = tc_idesc(nmma);
+        const uint32_t idesc = tc_idesc(op.nmma);
         const uint32_t sbase = smem_u32(smem_raw);
-        for (int kb = 0; kb < nkb; kb++) {
+        for (int kb = 0; kb < op.nkb; kb++) {
             const int sidx = kb % TC_STAGES;
             if (!mbar_wait(&full[sidx], (kb / TC_STAGES) & 1)) {
                 late = 1;
@@ -1846,16 +1814,75 @@ __global__ void __launch_bounds__(128, 4) k_update_tc(DevStruct s, const UpdTile
     tc_fence_after();
     if (aborted) {
         if (tid == 0) atomicExch(status, PGPU_STATUS_TIMEOUT);
-    } else {
-        // epilogue: warp w reads accumulator lanes 32 w .. 32 w + 31, one tile row per thread
-        const int row = 32 * warp + lane;
-        const int rr = rt[row];
+    } else {  // warp w reads accumulator lanes 32 w .. 32 w + 31, one tile row per thread
         const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
 #pragma unroll 1
-        for (int c0 = 0; c0 < nmma; c0 += 16) {
+        for (int c0 = 0; c0 < op.nmma; c0 += 16) {
             float v[16];
             tmem_ld16(taddr + c0, v);
-            if (rr < 0) continue;
+            epi(32 * warp + lane, c0, v);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
+    return !aborted;
+}
+
+// imgA / imgB: the BF16 images holding the A and B operands of this kind
+// (POTRF: L, L; SYTRF: L, L D; GETRF: L and U, swapped on the U side).
+template <int FACT>
+__global__ void __launch_bounds__(128, 4) k_update_tc(DevStruct s, const UpdTile *__restrict__ tiles, float *L,
+                                                       float *U, const unsigned char *img0,
+                                                       const unsigned char *img1, const int64_t *__restrict__ sp_off,
+                                                       int *status) {
+    __shared__ int rt[TC_BM];
+    __shared__ int ct[TC_BN];
+    const UpdTile tl = tiles[blockIdx.x];
+    const TaskDev tk = s.tasks[tl.task];
+    const int k = tk.src, f = tk.dst;
+    const int K = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+    const int st = s.cb_stride[k];
+    const int ra = tk.row0 + (tl.side ? tk.n : 0);  // first A row of the task
+    const int rend = tk.row0 + tk.m;                // end of the A rows
+    const int rb = tk.row0, rbe = tk.row0 + tk.n;   // B rows
+    const bool swap = (FACT == FACT_GETRF && tl.side == 1);
+    TcOperands op;
+    op.nkb = split_nkb(K);
+    op.ngA = op.ngB = split_ng(st);
+    op.termA = op.termB = (size_t)op.nkb * op.ngA * TC_GROUP;
+    op.ga = (ra >> 3) + 16 * tl.mt;
+    op.gb = (rb >> 3) + 16 * tl.nt;
+    op.nmma = (min(TC_BN, rbe - 8 * op.gb) + 15) & ~15;
+    op.iA = (swap ? img1 : img0) + sp_off[k];
+    op.iB = ((FACT == FACT_POTRF) ? img0 : (swap ? img0 : img1)) + sp_off[k];
+    float *Cp = (swap ? U : L) + s.cb_coef[f];
+    const int stf = s.cb_stride[f];
+    if (*(volatile int *)status != 0) return;  // an earlier tile gave up: leave the tensor cores alone
+    const int tid = threadIdx.x;
+    tc_tile(
+        op, status,
+        [&] {  // target rows and columns in the facing panel (-1: outside the task)
+            const int *ridx = s.rowidx + s.cb_rowidx[k];
+            const int pr = 8 * op.ga + tid;
+            int r = -1;
+            if (pr >= ra && pr < rend) {
+                const int g = ridx[pr];
+                int lo = s.cb_fblok[f], hi = s.cb_fblok[f + 1] - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s.bk_frow[mid] <= g) lo = mid;
+                    else hi = mid - 1;
+                }
+                r = s.bk_rowoff[lo] + (g - s.bk_frow[lo]);
+            }
+            rt[tid] = r;
+            const int pc = 8 * op.gb + tid;
+            ct[tid] = (pc >= rb && pc < rbe) ? (ridx[pc] - s.cb_fcol[f]) : -1;
+        },
+        [&](int row, int c0, const float *v) {
+            const int rr = rt[row];
+            if (rr < 0) return;
             float *dst[16];
 #pragma unroll
             for (int j = 0; j < 16; j++) {
@@ -1874,11 +1901,170 @@ __global__ void __launch_bounds__(128, 4) k_update_tc(DevStruct s, const UpdTile
                 for (int j = 0; j < 16; j++)
                     if (dst[j]) atomicAdd(dst[j], -v[j]);
             }
-        }
-    }
-    tc_fence_before();
+        });
+}
+
+// ---------------------------------------------------------------------------
+// Inverse of the upper triangular factor T of a wide cblk's diagonal block
+// (T as in the off-diagonal TRSM: L^T for POTRF, D L^T for SYTRF, U and L^T
+// for the two GETRF sides), so that the FP32 TRSM X T = A becomes the GEMM
+// X = A T^{-1} on the tensor cores.  CTA (cblk, block column j, side) forms
+// block column j of T^{-1} from the inverted 32 x 32 diagonal blocks Z_i:
+//   Y_j = Z_j,   Y_i = -Z_i sum_{k = i+1..j} T_ik Y_k   (i = j-1 .. 0)
+// on DMMA in FP64, and stores it transposed (row c of the output = column c
+// of T^{-1}) in FP32, ready to be split into the BF16 operand image.
+// ---------------------------------------------------------------------------
+constexpr int TI_KC = 64;  // columns of T staged per chunk
+
+template <typename T, int FACT>
+__global__ void __launch_bounds__(256, 1) k_trinv(DevStruct s, const int *__restrict__ list, const T *L, const T *U,
+                                                   const T *__restrict__ dinv, const int64_t *__restrict__ ti_off,
+                                                   float *tinv) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *Yb = reinterpret_cast<double *>(smem_raw);  // rows 0 .. 32 j + 31 of the block column, ld DG_LD
+    __shared__ double Ts[32 * (TI_KC + 4)];
+    __shared__ double Zs[32 * DG_LD], Ss[32 * DG_LD];
+    const int k = list[blockIdx.x];
+    const int j = blockIdx.y;
+    const int side = blockIdx.z;
+    const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+    const int st = s.cb_stride[k];
+    const int nzb = (nc + 31) / 32;
+    if (j >= nzb || ti_off[k] < 0) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
+    const T *D = L + s.cb_coef[k];
+    const T *gZ = dinv + s.cb_dinv[k] + (size_t)(side ? nzb : 0) * 1024;
+    float *out = tinv + ti_off[k] + (size_t)side * nc * nc;
+    const int orf = warp >> 1, ocf = 2 * (warp & 1);  // this warp's two 8 x 8 fragments of a 32 x 32 block
+    // Y_j = Z_j
+    for (int e = tid; e < 1024; e += blockDim.x) Yb[(32 * j + (e >> 5)) * DG_LD + (e & 31)] = (double)gZ[(size_t)j * 1024 + e];
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
+    for (int i = j - 1; i >= 0; i--) {
+        // S = T_{i, i+1..j} Y_{i+1..j}, K = 32 (j - i), staged by chunks of TI_KC columns of T
+        double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+        const int k0 = 32 * (i + 1), kend = 32 * (j + 1);
+        for (int kc = k0; kc < kend; kc += TI_KC) {
+            const int kw = min(TI_KC, kend - kc);
+            for (int e = tid; e < 32 * TI_KC; e += blockDim.x) {
+                const int r = e / TI_KC, c = e % TI_KC;
+                const int a = 32 * i + r, b = kc + c;
+                Ts[r * (TI_KC + 4) + c] = (c < kw && b < nc) ? trsm_tval<T, FACT>(D, st, a, b, side) : 0.0;
+            }
+            __syncthreads();
+            for (int ks = 0; ks < kw / 4; ks++) {
+                const double a = Ts[(8 * orf + g) * (TI_KC + 4) + 4 * ks + t4];
+#pragma unroll
+                for (int c = 0; c < 2; c++)
+                    dmma884(acc[c][0], acc[c][1], a, Yb[(kc + 4 * ks + t4) * DG_LD + 8 * (ocf + c) + g]);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            Ss[(8 * orf + g) * DG_LD + 8 * (ocf + c) + 2 * t4] = acc[c][0];
+            Ss[(8 * orf + g) * DG_LD + 8 * (ocf + c) + 2 * t4 + 1] = acc[c][1];
+        }
+        for (int e = tid; e < 1024; e += blockDim.x) Zs[(e >> 5) * DG_LD + (e & 31)] = (double)gZ[(size_t)i * 1024 + e];
+        __syncthreads();
+        // Y_i = -Z_i S
+        double y[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+        for (int ks = 0; ks < 8; ks++) {
+            const double a = -Zs[(8 * orf + g) * DG_LD + 4 * ks + t4];
+#pragma unroll
+            for (int c = 0; c < 2; c++) dmma884(y[c][0], y[c][1], a, Ss[(4 * ks + t4) * DG_LD + 8 * (ocf + c) + g]);
+        }
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            Yb[(32 * i + 8 * orf + g) * DG_LD + 8 * (ocf + c) + 2 * t4] = y[c][0];
+            Yb[(32 * i + 8 * orf + g) * DG_LD + 8 * (ocf + c) + 2 * t4 + 1] = y[c][1];
+        }
+        __syncthreads();
+    }
+    // out[c + kk * nc] = T^{-1}[kk][c] for the block column's columns c and rows kk <= 32 j + 31
+    const int ncol = min(32, nc - 32 * j);
+    for (int e = tid; e < 32 * (j + 1) * 32; e += blockDim.x) {
+        const int kk = e >> 5, c = e & 31;
+        if (c < ncol && kk < nc) out[(32 * j + c) + (size_t)kk * nc] = (float)Yb[kk * DG_LD + c];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_split_dense(const DenseSlab *__restrict__ slabs, const float *src,
+                                                     unsigned char *img) {
+    const DenseSlab sl = slabs[blockIdx.x];
+    const int nkb = split_nkb(sl.cols), ng = split_ng(sl.rows);
+    const float *A = src + sl.src;
+    unsigned char *out = img + sl.img;
+    const int rows = min(128, 8 * ((sl.rows + 7) / 8) - sl.r0);
+    const int nch = TC_CH * nkb;
+    for (int it = threadIdx.x; it < 128 * nch; it += blockDim.x) {
+        const int r = it & 127, ch = it >> 7;
+        if (r >= rows) continue;
+        const int pr = sl.r0 + r;
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int c = 8 * ch + j;
+            v[j] = (pr < sl.rows && c < sl.cols) ? A[pr + (size_t)c * sl.ld] : 0.f;
+        }
+        uint32_t w[3][4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            uint32_t a0, a1, a2, b0, b1, b2;
+            split_bf16x3(v[2 * j], a0, a1, a2);
+            split_bf16x3(v[2 * j + 1], b0, b1, b2);
+            w[0][j] = a0 | (b0 << 16);
+            w[1][j] = a1 | (b1 << 16);
+            w[2][j] = a2 | (b2 << 16);
+        }
+        const size_t base = (size_t)(ch / TC_CH) * ng * TC_GROUP + (size_t)(pr >> 3) * TC_GROUP +
+                            (ch % TC_CH) * 128 + (pr & 7) * 16;
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+            *reinterpret_cast<uint4 *>(out + base + (size_t)p * nkb * ng * TC_GROUP) =
+                make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
+    }
+}
+
+// FP32 off-diagonal TRSM as the GEMM X = A T^{-1} on tcgen05: A from the
+// BF16 image of the panel taken before the TRSM, T^{-1} from the image of its
+// transpose (k_trinv, k_split_dense); the 128 x 128 tile of X overwrites the
+// panel rows below the diagonal block.  Tile: cblk, mt (128-row window from
+// the first off-diagonal row group), nt (128 columns), side (GETRF U panel).
+template <int FACT>
+__global__ void __launch_bounds__(128, 4) k_trsm_tc(DevStruct s, const UpdTile *__restrict__ tiles, float *L,
+                                                     float *U, const unsigned char *img0, const unsigned char *img1,
+                                                     const int64_t *__restrict__ sp_off,
+                                                     const unsigned char *timg, const int64_t *__restrict__ ti_img,
+                                                     int *status) {
+    const UpdTile tl = tiles[blockIdx.x];
+    const int k = tl.task;  // the cblk
+    const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+    const int st = s.cb_stride[k];
+    const bool uside = (FACT == FACT_GETRF && tl.side == 1);
+    TcOperands op;
+    op.nkb = split_nkb(nc);
+    op.ngA = split_ng(st);
+    op.ngB = split_ng(nc);
+    op.termA = (size_t)op.nkb * op.ngA * TC_GROUP;
+    op.termB = (size_t)op.nkb * op.ngB * TC_GROUP;
+    op.ga = (nc >> 3) + 16 * tl.mt;
+    op.gb = 16 * tl.nt;
+    op.nmma = (min(TC_BN, nc - 128 * tl.nt) + 15) & ~15;
+    op.iA = (uside ? img1 : img0) + sp_off[k];
+    op.iB = timg + ti_img[k] + (uside ? (size_t)3 * op.termB : 0);
+    float *P = (uside ? U : L) + s.cb_coef[k];
+    if (*(volatile int *)status != 0) return;
+    tc_tile(
+        op, status, [] {},
+        [&](int row, int c0, const float *v) {
+            const int pr = 8 * op.ga + row;  // panel row
+            if (pr < nc || pr >= st) return;
+            const int cb = 128 * tl.nt + c0;
+#pragma unroll
+            for (int j = 0; j < 16; j++)
+                if (cb + j < nc) P[pr + (size_t)(cb + j) * st] = v[j];
+        });
 }
 
 // ---------------------------------------------------------------------------
@@ -1955,6 +2141,28 @@ void launch_update_tc(const DevStruct &s, const UpdTile *tiles, int count, float
     k_update_tc<FACT><<<count, 128, TC_SMEM, st>>>(s, tiles, L, U, img0, img1, sp_off, status);
 }
 
+template <int FACT>
+void launch_trinv(const DevStruct &s, const int *list, int count, int maxnzb, const float *L, const float *U,
+                  const float *dinv, const int64_t *ti_off, float *tinv, cudaStream_t st) {
+    if (count <= 0 || maxnzb <= 0) return;
+    dim3 grid(count, maxnzb, FACT == FACT_GETRF ? 2 : 1);
+    k_trinv<float, FACT><<<grid, 256, (size_t)32 * maxnzb * DG_LD * sizeof(double), st>>>(s, list, L, U, dinv,
+                                                                                          ti_off, tinv);
+}
+
+void launch_split_dense(const DenseSlab *slabs, int count, const float *src, unsigned char *img, cudaStream_t st) {
+    if (count <= 0) return;
+    k_split_dense<<<count, 256, 0, st>>>(slabs, src, img);
+}
+
+template <int FACT>
+void launch_trsm_tc(const DevStruct &s, const UpdTile *tiles, int count, float *L, float *U,
+                    const unsigned char *img0, const unsigned char *img1, const int64_t *sp_off,
+                    const unsigned char *timg, const int64_t *ti_img, int *status, cudaStream_t st) {
+    if (count <= 0) return;
+    k_trsm_tc<FACT><<<count, 128, TC_SMEM, st>>>(s, tiles, L, U, img0, img1, sp_off, timg, ti_img, status);
+}
+
 void launch_split(const DevStruct &s, const SplitSlab *slabs, int count, const float *P, const float *D,
                   const int64_t *sp_off, unsigned char *img, int scale, cudaStream_t st) {
     if (count <= 0) return;
@@ -1962,6 +2170,7 @@ void launch_split(const DevStruct &s, const SplitSlab *slabs, int count, const f
 }
 
 long long split_image_bytes(int nc, int st) { return split_bytes(nc, st); }
+int trinv_max_blocks() { return DG_MAXNC / 32; }
 
 // Opt every kernel with dynamic shared memory into the largest size the
 // device allows next to its static shared memory.
@@ -1990,6 +2199,8 @@ cudaError_t set_smem_attrs(size_t, size_t, size_t) {
         if ((e = opt_in_smem(k_update_dmma<FACT>)) != cudaSuccess) return e;
     } else {
         if ((e = opt_in_smem(k_update_tc<FACT>)) != cudaSuccess) return e;
+        if ((e = opt_in_smem(k_trsm_tc<FACT>)) != cudaSuccess) return e;
+        if ((e = opt_in_smem(k_trinv<float, FACT>)) != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
@@ -2011,12 +2222,27 @@ PGPU_INST_FACT(double, FACT_GETRF)
 PGPU_INST_FACT(float, FACT_POTRF)
 PGPU_INST_FACT(float, FACT_SYTRF)
 PGPU_INST_FACT(float, FACT_GETRF)
+template void launch_trinv<FACT_POTRF>(const DevStruct &, const int *, int, int, const float *, const float *,
+                                      const float *, const int64_t *, float *, cudaStream_t);
+template void launch_trsm_tc<FACT_POTRF>(const DevStruct &, const UpdTile *, int, float *, float *, const unsigned char *,
+                                        const unsigned char *, const int64_t *, const unsigned char *,
+                                        const int64_t *, int *, cudaStream_t);
 template void launch_update_tc<FACT_POTRF>(const DevStruct &, const UpdTile *, int, float *, float *,
                                            const unsigned char *, const unsigned char *, const int64_t *, int *,
                                            cudaStream_t);
+template void launch_trinv<FACT_SYTRF>(const DevStruct &, const int *, int, int, const float *, const float *,
+                                      const float *, const int64_t *, float *, cudaStream_t);
+template void launch_trsm_tc<FACT_SYTRF>(const DevStruct &, const UpdTile *, int, float *, float *, const unsigned char *,
+                                        const unsigned char *, const int64_t *, const unsigned char *,
+                                        const int64_t *, int *, cudaStream_t);
 template void launch_update_tc<FACT_SYTRF>(const DevStruct &, const UpdTile *, int, float *, float *,
                                            const unsigned char *, const unsigned char *, const int64_t *, int *,
                                            cudaStream_t);
+template void launch_trinv<FACT_GETRF>(const DevStruct &, const int *, int, int, const float *, const float *,
+                                      const float *, const int64_t *, float *, cudaStream_t);
+template void launch_trsm_tc<FACT_GETRF>(const DevStruct &, const UpdTile *, int, float *, float *, const unsigned char *,
+                                        const unsigned char *, const int64_t *, const unsigned char *,
+                                        const int64_t *, int *, cudaStream_t);
 template void launch_update_tc<FACT_GETRF>(const DevStruct &, const UpdTile *, int, float *, float *,
                                            const unsigned char *, const unsigned char *, const int64_t *, int *,
                                            cudaStream_t);

@@ -71,10 +71,10 @@ template <typename T>
 void launch_bwd_update(const DevStruct &, const RowTile *, int, int, const T *, T *, int, int, cudaStream_t);
 template <typename T>
 void launch_fwd_diag_inv(const DevStruct &, const int *, int, int, const T *, const T *, int, int, const T *, T *,
-                         int, int, cudaStream_t);
+                         int, int, const float *, const int64_t *, cudaStream_t);
 template <typename T>
 void launch_bwd_diag_inv(const DevStruct &, const int *, int, int, const T *, const T *, int, int, const T *, T *,
-                         int, int, cudaStream_t);
+                         int, int, const float *, const int64_t *, cudaStream_t);
 template <typename T>
 void launch_bwd_diag(const DevStruct &, const int *, int, int, const T *, int, T *, int, int, cudaStream_t);
 template <typename T>
@@ -1291,6 +1291,12 @@ extern "C" int pgpu_device_status(const pastix_data_t *pd) {
 // ---------------------------------------------------------------------------
 // solve on permuted device vectors
 // ---------------------------------------------------------------------------
+// Full inverses of the wide cblks' diagonal factors: kept by the FP32 factorization only.
+template <typename T>
+static const float *tinv_of(const Device &d) {
+    return (sizeof(T) == 4 && d.tinv.n > 0) ? d.tinv.p : nullptr;
+}
+
 // Forward sweep with the block-lower panel P (unit diagonal or not).  Wide
 // cblks apply their diagonal blocks with the inverted sub-blocks (set zside,
 // D scaling for LDL^T), narrow ones by substitution.
@@ -1307,7 +1313,7 @@ static void sweep_forward(pastix_data_t *pd, const T *P, int unit, int zside, in
         });
         launch_cls(pd, PC_FWD_DIAG, lv.large1 - lv.large0, [&] {
             pgpu::launch_fwd_diag_inv<T>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0, lv.maxnc, P, Dinv,
-                                         zside, scaled, Ld, Y, ldy, nrhs, d.stream);
+                                         zside, scaled, Ld, Y, ldy, nrhs, tinv_of<T>(d), d.ti_off.p, d.stream);
         });
         launch_cls(pd, PC_FWD_UPDATE, lv.st1 - lv.st0, [&] {
             pgpu::launch_fwd_update<T>(d.ds, d.solve_tiles.p + lv.st0, lv.st1 - lv.st0, lv.maxnc, P, Y, ldy, nrhs,
@@ -1333,7 +1339,7 @@ static void sweep_backward(pastix_data_t *pd, const T *P, int unit, int zside, i
         });
         launch_cls(pd, PC_BWD_DIAG, lv.large1 - lv.large0, [&] {
             pgpu::launch_bwd_diag_inv<T>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0, lv.maxnc, P, Dinv,
-                                         zside, scaled, Ld, Y, ldy, nrhs, d.stream);
+                                         zside, scaled, Ld, Y, ldy, nrhs, tinv_of<T>(d), d.ti_off.p, d.stream);
         });
     }
 }

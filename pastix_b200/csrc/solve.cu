@@ -145,10 +145,86 @@ __global__ void __launch_bounds__(256) k_bwd_diag(DevStruct s, const int *__rest
 //   backward  x_j -= P[below, j]^T x[below],  then  x_j <- Z S x_j
 // with S = D (LDL^T, scaled) or I.  zside picks the Z set (GETRF: 0 = U, 1 = L^T).
 // ---------------------------------------------------------------------------
+// Diagonal steps with the full inverse of the block's triangular factor, kept
+// (transposed, FP32) by the FP32 factorization for its TRSM: Pt = T^{-T},
+// column major nc x nc.  Forward: y <- S Pt y; backward: x <- Pt^T S x (S = D
+// for LDL^T, else I) -- the blocked steps below, as one dense product each, so
+// a cblk's diagonal step is a single parallel pass instead of a chain of
+// 32-column blocks.  One right-hand side; y in shared memory; result to out.
+// Forward: the 8 warps split the columns of Pt, lanes take rows (coalesced),
+// 48 loads in flight per thread; partial sums meet in shared memory.
+template <typename T>
+__device__ __forceinline__ void tinv_fwd_gemv(const float *Pt, int nc, const T *Dl, int st, const T *y, T *out) {
+    __shared__ float part[8][384];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int kper = (nc + 7) / 8, k0 = warp * kper, k1 = min(nc, k0 + kper);
+    float acc[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) acc[i] = 0.f;
+    for (int kk = k0; kk < k1; kk += 4) {
+        float p[4][12];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int i = 0; i < 12; i++) {
+                const int c = lane + 32 * i;
+                p[u][i] = (c < nc && kk + u < k1) ? Pt[c + (size_t)(kk + u) * nc] : 0.f;
+            }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const float yk = (kk + u < k1) ? (float)y[kk + u] : 0.f;
+#pragma unroll
+            for (int i = 0; i < 12; i++) acc[i] += p[u][i] * yk;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 12; i++)
+        if (lane + 32 * i < nc) part[warp][lane + 32 * i] = acc[i];
+    __syncthreads();
+    for (int c = tid; c < nc; c += blockDim.x) {
+        float v = 0.f;
+#pragma unroll
+        for (int w = 0; w < 8; w++) v += part[w][c];
+        if (Dl) v *= (float)Dl[c + (size_t)c * st];
+        out[c] = (T)v;
+    }
+}
+// Backward: 4 outputs per warp at a time, lanes over the rows of Pt's columns
+// (coalesced), shuffle reductions.
+template <typename T>
+__device__ __forceinline__ void tinv_bwd_gemv(const float *Pt, int nc, const T *Dl, int st, const T *y, T *out) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float xv[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) {
+        const int c = lane + 32 * i;
+        xv[i] = (c < nc) ? (float)y[c] * (Dl ? (float)Dl[c + (size_t)c * st] : 1.f) : 0.f;
+    }
+    for (int kb = 4 * warp; kb < nc; kb += 32) {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int i = 0; i < 12; i++) {
+            const int c = lane + 32 * i;
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                acc[u] += ((c < nc && kb + u < nc) ? Pt[c + (size_t)(kb + u) * nc] : 0.f) * xv[i];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            float v = acc[u];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0 && kb + u < nc) out[kb + u] = (T)v;
+        }
+    }
+}
+
 template <typename T, int RC>
 __global__ void __launch_bounds__(256) k_fwd_diag_inv(DevStruct s, const int *__restrict__ list, const T *P,
                                                        const T *__restrict__ dinv, int zside, int scaled,
-                                                       const T *Ldiag, T *Y, int ldy, int nrhs) {
+                                                       const T *Ldiag, T *Y, int ldy, int nrhs,
+                                                       const float *__restrict__ tinv,
+                                                       const int64_t *__restrict__ ti_off) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *y = reinterpret_cast<T *>(smem_raw);  // nc x RC
     __shared__ T Z[32 * 33];
@@ -167,6 +243,12 @@ __global__ void __launch_bounds__(256) k_fwd_diag_inv(DevStruct s, const int *__
     for (int e = tid; e < nc * nr; e += nt) {
         int i = e % nc, j = e / nc;
         y[i + j * nc] = Y[(fc + i) + (size_t)(j0 + j) * ldy];
+    }
+    if (RC == 1 && tinv != nullptr && ti_off[k] >= 0) {  // full inverse kept by the FP32 factorization
+        __syncthreads();
+        tinv_fwd_gemv<T>(tinv + ti_off[k] + (size_t)zside * nc * nc, nc, scaled ? Dl : nullptr, st, y,
+                         Y + fc + (size_t)j0 * ldy);
+        return;
     }
     for (int jb = 0; jb < nc; jb += 32) {
         const int nb = min(32, nc - jb);
@@ -221,7 +303,9 @@ __global__ void __launch_bounds__(256) k_fwd_diag_inv(DevStruct s, const int *__
 template <typename T, int RC>
 __global__ void __launch_bounds__(256) k_bwd_diag_inv(DevStruct s, const int *__restrict__ list, const T *P,
                                                        const T *__restrict__ dinv, int zside, int scaled,
-                                                       const T *Ldiag, T *Y, int ldy, int nrhs) {
+                                                       const T *Ldiag, T *Y, int ldy, int nrhs,
+                                                       const float *__restrict__ tinv,
+                                                       const int64_t *__restrict__ ti_off) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *y = reinterpret_cast<T *>(smem_raw);  // nc x RC
     __shared__ T Z[32 * 33];
@@ -242,6 +326,11 @@ __global__ void __launch_bounds__(256) k_bwd_diag_inv(DevStruct s, const int *__
         y[i + j * nc] = Y[(fc + i) + (size_t)(j0 + j) * ldy];
     }
     __syncthreads();
+    if (RC == 1 && tinv != nullptr && ti_off[k] >= 0) {
+        tinv_bwd_gemv<T>(tinv + ti_off[k] + (size_t)zside * nc * nc, nc, scaled ? Dl : nullptr, st, y,
+                         Y + fc + (size_t)j0 * ldy);
+        return;
+    }
     for (int b = nzb - 1; b >= 0; b--) {
         const int jb = b * 32;
         const int nb = min(32, nc - jb);
@@ -430,19 +519,21 @@ void launch_bwd_diag(const DevStruct &s, const int *list, int count, int maxnc, 
 }
 template <typename T>
 void launch_fwd_diag_inv(const DevStruct &s, const int *list, int count, int maxnc, const T *P, const T *dinv,
-                         int zside, int scaled, const T *Ld, T *Y, int ldy, int nrhs, cudaStream_t st) {
+                         int zside, int scaled, const T *Ld, T *Y, int ldy, int nrhs, const float *tinv,
+                         const int64_t *ti_off, cudaStream_t st) {
     if (count <= 0) return;
     const int ZDIM = 1;
     PGPU_RC_DISPATCH(nrhs, k_fwd_diag_inv, count, (size_t)maxnc * sizeof(T), s, list, P, dinv, zside, scaled, Ld,
-                     Y, ldy, nrhs);
+                     Y, ldy, nrhs, tinv, ti_off);
 }
 template <typename T>
 void launch_bwd_diag_inv(const DevStruct &s, const int *list, int count, int maxnc, const T *P, const T *dinv,
-                         int zside, int scaled, const T *Ld, T *Y, int ldy, int nrhs, cudaStream_t st) {
+                         int zside, int scaled, const T *Ld, T *Y, int ldy, int nrhs, const float *tinv,
+                         const int64_t *ti_off, cudaStream_t st) {
     if (count <= 0) return;
     const int ZDIM = 1;
     PGPU_RC_DISPATCH(nrhs, k_bwd_diag_inv, count, (size_t)maxnc * sizeof(T), s, list, P, dinv, zside, scaled, Ld,
-                     Y, ldy, nrhs);
+                     Y, ldy, nrhs, tinv, ti_off);
 }
 template <typename T>
 void launch_fwd_update(const DevStruct &s, const RowTile *tiles, int count, int maxnc, const T *P, T *Y, int ldy,
@@ -471,9 +562,11 @@ int solve_rows_per_tile() { return ST_R; }
     template void launch_bwd_diag<T>(const DevStruct &, const int *, int, int, const T *, int, T *, int, int,     \
                                      cudaStream_t);                                                              \
     template void launch_fwd_diag_inv<T>(const DevStruct &, const int *, int, int, const T *, const T *, int,     \
-                                         int, const T *, T *, int, int, cudaStream_t);                           \
+                                         int, const T *, T *, int, int, const float *, const int64_t *,          \
+                                         cudaStream_t);                                                          \
     template void launch_bwd_diag_inv<T>(const DevStruct &, const int *, int, int, const T *, const T *, int,     \
-                                         int, const T *, T *, int, int, cudaStream_t);                           \
+                                         int, const T *, T *, int, int, const float *, const int64_t *,          \
+                                         cudaStream_t);                                                          \
     template void launch_fwd_update<T>(const DevStruct &, const RowTile *, int, int, const T *, T *, int, int,    \
                                        cudaStream_t);                                                            \
     template void launch_bwd_update<T>(const DevStruct &, const RowTile *, int, int, const T *, T *, int, int,    \

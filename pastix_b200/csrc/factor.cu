@@ -1889,18 +1889,10 @@ __global__ void __launch_bounds__(128, 4) k_update_tc(DevStruct s, const UpdTile
                 const int cc = ct[c0 + j];
                 dst[j] = (cc < 0) ? nullptr : Cp + rr + (size_t)cc * stf;
             }
-            if (tk.excl) {
-                float old[16];
+            // reductions without return (no round trip) for every target, exclusive or not
 #pragma unroll
-                for (int j = 0; j < 16; j++) old[j] = dst[j] ? *dst[j] : 0.f;
-#pragma unroll
-                for (int j = 0; j < 16; j++)
-                    if (dst[j]) *dst[j] = old[j] - v[j];
-            } else {
-#pragma unroll
-                for (int j = 0; j < 16; j++)
-                    if (dst[j]) atomicAdd(dst[j], -v[j]);
-            }
+            for (int j = 0; j < 16; j++)
+                if (dst[j]) atomicAdd(dst[j], -v[j]);
         });
 }
 

@@ -2060,8 +2060,294 @@ __global__ void __launch_bounds__(128, 4) k_trsm_tc(DevStruct s, const UpdTile *
 }
 
 // ---------------------------------------------------------------------------
+// Persistent, warp-specialized form of the tcgen05 tile loop.  A CTA walks the
+// tiles blockIdx.x, blockIdx.x + gridDim.x, ...: warp 4 (one thread) issues the
+// bulk copies of every K block through TP_STAGES shared-memory stages, warp 5
+// (one thread) issues the MMAs into one of two 128-column accumulators in
+// tensor memory, and warps 0-3 drain the other accumulator (tcgen05.ld, one
+// tile row per thread) while the next tile is multiplied.  Hand-offs:
+// full/empty mbarriers per stage (bulk-copy bytes / tcgen05.commit), tfull per
+// accumulator (tcgen05.commit), tempty per accumulator (128 epilogue arrivals).
+// Two CTAs per SM hold all 512 tensor-memory columns.  Every wait is bounded;
+// a role that gives up makes the others give up too and the kernel records
+// PGPU_STATUS_TIMEOUT.
+//   setup(t, op)            operands of tile t
+//   rowinfo(t, op, row)     per-row value kept in a register by the epilogue thread
+//   colinfo(t, op, col)     per-column value shared through shared memory
+//   epi(t, op, rinfo, ct, row, c0, v)  accumulator columns c0 .. c0 + 15 of a row
+// ---------------------------------------------------------------------------
+constexpr int TP_STAGES = 4;
+constexpr size_t TP_SMEM = (size_t)TP_STAGES * TC_STAGE;
+constexpr int TP_THREADS = 192;
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// OR of `pred` over the 128 epilogue threads (named barrier 1, which also orders them)
+__device__ __forceinline__ int epi_bar_or(int pred) {
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.b32 p, %1, 0;\n\tbarrier.red.or.pred q, 1, 128, p;\n\t"
+        "selp.b32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"(pred)
+        : "memory");
+    return r;
+}
+
+template <typename Setup, typename RowInfo, typename ColInfo, typename Epi>
+__device__ __forceinline__ void tc_persistent(int count, int *status, Setup setup, RowInfo rowinfo, ColInfo colinfo,
+                                              Epi epi) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[TP_STAGES], empty[TP_STAGES], tfull[2], tempty[2];
+    __shared__ uint32_t tmem_sh;
+    __shared__ int ctab[2][TC_BN];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (warp == 5) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
+                     "r"(2 * TC_BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        for (int i = 0; i < TP_STAGES; i++) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; i++) {
+            mbar_init(&tfull[i], 1);
+            mbar_init(&tempty[i], 4 * 32);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_sh;
+    int late = 0;
+    if (warp == 4) {
+        if (lane == 0) {  // producer
+            uint32_t g = 0;
+            for (int t = blockIdx.x; t < count && !late; t += gridDim.x) {
+                TcOperands op;
+                setup(t, op);
+                const uint32_t bbytes = (uint32_t)(op.nmma / 8) * TC_GROUP;
+                for (int kb = 0; kb < op.nkb; kb++, g++) {
+                    const int sidx = g % TP_STAGES;
+                    if (g >= TP_STAGES && !mbar_wait(&empty[sidx], ((g / TP_STAGES) - 1) & 1)) {
+                        late = 1;
+                        break;
+                    }
+                    unsigned char *sp = smem_raw + (size_t)sidx * TC_STAGE;
+                    mbar_expect_tx(&full[sidx], 3u * TC_PIECE + 3u * bbytes);
+#pragma unroll
+                    for (int p = 0; p < 3; p++) {
+                        bulk_g2s(sp + p * TC_PIECE, op.iA + p * op.termA + ((size_t)kb * op.ngA + op.ga) * TC_GROUP,
+                                 TC_PIECE, &full[sidx]);
+                        bulk_g2s(sp + (3 + p) * TC_PIECE,
+                                 op.iB + p * op.termB + ((size_t)kb * op.ngB + op.gb) * TC_GROUP, bbytes, &full[sidx]);
+                    }
+                }
+            }
+        }
+    } else if (warp == 5) {
+        if (lane == 0) {  // MMA issuer
+            const uint32_t sbase = smem_u32(smem_raw);
+            uint32_t g = 0;
+            int i = 0;
+            for (int t = blockIdx.x; t < count && !late; t += gridDim.x, i++) {
+                TcOperands op;
+                setup(t, op);
+                const int b = i & 1;
+                if (i >= 2 && !mbar_wait(&tempty[b], ((i >> 1) - 1) & 1)) {
+                    late = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t idesc = tc_idesc(op.nmma);
+                const uint32_t acc = tmem + (uint32_t)(TC_BN * b);
+                for (int kb = 0; kb < op.nkb; kb++, g++) {
+                    const int sidx = g % TP_STAGES;
+                    if (!mbar_wait(&full[sidx], (g / TP_STAGES) & 1)) {
+                        late = 1;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t st0 = sbase + sidx * TC_STAGE;
+#pragma unroll
+                    for (int ks = 0; ks < TC_BK / 16; ks++) {
+#pragma unroll
+                        for (int p = 0; p < 6; p++) {
+                            const int pa = (p == 2 || p == 4) ? 1 : (p == 5 ? 2 : 0);
+                            const int pb = (p == 1 || p == 4) ? 1 : (p == 3 ? 2 : 0);
+                            tc_mma(acc, tc_desc(st0 + pa * TC_PIECE + ks * 256),
+                                   tc_desc(st0 + (3 + pb) * TC_PIECE + ks * 256), idesc, (kb | ks | p) != 0);
+                        }
+                    }
+                    tc_commit(&empty[sidx]);
+                }
+                if (late) break;
+                tc_commit(&tfull[b]);
+            }
+        }
+    } else {  // epilogue warps 0-3: tile row = tid, tensor-memory lanes 32 warp .. 32 warp + 31
+        int i = 0;
+        for (int t = blockIdx.x; t < count; t += gridDim.x, i++) {
+            TcOperands op;
+            setup(t, op);
+            const int b = i & 1;
+            const int rinfo = rowinfo(t, op, tid);
+            ctab[b][tid] = colinfo(t, op, tid);
+            const int fail = epi_bar_or(!mbar_wait(&tfull[b], (i >> 1) & 1));
+            if (fail) {
+                late = 1;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(TC_BN * b);
+#pragma unroll 1
+            for (int c0 = 0; c0 < op.nmma; c0 += 16) {
+                float v[16];
+                tmem_ld16(taddr + c0, v);
+                epi(t, op, rinfo, ctab[b], tid, c0, v);
+            }
+            tc_fence_before();
+            mbar_arrive(&tempty[b]);
+        }
+    }
+    __syncwarp();
+    const int aborted = __syncthreads_or(late);
+    if (aborted && tid == 0) atomicExch(status, PGPU_STATUS_TIMEOUT);
+    tc_fence_after();
+    if (warp == 5) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC_BN));
+}
+
+template <int FACT>
+__global__ void __launch_bounds__(TP_THREADS, 2) k_update_tcp(DevStruct s, const UpdTile *__restrict__ tiles,
+                                                               int count, float *L, float *U,
+                                                               const unsigned char *img0, const unsigned char *img1,
+                                                               const int64_t *__restrict__ sp_off, int *status) {
+    if (*(volatile int *)status != 0) return;
+    auto setup = [&](int t, TcOperands &op) {
+        const UpdTile tl = tiles[t];
+        const TaskDev tk = s.tasks[tl.task];
+        const int k = tk.src;
+        const int K = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+        const int st = s.cb_stride[k];
+        const int ra = tk.row0 + (tl.side ? tk.n : 0);
+        const int rbe = tk.row0 + tk.n;
+        const bool swap = (FACT == FACT_GETRF && tl.side == 1);
+        op.nkb = split_nkb(K);
+        op.ngA = op.ngB = split_ng(st);
+        op.termA = op.termB = (size_t)op.nkb * op.ngA * TC_GROUP;
+        op.ga = (ra >> 3) + 16 * tl.mt;
+        op.gb = (tk.row0 >> 3) + 16 * tl.nt;
+        op.nmma = (min(TC_BN, rbe - 8 * op.gb) + 15) & ~15;
+        op.iA = (swap ? img1 : img0) + sp_off[k];
+        op.iB = ((FACT == FACT_POTRF) ? img0 : (swap ? img0 : img1)) + sp_off[k];
+    };
+    auto rowinfo = [&](int t, const TcOperands &op, int row) {  // offset of the target row in the facing panel
+        const UpdTile tl = tiles[t];
+        const TaskDev tk = s.tasks[tl.task];
+        const int k = tk.src, f = tk.dst;
+        const int ra = tk.row0 + (tl.side ? tk.n : 0), rend = tk.row0 + tk.m;
+        const int pr = 8 * op.ga + row;
+        if (pr < ra || pr >= rend) return -1;
+        const int g = s.rowidx[s.cb_rowidx[k] + pr];
+        int lo = s.cb_fblok[f], hi = s.cb_fblok[f + 1] - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s.bk_frow[mid] <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        return s.bk_rowoff[lo] + (g - s.bk_frow[lo]);
+    };
+    auto colinfo = [&](int t, const TcOperands &op, int col) {  // target column in the facing panel
+        const UpdTile tl = tiles[t];
+        const TaskDev tk = s.tasks[tl.task];
+        const int pc = 8 * op.gb + col;
+        if (pc < tk.row0 || pc >= tk.row0 + tk.n) return -1;
+        return s.rowidx[s.cb_rowidx[tk.src] + pc] - s.cb_fcol[tk.dst];
+    };
+    auto epi = [&](int t, const TcOperands &op, int rr, const int *ct, int row, int c0, const float *v) {
+        if (rr < 0) return;
+        const UpdTile tl = tiles[t];
+        const TaskDev tk = s.tasks[tl.task];
+        const bool swap = (FACT == FACT_GETRF && tl.side == 1);
+        float *Cp = (swap ? U : L) + s.cb_coef[tk.dst] + rr;
+        const int stf = s.cb_stride[tk.dst];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const int cc = ct[c0 + j];
+            if (cc >= 0) atomicAdd(Cp + (size_t)cc * stf, -v[j]);  // reduction without return
+        }
+    };
+    tc_persistent(count, status, setup, rowinfo, colinfo, epi);
+}
+
+template <int FACT>
+__global__ void __launch_bounds__(TP_THREADS, 2) k_trsm_tcp(DevStruct s, const UpdTile *__restrict__ tiles, int count,
+                                                             float *L, float *U, const unsigned char *img0,
+                                                             const unsigned char *img1,
+                                                             const int64_t *__restrict__ sp_off,
+                                                             const unsigned char *timg,
+                                                             const int64_t *__restrict__ ti_img, int *status) {
+    if (*(volatile int *)status != 0) return;
+    auto setup = [&](int t, TcOperands &op) {
+        const UpdTile tl = tiles[t];
+        const int k = tl.task;
+        const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+        const int st = s.cb_stride[k];
+        const bool uside = (FACT == FACT_GETRF && tl.side == 1);
+        op.nkb = split_nkb(nc);
+        op.ngA = split_ng(st);
+        op.ngB = split_ng(nc);
+        op.termA = (size_t)op.nkb * op.ngA * TC_GROUP;
+        op.termB = (size_t)op.nkb * op.ngB * TC_GROUP;
+        op.ga = (nc >> 3) + 16 * tl.mt;
+        op.gb = 16 * tl.nt;
+        op.nmma = (min(TC_BN, nc - 128 * tl.nt) + 15) & ~15;
+        op.iA = (uside ? img1 : img0) + sp_off[k];
+        op.iB = timg + ti_img[k] + (uside ? (size_t)3 * op.termB : 0);
+    };
+    auto rowinfo = [&](int t, const TcOperands &op, int row) {  // panel row, -1 outside the rows below
+        const int k = tiles[t].task;
+        const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+        const int pr = 8 * op.ga + row;
+        return (pr >= nc && pr < s.cb_stride[k]) ? pr : -1;
+    };
+    auto colinfo = [&](int t, const TcOperands &op, int col) {
+        const int k = tiles[t].task;
+        const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
+        const int c = 128 * tiles[t].nt + col;
+        return (c < nc) ? c : -1;
+    };
+    auto epi = [&](int t, const TcOperands &op, int pr, const int *ct, int row, int c0, const float *v) {
+        if (pr < 0) return;
+        const UpdTile tl = tiles[t];
+        const int k = tl.task;
+        const int st = s.cb_stride[k];
+        float *P = ((FACT == FACT_GETRF && tl.side == 1) ? U : L) + s.cb_coef[k] + pr;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const int c = ct[c0 + j];
+            if (c >= 0) P[(size_t)c * st] = v[j];
+        }
+    };
+    tc_persistent(count, status, setup, rowinfo, colinfo, epi);
+}
+
+// ---------------------------------------------------------------------------
 // Host launch wrappers (called from the driver with level lists in device memory)
 // ---------------------------------------------------------------------------
+static int sm_count() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            n = 1;
+    }
+    return n;
+}
 template <typename T>
 void launch_fill_coef(int64_t nnz, const double *vals, const int64_t *lmap, const int64_t *umap, T *L, T *U,
                       cudaStream_t st) {
@@ -2130,7 +2416,8 @@ void launch_update_tc(const DevStruct &s, const UpdTile *tiles, int count, float
                       const unsigned char *img0, const unsigned char *img1, const int64_t *sp_off, int *status,
                       cudaStream_t st) {
     if (count <= 0) return;
-    k_update_tc<FACT><<<count, 128, TC_SMEM, st>>>(s, tiles, L, U, img0, img1, sp_off, status);
+    const int grid = std::min(count, 2 * sm_count());
+    k_update_tcp<FACT><<<grid, TP_THREADS, TP_SMEM, st>>>(s, tiles, count, L, U, img0, img1, sp_off, status);
 }
 
 template <int FACT>
@@ -2152,7 +2439,9 @@ void launch_trsm_tc(const DevStruct &s, const UpdTile *tiles, int count, float *
                     const unsigned char *img0, const unsigned char *img1, const int64_t *sp_off,
                     const unsigned char *timg, const int64_t *ti_img, int *status, cudaStream_t st) {
     if (count <= 0) return;
-    k_trsm_tc<FACT><<<count, 128, TC_SMEM, st>>>(s, tiles, L, U, img0, img1, sp_off, timg, ti_img, status);
+    const int grid = std::min(count, 2 * sm_count());
+    k_trsm_tcp<FACT><<<grid, TP_THREADS, TP_SMEM, st>>>(s, tiles, count, L, U, img0, img1, sp_off, timg, ti_img,
+                                                         status);
 }
 
 void launch_split(const DevStruct &s, const SplitSlab *slabs, int count, const float *P, const float *D,
@@ -2192,6 +2481,8 @@ cudaError_t set_smem_attrs(size_t, size_t, size_t) {
     } else {
         if ((e = opt_in_smem(k_update_tc<FACT>)) != cudaSuccess) return e;
         if ((e = opt_in_smem(k_trsm_tc<FACT>)) != cudaSuccess) return e;
+        if ((e = opt_in_smem(k_update_tcp<FACT>)) != cudaSuccess) return e;
+        if ((e = opt_in_smem(k_trsm_tcp<FACT>)) != cudaSuccess) return e;
         if ((e = opt_in_smem(k_trinv<float, FACT>)) != cudaSuccess) return e;
     }
     return cudaSuccess;

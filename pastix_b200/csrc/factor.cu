@@ -1906,15 +1906,21 @@ __global__ void __launch_bounds__(128, 4) k_update_tc(DevStruct s, const UpdTile
 // on DMMA in FP64, and stores it transposed (row c of the output = column c
 // of T^{-1}) in FP32, ready to be split into the BF16 operand image.
 // ---------------------------------------------------------------------------
-constexpr int TI_KC = 64;  // columns of T staged per chunk
+// Dynamic shared memory of k_trinv for blocks of up to maxnzb 32-column blocks:
+// the block column of T^{-1} (FP64) and one block row of T (FP32).
+__host__ __device__ inline int ti_ts_ld(int maxnzb) { return 32 * maxnzb + 4; }
+__host__ __device__ inline long long trinv_smem_bytes(int maxnzb) {
+    return 32LL * maxnzb * DG_LD * 8 + 32LL * ti_ts_ld(maxnzb) * 4;
+}
 
 template <typename T, int FACT>
 __global__ void __launch_bounds__(256, 1) k_trinv(DevStruct s, const int *__restrict__ list, const T *L, const T *U,
                                                    const T *__restrict__ dinv, const int64_t *__restrict__ ti_off,
-                                                   float *tinv) {
+                                                   float *tinv, int maxnzb) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *Yb = reinterpret_cast<double *>(smem_raw);  // rows 0 .. 32 j + 31 of the block column, ld DG_LD
-    __shared__ double Ts[32 * (TI_KC + 4)];
+    double *Yb = reinterpret_cast<double *>(smem_raw);       // rows 0 .. 32 j + 31 of the block column, ld DG_LD
+    float *Ts = reinterpret_cast<float *>(Yb + 32 * maxnzb * DG_LD);  // block row i of T, ld ti_ts_ld
+    const int tld = ti_ts_ld(maxnzb);
     __shared__ double Zs[32 * DG_LD], Ss[32 * DG_LD];
     const int k = list[blockIdx.x];
     const int j = blockIdx.y;
@@ -1930,33 +1936,29 @@ __global__ void __launch_bounds__(256, 1) k_trinv(DevStruct s, const int *__rest
     const int orf = warp >> 1, ocf = 2 * (warp & 1);  // this warp's two 8 x 8 fragments of a 32 x 32 block
     // Y_j = Z_j
     for (int e = tid; e < 1024; e += blockDim.x) Yb[(32 * j + (e >> 5)) * DG_LD + (e & 31)] = (double)gZ[(size_t)j * 1024 + e];
-    __syncthreads();
     for (int i = j - 1; i >= 0; i--) {
-        // S = T_{i, i+1..j} Y_{i+1..j}, K = 32 (j - i), staged by chunks of TI_KC columns of T
+        // stage block row i of T (columns 32 (i + 1) .. 32 j + 31) and Z_i in one pass
+        const int k0 = 32 * (i + 1), K = 32 * (j - i);
+        for (int e = tid; e < 32 * K; e += blockDim.x) {
+            const int r = e / K, c = e - r * K;
+            const int b = k0 + c;
+            Ts[r * tld + c] = (b < nc) ? (float)trsm_tval<T, FACT>(D, st, 32 * i + r, b, side) : 0.f;
+        }
+        for (int e = tid; e < 1024; e += blockDim.x) Zs[(e >> 5) * DG_LD + (e & 31)] = (double)gZ[(size_t)i * 1024 + e];
+        __syncthreads();
+        // S = T_{i, i+1..j} Y_{i+1..j}
         double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
-        const int k0 = 32 * (i + 1), kend = 32 * (j + 1);
-        for (int kc = k0; kc < kend; kc += TI_KC) {
-            const int kw = min(TI_KC, kend - kc);
-            for (int e = tid; e < 32 * TI_KC; e += blockDim.x) {
-                const int r = e / TI_KC, c = e % TI_KC;
-                const int a = 32 * i + r, b = kc + c;
-                Ts[r * (TI_KC + 4) + c] = (c < kw && b < nc) ? trsm_tval<T, FACT>(D, st, a, b, side) : 0.0;
-            }
-            __syncthreads();
-            for (int ks = 0; ks < kw / 4; ks++) {
-                const double a = Ts[(8 * orf + g) * (TI_KC + 4) + 4 * ks + t4];
+        for (int ks = 0; ks < K / 4; ks++) {
+            const double a = (double)Ts[(8 * orf + g) * tld + 4 * ks + t4];
 #pragma unroll
-                for (int c = 0; c < 2; c++)
-                    dmma884(acc[c][0], acc[c][1], a, Yb[(kc + 4 * ks + t4) * DG_LD + 8 * (ocf + c) + g]);
-            }
-            __syncthreads();
+            for (int c = 0; c < 2; c++)
+                dmma884(acc[c][0], acc[c][1], a, Yb[(k0 + 4 * ks + t4) * DG_LD + 8 * (ocf + c) + g]);
         }
 #pragma unroll
         for (int c = 0; c < 2; c++) {
             Ss[(8 * orf + g) * DG_LD + 8 * (ocf + c) + 2 * t4] = acc[c][0];
             Ss[(8 * orf + g) * DG_LD + 8 * (ocf + c) + 2 * t4 + 1] = acc[c][1];
         }
-        for (int e = tid; e < 1024; e += blockDim.x) Zs[(e >> 5) * DG_LD + (e & 31)] = (double)gZ[(size_t)i * 1024 + e];
         __syncthreads();
         // Y_i = -Z_i S
         double y[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
@@ -1973,6 +1975,7 @@ __global__ void __launch_bounds__(256, 1) k_trinv(DevStruct s, const int *__rest
         }
         __syncthreads();
     }
+    __syncthreads();
     // out[c + kk * nc] = T^{-1}[kk][c] for the block column's columns c and rows kk <= 32 j + 31
     const int ncol = min(32, nc - 32 * j);
     for (int e = tid; e < 32 * (j + 1) * 32; e += blockDim.x) {
@@ -1981,6 +1984,7 @@ __global__ void __launch_bounds__(256, 1) k_trinv(DevStruct s, const int *__rest
     }
 }
 
+// Split slabs of dense column-major FP32 matrices into their BF16 images.
 __global__ void __launch_bounds__(256) k_split_dense(const DenseSlab *__restrict__ slabs, const float *src,
                                                      unsigned char *img) {
     const DenseSlab sl = slabs[blockIdx.x];
@@ -2425,8 +2429,8 @@ void launch_trinv(const DevStruct &s, const int *list, int count, int maxnzb, co
                   const float *dinv, const int64_t *ti_off, float *tinv, cudaStream_t st) {
     if (count <= 0 || maxnzb <= 0) return;
     dim3 grid(count, maxnzb, FACT == FACT_GETRF ? 2 : 1);
-    k_trinv<float, FACT><<<grid, 256, (size_t)32 * maxnzb * DG_LD * sizeof(double), st>>>(s, list, L, U, dinv,
-                                                                                          ti_off, tinv);
+    k_trinv<float, FACT><<<grid, 256, (size_t)trinv_smem_bytes(maxnzb), st>>>(s, list, L, U, dinv, ti_off, tinv,
+                                                                               maxnzb);
 }
 
 void launch_split_dense(const DenseSlab *slabs, int count, const float *src, unsigned char *img, cudaStream_t st) {

@@ -1579,21 +1579,15 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
 //
 // Tiles.  A task's A rows and B rows are covered by 128-row windows aligned to
 // row groups; rows and columns outside the task are masked in the epilogue.
-// Per K block one thread issues six bulk copies (three terms of A and of B)
-// onto the stage's mbarrier, one thread issues the six MMAs per 16 columns and
-// commits them to the stage's "empty" mbarrier.  Two stages of 24 KB keep four
-// CTAs (and their 128-column accumulators, all of tensor memory) on an SM, so
-// one tile's epilogue overlaps the others' MMAs.  The epilogue reads the
-// accumulator with tcgen05.ld (one tile row per thread) and scatters it into
-// the facing panel (core_zgemmsp_2d2d semantics, like k_update).  Every wait
+// The tile loop itself (bulk copies through mbarrier stages, MMAs, tensor
+// memory epilogue) is the persistent engine tc_persistent below.  Every wait
 // is bounded; on expiry the kernel records PGPU_STATUS_TIMEOUT and returns.
 // ---------------------------------------------------------------------------
-constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 16, TC_STAGES = 2;
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 16;
 constexpr int TC_CH = TC_BK / 8;                    // 8-column chunks per K block
 constexpr int TC_GROUP = 128 * TC_CH;               // bytes of 8 rows x TC_BK columns of one term
 constexpr int TC_PIECE = (TC_BM / 8) * TC_GROUP;    // one term of a 128-row operand block
 constexpr int TC_STAGE = 6 * TC_PIECE;              // A0 A1 A2 B0 B1 B2
-constexpr size_t TC_SMEM = (size_t)TC_STAGES * TC_STAGE;
 constexpr int TC_SPIN = 1 << 20;                    // try_wait rounds before giving up
 constexpr int PGPU_STATUS_TIMEOUT = 3;
 
@@ -1724,177 +1718,14 @@ __global__ void __launch_bounds__(256) k_split(DevStruct s, const SplitSlab *__r
     }
 }
 
-// One 128 x nmma tile on tcgen05: operands from two BF16 images (A rows from
-// row group ga of an image with ngA row groups, B rows from group gb of one
-// with ngB groups; nkb K blocks; `term*` bytes between the three terms).  All
-// 128 threads call it; `pro` runs once the first stages are in flight (the
-// caller's per-tile set-up), `epi(row, c0, v)` receives 16 accumulator
-// columns c0 .. c0 + 15 of tile row `row`.  Returns false when a bounded wait
-// expired (PGPU_STATUS_TIMEOUT recorded, no epilogue run).
+// Operands of one 128 x nmma tile: A rows from row group ga of a BF16 image
+// with ngA row groups, B rows from group gb of one with ngB groups; nkb K
+// blocks; `term*` bytes between the three terms of an image.
 struct TcOperands {
     const unsigned char *iA, *iB;
     size_t termA, termB;
     int ngA, ngB, nkb, ga, gb, nmma;
 };
-template <typename Pro, typename Epi>
-__device__ __forceinline__ bool tc_tile(const TcOperands &op, int *status, Pro pro, Epi epi) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES], done;
-    __shared__ uint32_t tmem_sh;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
-                     "r"(TC_BN));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    const uint32_t bbytes = (uint32_t)(op.nmma / 8) * TC_GROUP;
-    auto produce = [&](int kb) {
-        const int sidx = kb % TC_STAGES;
-        unsigned char *sp = smem_raw + (size_t)sidx * TC_STAGE;
-        mbar_expect_tx(&full[sidx], 3u * TC_PIECE + 3u * bbytes);
-#pragma unroll
-        for (int p = 0; p < 3; p++) {
-            bulk_g2s(sp + p * TC_PIECE, op.iA + p * op.termA + ((size_t)kb * op.ngA + op.ga) * TC_GROUP, TC_PIECE,
-                     &full[sidx]);
-            bulk_g2s(sp + (3 + p) * TC_PIECE, op.iB + p * op.termB + ((size_t)kb * op.ngB + op.gb) * TC_GROUP,
-                     bbytes, &full[sidx]);
-        }
-    };
-    if (tid == 0) {
-        for (int i = 0; i < TC_STAGES; i++) {
-            mbar_init(&full[i], 1);
-            mbar_init(&empty[i], 1);
-        }
-        mbar_init(&done, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        for (int kb = 0; kb < min(op.nkb, TC_STAGES); kb++) produce(kb);
-    }
-    pro();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = tmem_sh;
-    int late = 0;
-    if (tid == 0) {  // producer: the remaining K blocks, each once its stage is released
-        for (int kb = TC_STAGES; kb < op.nkb; kb++) {
-            if (!mbar_wait(&empty[kb % TC_STAGES], ((kb / TC_STAGES) - 1) & 1)) {
-                late = 1;
-                break;
-            }
-            produce(kb);
-        }
-    } else if (tid == 32) {  // MMA issuer
-        const uint32_t idesc = tc_idesc(op.nmma);
-        const uint32_t sbase = smem_u32(smem_raw);
-        for (int kb = 0; kb < op.nkb; kb++) {
-            const int sidx = kb % TC_STAGES;
-            if (!mbar_wait(&full[sidx], (kb / TC_STAGES) & 1)) {
-                late = 1;
-                break;
-            }
-            tc_fence_after();
-            const uint32_t st0 = sbase + sidx * TC_STAGE;
-#pragma unroll
-            for (int ks = 0; ks < TC_BK / 16; ks++) {
-#pragma unroll
-                for (int p = 0; p < 6; p++) {
-                    const int pa = (p == 2 || p == 4) ? 1 : (p == 5 ? 2 : 0);
-                    const int pb = (p == 1 || p == 4) ? 1 : (p == 3 ? 2 : 0);
-                    tc_mma(tmem, tc_desc(st0 + pa * TC_PIECE + ks * 256),
-                           tc_desc(st0 + (3 + pb) * TC_PIECE + ks * 256), idesc, (kb | ks | p) != 0);
-                }
-            }
-            tc_commit(&empty[sidx]);
-        }
-        if (!late) tc_commit(&done);
-    }
-    __syncwarp();
-    if (!mbar_wait(&done, 0)) late = 1;
-    const int aborted = __syncthreads_or(late);
-    tc_fence_after();
-    if (aborted) {
-        if (tid == 0) atomicExch(status, PGPU_STATUS_TIMEOUT);
-    } else {  // warp w reads accumulator lanes 32 w .. 32 w + 31, one tile row per thread
-        const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
-#pragma unroll 1
-        for (int c0 = 0; c0 < op.nmma; c0 += 16) {
-            float v[16];
-            tmem_ld16(taddr + c0, v);
-            epi(32 * warp + lane, c0, v);
-        }
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
-    return !aborted;
-}
-
-// imgA / imgB: the BF16 images holding the A and B operands of this kind
-// (POTRF: L, L; SYTRF: L, L D; GETRF: L and U, swapped on the U side).
-template <int FACT>
-__global__ void __launch_bounds__(128, 4) k_update_tc(DevStruct s, const UpdTile *__restrict__ tiles, float *L,
-                                                       float *U, const unsigned char *img0,
-                                                       const unsigned char *img1, const int64_t *__restrict__ sp_off,
-                                                       int *status) {
-    __shared__ int rt[TC_BM];
-    __shared__ int ct[TC_BN];
-    const UpdTile tl = tiles[blockIdx.x];
-    const TaskDev tk = s.tasks[tl.task];
-    const int k = tk.src, f = tk.dst;
-    const int K = s.cb_lcol[k] - s.cb_fcol[k] + 1;
-    const int st = s.cb_stride[k];
-    const int ra = tk.row0 + (tl.side ? tk.n : 0);  // first A row of the task
-    const int rend = tk.row0 + tk.m;                // end of the A rows
-    const int rb = tk.row0, rbe = tk.row0 + tk.n;   // B rows
-    const bool swap = (FACT == FACT_GETRF && tl.side == 1);
-    TcOperands op;
-    op.nkb = split_nkb(K);
-    op.ngA = op.ngB = split_ng(st);
-    op.termA = op.termB = (size_t)op.nkb * op.ngA * TC_GROUP;
-    op.ga = (ra >> 3) + 16 * tl.mt;
-    op.gb = (rb >> 3) + 16 * tl.nt;
-    op.nmma = (min(TC_BN, rbe - 8 * op.gb) + 15) & ~15;
-    op.iA = (swap ? img1 : img0) + sp_off[k];
-    op.iB = ((FACT == FACT_POTRF) ? img0 : (swap ? img0 : img1)) + sp_off[k];
-    float *Cp = (swap ? U : L) + s.cb_coef[f];
-    const int stf = s.cb_stride[f];
-    if (*(volatile int *)status != 0) return;  // an earlier tile gave up: leave the tensor cores alone
-    const int tid = threadIdx.x;
-    tc_tile(
-        op, status,
-        [&] {  // target rows and columns in the facing panel (-1: outside the task)
-            const int *ridx = s.rowidx + s.cb_rowidx[k];
-            const int pr = 8 * op.ga + tid;
-            int r = -1;
-            if (pr >= ra && pr < rend) {
-                const int g = ridx[pr];
-                int lo = s.cb_fblok[f], hi = s.cb_fblok[f + 1] - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (s.bk_frow[mid] <= g) lo = mid;
-                    else hi = mid - 1;
-                }
-                r = s.bk_rowoff[lo] + (g - s.bk_frow[lo]);
-            }
-            rt[tid] = r;
-            const int pc = 8 * op.gb + tid;
-            ct[tid] = (pc >= rb && pc < rbe) ? (ridx[pc] - s.cb_fcol[f]) : -1;
-        },
-        [&](int row, int c0, const float *v) {
-            const int rr = rt[row];
-            if (rr < 0) return;
-            float *dst[16];
-#pragma unroll
-            for (int j = 0; j < 16; j++) {
-                const int cc = ct[c0 + j];
-                dst[j] = (cc < 0) ? nullptr : Cp + rr + (size_t)cc * stf;
-            }
-            // reductions without return (no round trip) for every target, exclusive or not
-#pragma unroll
-            for (int j = 0; j < 16; j++)
-                if (dst[j]) atomicAdd(dst[j], -v[j]);
-        });
-}
 
 // ---------------------------------------------------------------------------
 // Inverse of the upper triangular factor T of a wide cblk's diagonal block
@@ -2022,46 +1853,12 @@ __global__ void __launch_bounds__(256) k_split_dense(const DenseSlab *__restrict
     }
 }
 
-// FP32 off-diagonal TRSM as the GEMM X = A T^{-1} on tcgen05: A from the
-// BF16 image of the panel taken before the TRSM, T^{-1} from the image of its
-// transpose (k_trinv, k_split_dense); the 128 x 128 tile of X overwrites the
-// panel rows below the diagonal block.  Tile: cblk, mt (128-row window from
-// the first off-diagonal row group), nt (128 columns), side (GETRF U panel).
-template <int FACT>
-__global__ void __launch_bounds__(128, 4) k_trsm_tc(DevStruct s, const UpdTile *__restrict__ tiles, float *L,
-                                                     float *U, const unsigned char *img0, const unsigned char *img1,
-                                                     const int64_t *__restrict__ sp_off,
-                                                     const unsigned char *timg, const int64_t *__restrict__ ti_img,
-                                                     int *status) {
-    const UpdTile tl = tiles[blockIdx.x];
-    const int k = tl.task;  // the cblk
-    const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
-    const int st = s.cb_stride[k];
-    const bool uside = (FACT == FACT_GETRF && tl.side == 1);
-    TcOperands op;
-    op.nkb = split_nkb(nc);
-    op.ngA = split_ng(st);
-    op.ngB = split_ng(nc);
-    op.termA = (size_t)op.nkb * op.ngA * TC_GROUP;
-    op.termB = (size_t)op.nkb * op.ngB * TC_GROUP;
-    op.ga = (nc >> 3) + 16 * tl.mt;
-    op.gb = 16 * tl.nt;
-    op.nmma = (min(TC_BN, nc - 128 * tl.nt) + 15) & ~15;
-    op.iA = (uside ? img1 : img0) + sp_off[k];
-    op.iB = timg + ti_img[k] + (uside ? (size_t)3 * op.termB : 0);
-    float *P = (uside ? U : L) + s.cb_coef[k];
-    if (*(volatile int *)status != 0) return;
-    tc_tile(
-        op, status, [] {},
-        [&](int row, int c0, const float *v) {
-            const int pr = 8 * op.ga + row;  // panel row
-            if (pr < nc || pr >= st) return;
-            const int cb = 128 * tl.nt + c0;
-#pragma unroll
-            for (int j = 0; j < 16; j++)
-                if (cb + j < nc) P[pr + (size_t)(cb + j) * st] = v[j];
-        });
-}
+// FP32 off-diagonal TRSM as the GEMM X = A T^{-1} on tcgen05 (k_trsm_tcp
+// below): A from the BF16 image of the panel taken before the TRSM, T^{-1}
+// from the image of its transpose (k_trinv, k_split_dense); the 128 x 128 tile
+// of X overwrites the panel rows below the diagonal block.  Tile: cblk, mt
+// (128-row window from the first off-diagonal row group), nt (128 columns),
+// side (GETRF U panel).
 
 // ---------------------------------------------------------------------------
 // Persistent, warp-specialized form of the tcgen05 tile loop.  A CTA walks the
@@ -2483,8 +2280,6 @@ cudaError_t set_smem_attrs(size_t, size_t, size_t) {
     if constexpr (sizeof(T) == 8) {
         if ((e = opt_in_smem(k_update_dmma<FACT>)) != cudaSuccess) return e;
     } else {
-        if ((e = opt_in_smem(k_update_tc<FACT>)) != cudaSuccess) return e;
-        if ((e = opt_in_smem(k_trsm_tc<FACT>)) != cudaSuccess) return e;
         if ((e = opt_in_smem(k_update_tcp<FACT>)) != cudaSuccess) return e;
         if ((e = opt_in_smem(k_trsm_tcp<FACT>)) != cudaSuccess) return e;
         if ((e = opt_in_smem(k_trinv<float, FACT>)) != cudaSuccess) return e;

@@ -51,6 +51,7 @@ void launch_update_tc(const DevStruct &, const UpdTile *, int, float *, float *,
 void launch_split(const DevStruct &, const SplitSlab *, int, const float *, const float *, const int64_t *,
                   unsigned char *, int, cudaStream_t);
 long long split_image_bytes(int nc, int st);
+long long panel_small_bytes(long long panel_elems, int tsize, int maxst);
 int trinv_max_blocks();
 template <int F>
 void launch_trinv(const DevStruct &, const int *, int, int, const float *, const float *, const float *,
@@ -164,6 +165,7 @@ struct LevelLists {
     int trsm_maxnc;         // widest cblk with TRSM tiles
     int diag_maxnc;         // widest cblk of the large list
     size_t small_smem_elems, diag_smem_elems, trsm_smem_elems;
+    int small_maxst;        // tallest narrow cblk (tables of the fused updates)
 };
 
 struct Device {
@@ -703,7 +705,8 @@ static int build_maps_and_lists(pastix_data_t *pd) {
     pd->split_slabs.clear();
     for (const auto &tk : sv.tasks) {
         const idx_t K = sv.cb_lcol[tk.src] - sv.cb_fcol[tk.src] + 1;
-        if (K >= TC_MIN_K && pd->sp_off[tk.src] < 0) pd->sp_off[tk.src] = 0;
+        if (K >= TC_MIN_K && K * sv.cb_stride[tk.src] > SMALL_PANEL_ELEMS && pd->sp_off[tk.src] < 0)
+            pd->sp_off[tk.src] = 0;
     }
     for (idx_t k = 0; k < sv.cblknbr; k++) {
         if (pd->sp_off[k] < 0) continue;
@@ -738,6 +741,7 @@ static int build_maps_and_lists(pastix_data_t *pd) {
         L.trsm_maxnc = 0;
         L.diag_maxnc = 0;
         L.small_smem_elems = L.diag_smem_elems = L.trsm_smem_elems = 0;
+        L.small_maxst = 0;
         for (idx_t p = sv.lvl_ptr[l]; p < sv.lvl_ptr[l + 1]; p++) {
             idx_t k = sv.lvl_cblk[p];
             idx_t nc = sv.cb_lcol[k] - sv.cb_fcol[k] + 1, st = sv.cb_stride[k];
@@ -746,6 +750,7 @@ static int build_maps_and_lists(pastix_data_t *pd) {
             if (st * nc <= SMALL_PANEL_ELEMS) {
                 pd->small_list.push_back((int)k);
                 L.small_smem_elems = std::max<size_t>(L.small_smem_elems, (size_t)(st * nc) * (fk == pgpu::FACT_GETRF ? 2 : 1));
+                L.small_maxst = std::max<int>(L.small_maxst, (int)st);
             } else {
                 pd->large_list.push_back((int)k);
                 pd->cb_dinv[k] = pd->dinv_total;
@@ -805,6 +810,7 @@ static int build_maps_and_lists(pastix_data_t *pd) {
         for (idx_t t = sv.lvl_task_ptr[l]; t < sv.lvl_task_ptr[l + 1]; t++) {
             const auto &tk = sv.tasks[t];
             const idx_t K = sv.cb_lcol[tk.src] - sv.cb_fcol[tk.src] + 1;
+            if (K * sv.cb_stride[tk.src] <= SMALL_PANEL_ELEMS) continue;  // done by k_panel_small
             const bool big = tk.n >= 32 && K >= 32;       // FP64: DMMA tiles
             const bool tc = K >= TC_MIN_K;                // FP32: tcgen05 tiles
             const idx_t BM = big ? 128 : 64, BN = 64;
@@ -1024,7 +1030,9 @@ static int run_factor(pastix_data_t *pd, double criterion) {
         const LevelLists &lv = pd->levels[l];
         launch_cls(pd, PC_PANEL_SMALL, lv.small1 - lv.small0, [&] {
             pgpu::launch_panel_small<T, F>(d.ds, d.small_list.p + lv.small0, lv.small1 - lv.small0,
-                                           lv.small_smem_elems * sizeof(T), L, U, fp, st);
+                                           (size_t)pgpu::panel_small_bytes((long long)lv.small_smem_elems,
+                                                                           (int)sizeof(T), lv.small_maxst),
+                                           L, U, fp, st);
         });
         launch_cls(pd, PC_DIAG_LARGE, lv.large1 - lv.large0, [&] {
             pgpu::launch_diag_large<T, F>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0, lv.diag_maxnc,

@@ -71,6 +71,12 @@ __global__ void k_fill_coef(int64_t nnz, const double *__restrict__ vals, const 
 // panel rows.  This is potf2/getf2/sytf2 on the diagonal block fused with the
 // off-diagonal TRSM.
 // ---------------------------------------------------------------------------
+constexpr int PS_FB_CACHE = 512;  // facing bloks whose first rows k_panel_small keeps in shared memory
+// Shared memory of k_panel_small: the panel (twice for GETRF) and its int tables.
+__host__ __device__ inline long long panel_small_smem_bytes(long long panel_elems, int tsize, int maxst) {
+    return panel_elems * tsize + 4LL * (2 * maxst + 2 * PS_FB_CACHE);
+}
+
 template <typename T, int FACT>
 __global__ void __launch_bounds__(256) k_panel_small(DevStruct s, const int *__restrict__ list, T *L, T *U,
                                                       FactParams fp) {
@@ -142,6 +148,64 @@ __global__ void __launch_bounds__(256) k_panel_small(DevStruct s, const int *__r
     }
     for (int i = tid; i < tot; i += nt) gL[i] = P[i];
     if (tid == 0 && npiv) atomicAdd(fp.nbpivots, npiv);
+    // the updates of every task of this cblk (core_zgemmsp_2d2d), from the
+    // factored panel still in shared memory, scattered into the facing panels
+    // with reductions; rtab / ctab: target rows and columns of one task
+    __syncthreads();
+    int *rtab = reinterpret_cast<int *>(P + (FACT == FACT_GETRF ? 2 : 1) * tot);
+    int *ctab = rtab + st;
+    int *fbr = ctab + st;           // first rows of the facing cblk's bloks (when they fit)
+    int *fbo = fbr + PS_FB_CACHE;   // and their row offsets
+    const int *ridx = s.rowidx + s.cb_rowidx[k];
+    for (int b = s.cb_fblok[k] + 1; b < s.cb_fblok[k + 1]; b++) {
+        const int f = s.bk_fcblk[b];
+        const int row0 = s.bk_rowoff[b];
+        const int n = s.bk_lrow[b] - s.bk_frow[b] + 1;
+        const int M = st - row0;
+        const int fb0 = s.cb_fblok[f], nbf = s.cb_fblok[f + 1] - fb0;
+        const bool cached = nbf <= PS_FB_CACHE;
+        if (cached)
+            for (int e = tid; e < nbf; e += nt) {
+                fbr[e] = s.bk_frow[fb0 + e];
+                fbo[e] = s.bk_rowoff[fb0 + e];
+            }
+        __syncthreads();
+        for (int i = tid; i < M; i += nt) {
+            const int g = ridx[row0 + i];
+            int lo = 0, hi = nbf - 1;
+            while (lo < hi) {  // last blok of f whose first row is <= g
+                const int mid = (lo + hi + 1) >> 1;
+                if ((cached ? fbr[mid] : s.bk_frow[fb0 + mid]) <= g) lo = mid;
+                else hi = mid - 1;
+            }
+            rtab[i] = (cached ? fbo[lo] : s.bk_rowoff[fb0 + lo]) + (g - (cached ? fbr[lo] : s.bk_frow[fb0 + lo]));
+        }
+        for (int j = tid; j < n; j += nt) ctab[j] = ridx[row0 + j] - s.cb_fcol[f];
+        __syncthreads();
+        T *Cl = L + s.cb_coef[f];
+        const int stf = s.cb_stride[f];
+        for (int e = tid; e < M * n; e += nt) {
+            const int i = e % M, j = e / M;
+            T v = T(0);
+            for (int c = 0; c < nc; c++) {
+                T bj = (FACT == FACT_GETRF) ? Q[(row0 + j) + c * st] : P[(row0 + j) + c * st];
+                if (FACT == FACT_SYTRF) bj *= P[c + c * st];
+                v += P[(row0 + i) + c * st] * bj;
+            }
+            atomicAdd(&Cl[rtab[i] + (size_t)ctab[j] * stf], -v);
+        }
+        if (FACT == FACT_GETRF) {  // U side: rows strictly below the blok, into the U panel of f
+            T *Cu = U + s.cb_coef[f];
+            const int M1 = M - n;
+            for (int e = tid; e < M1 * n; e += nt) {
+                const int i = n + e % M1, j = e / M1;
+                T v = T(0);
+                for (int c = 0; c < nc; c++) v += Q[(row0 + i) + c * st] * P[(row0 + j) + c * st];
+                atomicAdd(&Cu[rtab[i] + (size_t)ctab[j] * stf], -v);
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -2252,6 +2316,9 @@ void launch_split(const DevStruct &s, const SplitSlab *slabs, int count, const f
 }
 
 long long split_image_bytes(int nc, int st) { return split_bytes(nc, st); }
+long long panel_small_bytes(long long panel_elems, int tsize, int maxst) {
+    return panel_small_smem_bytes(panel_elems, tsize, maxst);
+}
 int trinv_max_blocks() { return DG_MAXNC / 32; }
 
 // Opt every kernel with dynamic shared memory into the largest size the

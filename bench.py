@@ -380,7 +380,7 @@ def main():
         except Exception:
             traffic = None
     if best == "mixed":
-        roof = {"kernel": "k_update_tc (FP32 supernode update GEMMs on tcgen05, split BF16 terms, scatter-add)",
+        roof = {"kernel": "k_update_tcp (FP32 supernode update GEMMs on tcgen05, split BF16 terms, scatter-add)",
                 "bound": "tensor", "achieved": ach32, "peak": peak32, "unit": "TFLOP/s",
                 "frac": (ach32 / peak32) if ach32 else None, "traffic": traffic,
                 "peak_source": ("measured dense bf16 %s TFLOP/s (MEASURED_PEAKS.json, burst) / 6 BF16 products per "

@@ -154,6 +154,7 @@ struct LevelLists {
     int upds0, upds1;       // k_update tiles (64 x 64), FP32 factors (tasks the tcgen05 kernel does not take)
     int updb0, updb1;       // big update tiles (128 x 64): DMMA for FP64
     int updt0, updt1;       // the same tasks in 128-row aligned windows: tcgen05 for FP32
+    int updtn, updsn;       // FP32 lists: tiles before these target the next level's cblks
     int spl0, spl1;         // 128-row slabs of the level's cblks split into BF16 terms (FP32)
     int tt0, tt1;           // FP32 TRSM as GEMM tiles (tcgen05), task = cblk
     int ds0, ds1;           // 128-row slabs of the transposed triangular inverses
@@ -172,6 +173,8 @@ struct Device {
     bool ready = false;
     int dev = -1;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;                      // FP32 factorization: updates of later levels
+    std::vector<cudaEvent_t> ev_chain, ev_rest;       // per level: panels final / far updates done
     // structure
     DBuf<int> cb_fcol, cb_lcol, cb_stride, cb_fblok, bk_frow, bk_lrow, bk_rowoff, bk_fcblk, rowidx;
     DBuf<int64_t> cb_coef, cb_rowidx, cb_dinv, sp_off;
@@ -256,18 +259,20 @@ struct pastix_data_s {
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_ev;
 };
 
-// Run one launch of kernel class `cls` with `count` blocks through `fn`.
+// Run one launch of kernel class `cls` with `count` blocks through `fn`, on
+// stream `st` (the library stream by default).
 template <typename Fn>
-static inline void launch_cls(pastix_data_t *pd, int cls, long long count, Fn &&fn) {
+static inline void launch_cls(pastix_data_t *pd, int cls, long long count, Fn &&fn, cudaStream_t st = nullptr) {
     if (count <= 0) return;
     pd->launches[cls]++;
     if (!pd->prof_on) { fn(); return; }
+    if (!st) st = pd->dev.stream;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    cudaEventRecord(a, pd->dev.stream);
+    cudaEventRecord(a, st);
     fn();
-    cudaEventRecord(b, pd->dev.stream);
+    cudaEventRecord(b, st);
     pd->prof_ev.push_back({cls, {a, b}});
 }
 
@@ -807,6 +812,7 @@ static int build_maps_and_lists(pastix_data_t *pd) {
         L.updb0 = (int)pd->upd_big_tiles.size();
         L.updt0 = (int)pd->upd_tc_tiles.size();
         L.upds0 = (int)pd->upd_tiles32.size();
+        std::vector<pgpu::UpdTile> tc_far, s32_far;  // tiles whose target is two or more levels up
         for (idx_t t = sv.lvl_task_ptr[l]; t < sv.lvl_task_ptr[l + 1]; t++) {
             const auto &tk = sv.tasks[t];
             const idx_t K = sv.cb_lcol[tk.src] - sv.cb_fcol[tk.src] + 1;
@@ -825,12 +831,13 @@ static int build_maps_and_lists(pastix_data_t *pd) {
                         if (fk != pgpu::FACT_GETRF && (a + 1) * BM <= c * BN) continue;
                         list.push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
                     }
+                const bool near = sv.cb_level[tk.dst] == (idx_t)l + 1;
                 if (!tc) {  // FP32 tasks with a narrow source: SIMT 64 x 64 tiles
                     const idx_t mt3 = (M + 63) / 64, nt3 = (tk.n + 63) / 64;
                     for (idx_t a = 0; a < mt3; a++)
                         for (idx_t c = 0; c < nt3; c++) {
                             if (fk != pgpu::FACT_GETRF && (a + 1) * 64 <= c * 64) continue;
-                            pd->upd_tiles32.push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
+                            (near ? pd->upd_tiles32 : s32_far).push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
                         }
                 }
                 if (tc) {  // tcgen05 tiles (FP32 factors): 128-row windows aligned to groups of 8 rows
@@ -840,13 +847,17 @@ static int build_maps_and_lists(pastix_data_t *pd) {
                     for (idx_t a = 0; a < mt2; a++)
                         for (idx_t c = 0; c < nt2; c++) {
                             if (fk != pgpu::FACT_GETRF && (a + 1) * TB <= c * TB) continue;
-                            pd->upd_tc_tiles.push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
+                            (near ? pd->upd_tc_tiles : tc_far).push_back(pgpu::UpdTile{(int)t, (int)a, (int)c, side});
                         }
                 }
             }
         }
         L.upd1 = (int)pd->upd_tiles.size();
         L.updb1 = (int)pd->upd_big_tiles.size();
+        L.updtn = (int)pd->upd_tc_tiles.size();
+        L.updsn = (int)pd->upd_tiles32.size();
+        pd->upd_tc_tiles.insert(pd->upd_tc_tiles.end(), tc_far.begin(), tc_far.end());
+        pd->upd_tiles32.insert(pd->upd_tiles32.end(), s32_far.begin(), s32_far.end());
         L.updt1 = (int)pd->upd_tc_tiles.size();
         L.upds1 = (int)pd->upd_tiles32.size();
     }
@@ -942,6 +953,14 @@ static int device_setup(pastix_data_t *pd) {
     if (d.dev < 0) CUDA_TRY(cudaGetDevice(&d.dev));
     CUDA_TRY(cudaSetDevice(d.dev));
     if (!d.stream) CUDA_TRY(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
+    if (!d.side) CUDA_TRY(cudaStreamCreateWithFlags(&d.side, cudaStreamNonBlocking));
+    while (d.ev_chain.size() < pd->levels.size()) {
+        cudaEvent_t a, b;
+        CUDA_TRY(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+        d.ev_chain.push_back(a);
+        d.ev_rest.push_back(b);
+    }
     cudaStream_t st = d.stream;
     const pgpu::Solver &sv = pd->solver;
     if (sv.n >= INT32_MAX || (idx_t)sv.rowidx.size() >= INT32_MAX) { perr("problem too large"); return PASTIX_ERR_INTEGER_TYPE; }
@@ -1026,8 +1045,16 @@ static int run_factor(pastix_data_t *pd, double criterion) {
     T *U = reinterpret_cast<T *>(d.Uc.p);
     T *Dinv = reinterpret_cast<T *>(d.dinv.p);
     pgpu::FactParams fp{criterion, d.counters.p, d.counters.p + 1};
+    // FP32: the updates of level l whose targets sit two or more levels up run on a
+    // second stream and overlap level l + 1 (all FP32 update writes are reductions)
+    const bool two = sizeof(T) == 4;
+    if (two) {
+        CUDA_TRY(cudaEventRecord(d.ev_chain[0], st));
+        CUDA_TRY(cudaStreamWaitEvent(d.side, d.ev_chain[0], 0));
+    }
     for (size_t l = 0; l < pd->levels.size(); l++) {
         const LevelLists &lv = pd->levels[l];
+        if (two && l >= 2) CUDA_TRY(cudaStreamWaitEvent(st, d.ev_rest[l - 2], 0));
         launch_cls(pd, PC_PANEL_SMALL, lv.small1 - lv.small0, [&] {
             pgpu::launch_panel_small<T, F>(d.ds, d.small_list.p + lv.small0, lv.small1 - lv.small0,
                                            (size_t)pgpu::panel_small_bytes((long long)lv.small_smem_elems,
@@ -1066,8 +1093,8 @@ static int run_factor(pastix_data_t *pd, double criterion) {
                 pgpu::launch_update<T, F>(d.ds, d.upd_tiles.p + lv.upd0, lv.upd1 - lv.upd0, L, U, st);
             });
         } else {
-            launch_cls(pd, PC_UPDATE, lv.upds1 - lv.upds0, [&] {
-                pgpu::launch_update<T, F>(d.ds, d.upd_tiles32.p + lv.upds0, lv.upds1 - lv.upds0, L, U, st);
+            launch_cls(pd, PC_UPDATE, lv.updsn - lv.upds0, [&] {
+                pgpu::launch_update<T, F>(d.ds, d.upd_tiles32.p + lv.upds0, lv.updsn - lv.upds0, L, U, st);
             });
         }
         if constexpr (sizeof(T) == 4) {
@@ -1078,15 +1105,36 @@ static int run_factor(pastix_data_t *pd, double criterion) {
                 if (F == pgpu::FACT_SYTRF) pgpu::launch_split(d.ds, sl, cnt, L, L, d.sp_off.p, d.img1.p, 1, st);
                 if (F == pgpu::FACT_GETRF) pgpu::launch_split(d.ds, sl, cnt, U, L, d.sp_off.p, d.img1.p, 0, st);
             });
-            launch_cls(pd, PC_UPDATE_BIG, lv.updt1 - lv.updt0, [&] {
-                pgpu::launch_update_tc<F>(d.ds, d.upd_tc_tiles.p + lv.updt0, lv.updt1 - lv.updt0, L, U, d.img0.p,
+            launch_cls(pd, PC_UPDATE_BIG, lv.updtn - lv.updt0, [&] {
+                pgpu::launch_update_tc<F>(d.ds, d.upd_tc_tiles.p + lv.updt0, lv.updtn - lv.updt0, L, U, d.img0.p,
                                           d.img1.p, d.sp_off.p, d.counters.p + 1, st);
             });
+            // far targets on the side stream, once this level's panels and images are final
+            CUDA_TRY(cudaEventRecord(d.ev_chain[l], st));
+            CUDA_TRY(cudaStreamWaitEvent(d.side, d.ev_chain[l], 0));
+            launch_cls(
+                pd, PC_UPDATE, lv.upds1 - lv.updsn,
+                [&] {
+                    pgpu::launch_update<T, F>(d.ds, d.upd_tiles32.p + lv.updsn, lv.upds1 - lv.updsn, L, U, d.side);
+                },
+                d.side);
+            launch_cls(
+                pd, PC_UPDATE_BIG, lv.updt1 - lv.updtn,
+                [&] {
+                    pgpu::launch_update_tc<F>(d.ds, d.upd_tc_tiles.p + lv.updtn, lv.updt1 - lv.updtn, L, U,
+                                              d.img0.p, d.img1.p, d.sp_off.p, d.counters.p + 1, d.side);
+                },
+                d.side);
+            CUDA_TRY(cudaEventRecord(d.ev_rest[l], d.side));
         } else {
             launch_cls(pd, PC_UPDATE_BIG, lv.updb1 - lv.updb0, [&] {
                 pgpu::launch_update_big<T, F>(d.ds, d.upd_big_tiles.p + lv.updb0, lv.updb1 - lv.updb0, L, U, st);
             });
         }
+    }
+    if (two) {  // the library stream resumes once every far update is in
+        CUDA_TRY(cudaEventRecord(d.ev_chain[0], d.side));
+        CUDA_TRY(cudaStreamWaitEvent(st, d.ev_chain[0], 0));
     }
     CUDA_TRY(cudaGetLastError());
     return PASTIX_SUCCESS;

@@ -714,7 +714,7 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
             int rr = rt[tx + i * TX];
             dst[i] = (rr < 0) ? nullptr : Cp + rr + (size_t)cc * stf;
         }
-        if (tk.excl) {
+        if (tk.excl && sizeof(T) == 8) {  // FP32 updates of different levels may overlap: reductions only
             T old[TM];
 #pragma unroll
             for (int i = 0; i < TM; i++) old[i] = dst[i] ? *dst[i] : T(0);

@@ -1047,7 +1047,9 @@ static int run_factor(pastix_data_t *pd, double criterion) {
     pgpu::FactParams fp{criterion, d.counters.p, d.counters.p + 1};
     // FP32: the updates of level l whose targets sit two or more levels up run on a
     // second stream and overlap level l + 1 (all FP32 update writes are reductions)
-    const bool two = sizeof(T) == 4;
+    // (the profiled pass keeps one stream so that each class's events time it alone)
+    const bool two = sizeof(T) == 4 && !pd->prof_on;
+    const cudaStream_t sd = two ? d.side : st;
     if (two) {
         CUDA_TRY(cudaEventRecord(d.ev_chain[0], st));
         CUDA_TRY(cudaStreamWaitEvent(d.side, d.ev_chain[0], 0));
@@ -1110,22 +1112,24 @@ static int run_factor(pastix_data_t *pd, double criterion) {
                                           d.img1.p, d.sp_off.p, d.counters.p + 1, st);
             });
             // far targets on the side stream, once this level's panels and images are final
-            CUDA_TRY(cudaEventRecord(d.ev_chain[l], st));
-            CUDA_TRY(cudaStreamWaitEvent(d.side, d.ev_chain[l], 0));
+            if (two) {
+                CUDA_TRY(cudaEventRecord(d.ev_chain[l], st));
+                CUDA_TRY(cudaStreamWaitEvent(d.side, d.ev_chain[l], 0));
+            }
             launch_cls(
                 pd, PC_UPDATE, lv.upds1 - lv.updsn,
                 [&] {
-                    pgpu::launch_update<T, F>(d.ds, d.upd_tiles32.p + lv.updsn, lv.upds1 - lv.updsn, L, U, d.side);
+                    pgpu::launch_update<T, F>(d.ds, d.upd_tiles32.p + lv.updsn, lv.upds1 - lv.updsn, L, U, sd);
                 },
-                d.side);
+                sd);
             launch_cls(
                 pd, PC_UPDATE_BIG, lv.updt1 - lv.updtn,
                 [&] {
                     pgpu::launch_update_tc<F>(d.ds, d.upd_tc_tiles.p + lv.updtn, lv.updt1 - lv.updtn, L, U,
-                                              d.img0.p, d.img1.p, d.sp_off.p, d.counters.p + 1, d.side);
+                                              d.img0.p, d.img1.p, d.sp_off.p, d.counters.p + 1, sd);
                 },
-                d.side);
-            CUDA_TRY(cudaEventRecord(d.ev_rest[l], d.side));
+                sd);
+            if (two) CUDA_TRY(cudaEventRecord(d.ev_rest[l], d.side));
         } else {
             launch_cls(pd, PC_UPDATE_BIG, lv.updb1 - lv.updb0, [&] {
                 pgpu::launch_update_big<T, F>(d.ds, d.upd_big_tiles.p + lv.updb0, lv.updb1 - lv.updb0, L, U, st);

@@ -1084,88 +1084,95 @@ __device__ __forceinline__ double dg_t(const double *W, int a, int b, int side) 
     return (a == b) ? 1.0 : W[b * DG_LD + a];
 }
 
-// One warp: Z = T_jj^{-1} of the nb x nb leading block (identity beyond), to
-// shared memory (row major, ld DG_LD) and to `gZ` (32 x 32 row major).  Lane j
-// forms column j by back substitution.  A full block (nb = 32, every block
-// but possibly a cblk's last) runs fully unrolled without guards, so its
-// broadcast reads of T are issued ahead of the dependent sums.  Kept out of
-// line: inlined into the large factorization kernels its 32-entry column
-// would be demoted to local memory.
-template <typename T, int FACT>
-__device__ __noinline__ void dg_inverse(const double *W, int nb, int side, double *Z, T *gZ) {
-    const int lane = threadIdx.x & 31;
-    const double rl = (lane < nb) ? 1.0 / dg_t<FACT>(W, lane, lane, side) : 1.0;
-    if (nb == 32) {
-        double z[32];
-#pragma unroll
-        for (int i = 31; i >= 0; i--) {
-            double a0 = 0.0, a1 = 0.0;
-#pragma unroll
-            for (int kk = i + 1; kk < 32; kk++) {
-                if ((kk - i) & 1) a0 += dg_t<FACT>(W, i, kk, side) * z[kk];
-                else a1 += dg_t<FACT>(W, i, kk, side) * z[kk];
-            }
-            const double ri = __shfl_sync(0xffffffffu, rl, i);
-            z[i] = (i > lane) ? 0.0 : ((i == lane) ? rl : -(a0 + a1) * ri);
-        }
-#pragma unroll
-        for (int i = 0; i < 32; i++) {
-            Z[i * DG_LD + lane] = z[i];
-            gZ[i * 32 + lane] = (T)z[i];
-        }
-        return;
+// Pivot of a factorization step: the (warp-uniform) diagonal value a after
+// static pivoting, and the reciprocal that scales its column.  POTRF takes one
+// reciprocal square root: d = a rsqrt(a), 1 / d = rsqrt(a).
+template <int FACT>
+__device__ __forceinline__ void dg_pivot(double a, double crit, int &np, double &d, double &inv) {
+    if (fabs(a) < crit) {
+        a = (FACT == FACT_POTRF || a >= 0.0) ? crit : -crit;
+        np++;
     }
-    for (int i = 31; i >= 0; i--) {  // partial block: column kept in Z itself
-        double acc = 0.0;
-        for (int kk = i + 1; kk < nb; kk++) acc += dg_t<FACT>(W, i, kk, side) * Z[kk * DG_LD + lane];
-        const double ri = __shfl_sync(0xffffffffu, rl, i);
-        Z[i * DG_LD + lane] = (i > lane) ? 0.0 : ((i == lane) ? rl : -acc * ri);
+    if (FACT == FACT_POTRF) {
+        const double rs = rsqrt(a);
+        d = a * rs;
+        inv = rs;
+    } else {
+        d = a;
+        inv = 1.0 / a;
     }
-    for (int i = 0; i < 32; i++) gZ[i * 32 + lane] = (T)Z[i * DG_LD + lane];
 }
+
+constexpr int DG_BLD = 34;        // row stride (doubles) of the published factor steps
+constexpr int DG_SPIN = 1 << 22;  // bound on a warp's wait for the factorization's progress
+constexpr int PGPU_STATUS_TIMEOUT = 3;
 
 // One warp: factor the nb x nb top block held row major in W (ld DG_LD) in
 // place, one row per lane in registers, with static pivoting; returns the
 // number of replaced pivots.  POTRF leaves L (lower), SYTRF L (unit, strictly
-// lower) and D on the diagonal, GETRF L (unit, strictly lower) and U.  The
-// column (or, for GETRF, the row) of each step reaches the other lanes through
-// the 32-entry shared vector Ls as broadcast reads: a dependent chain of warp
-// shuffles costs several times more per step.
+// lower) and D on the diagonal, GETRF L (unit, strictly lower) and U.
+//
+// Step c publishes, in row c of Pub (ld DG_BLD, 16-byte aligned), what the
+// other lanes need for their update and what the inverse warps need, then
+// bumps *prog to c + 1:
+//   POTRF  Pub[c][i] = L(i, c)           (i > c), d_c at i = c;
+//   SYTRF  Pub[c][i] = D(c) L(i, c)      (i > c), d_c at i = c;
+//   GETRF  Pub[c][j] = row c of L \ U    (L(c, j) for j < c, d_c, U(c, j) for j > c);
+// and Pub[c][32] = 1 / d_c.  The row is read back as 16-byte pairs; each step
+// updates and pivots the next column before the rest of the row, so the
+// reciprocal (square root) of the next pivot overlaps the remaining updates.
 template <int FACT, bool FULL>
-__device__ __forceinline__ int dg_factor32_impl(double *W, int nbr, double crit, double *Ls) {
+__device__ __forceinline__ int dg_factor32_impl(double *W, int nbr, double crit, double *Pub, volatile int *prog) {
     const int nb = FULL ? 32 : nbr;  // a full block compiles without any bound test
     const int lane = threadIdx.x & 31;
     double r[32];
 #pragma unroll
     for (int j = 0; j < 32; j++) r[j] = (lane < nb && j < nb) ? W[lane * DG_LD + j] : (lane == j ? 1.0 : 0.0);
     int np = 0;
+    double d, inv;
+    dg_pivot<FACT>(__shfl_sync(0xffffffffu, r[0], 0), crit, np, d, inv);
 #pragma unroll
     for (int c = 0; c < 32; c++) {
         if (c < nb) {
-            const double d = static_pivot<double, FACT>(__shfl_sync(0xffffffffu, r[c], c), crit, np);
-            const double inv = 1.0 / d;
+            double *Pc = Pub + c * DG_BLD;
             const double u = r[c];
             if (lane == c) r[c] = d;
             else if (lane > c) r[c] *= inv;
-            if (FACT == FACT_POTRF) Ls[lane] = r[c];
-            else if (FACT == FACT_SYTRF) Ls[lane] = u;
-            else if (lane == c) {
+            if (FACT == FACT_GETRF) {
+                if (lane == c) {
 #pragma unroll
-                for (int j = 0; j < 32; j++) Ls[j] = r[j];
-            }
-            __syncwarp();
-            // no j < nb guard: beyond nb both Ls and the padded lanes' entries are zero,
-            // and an unguarded loop lets the 31 broadcast reads issue back to back
-#pragma unroll
-            for (int j = c + 1; j < 32; j++) {
-                const double v = Ls[j];
-                if (FACT == FACT_GETRF) {
-                    if (lane > c) r[j] -= r[c] * v;
-                } else if (lane >= j) {
-                    r[j] -= r[c] * v;
+                    for (int j = 0; j < 32; j += 2) *reinterpret_cast<double2 *>(Pc + j) = make_double2(r[j], r[j + 1]);
+                    Pc[32] = inv;
                 }
+            } else {
+                Pc[lane] = (FACT == FACT_SYTRF && lane != c) ? u : r[c];
+                if (lane == c) Pc[32] = inv;
             }
             __syncwarp();
+            if (lane == 0) {
+                __threadfence_block();
+                *prog = c + 1;
+            }
+            double v[32];
+#pragma unroll
+            for (int j = (c + 1) & ~1; j < 32; j += 2) {
+                const double2 t = *reinterpret_cast<const double2 *>(Pc + j);
+                v[j] = t.x;
+                v[j + 1] = t.y;
+            }
+            auto upd = [&](int j) {
+                if (FACT == FACT_GETRF) {
+                    if (lane > c) r[j] -= r[c] * v[j];
+                } else if (lane >= j) {
+                    r[j] -= r[c] * v[j];
+                }
+            };
+            if (c + 1 < 32) {
+                upd(c + 1);
+                if (c + 1 < nb) dg_pivot<FACT>(__shfl_sync(0xffffffffu, r[c + 1], c + 1), crit, np, d, inv);
+            }
+#pragma unroll
+            for (int j = c + 2; j < 32; j++) upd(j);
         }
     }
     if (lane < nb)
@@ -1174,9 +1181,167 @@ __device__ __forceinline__ int dg_factor32_impl(double *W, int nbr, double crit,
             if (j < nb) W[lane * DG_LD + j] = r[j];
     return np;
 }
+// POTRF / SYTRF: the same factorization and publication by blocks of 8
+// columns, so that the lanes exchange data once per block instead of once per
+// column.  Step b: the 8 rows of the diagonal block write their entries to
+// Blk; every lane factors that 8 x 8 block itself (the same arithmetic in every
+// lane), solves its own row against it, writes and publishes the 8 values
+// (Pub as above; Blk + 64 keeps row r's 8 values contiguous for the update)
+// and updates the rest of its row; the row then moves 8 places left, so the
+// loop over the blocks runs rolled with static register indices.  `Blk`: 320
+// doubles, 16-byte aligned.
 template <int FACT>
-__device__ __forceinline__ int dg_factor32(double *W, int nb, double crit, double *Ls) {
-    return (nb == 32) ? dg_factor32_impl<FACT, true>(W, 32, crit, Ls) : dg_factor32_impl<FACT, false>(W, nb, crit, Ls);
+__device__ __noinline__ int dg_factor32_sym(double *W, int nb, double crit, double *Pub, volatile int *prog,
+                                            double *Blk) {
+    const int lane = threadIdx.x & 31;
+    double *D8 = Blk, *Xr = Blk + 64;
+    double r[32];
+#pragma unroll
+    for (int j = 0; j < 32; j++) r[j] = (lane < nb && j < nb) ? W[lane * DG_LD + j] : (lane == j ? 1.0 : 0.0);
+    int np = 0;
+#pragma unroll 1
+    for (int jb = 0; jb < nb; jb += 8) {
+        const int q = lane - jb;
+        if (q >= 0 && q < 8) {
+#pragma unroll
+            for (int c = 0; c < 8; c += 2) *reinterpret_cast<double2 *>(D8 + q * 8 + c) = make_double2(r[c], r[c + 1]);
+        }
+        __syncwarp();
+        double a[8][8];
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+#pragma unroll
+            for (int c = 0; c <= i; c += 2) {
+                const double2 t = *reinterpret_cast<const double2 *>(D8 + i * 8 + c);
+                a[i][c] = t.x;
+                a[i][c + 1] = t.y;
+            }
+        // the 8 x 8 diagonal block, right looking (every lane alike)
+        double dd[8], iv[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            if (jb + c < nb) {
+                dg_pivot<FACT>(a[c][c], crit, np, dd[c], iv[c]);
+            } else {  // padding beyond nb: identity
+                dd[c] = 1.0;
+                iv[c] = 1.0;
+            }
+            double uc[8], lc[8];
+#pragma unroll
+            for (int i = c + 1; i < 8; i++) {
+                uc[i] = a[i][c];
+                lc[i] = uc[i] * iv[c];
+                a[i][c] = lc[i];
+            }
+#pragma unroll
+            for (int j = c + 1; j < 8; j++)
+#pragma unroll
+                for (int i = j; i < 8; i++) a[i][j] -= lc[i] * ((FACT == FACT_SYTRF) ? uc[j] : lc[j]);
+        }
+        // this lane's 8 values: L below the block's diagonal, the pivot on it, the
+        // untouched upper part above it
+        double x[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            double s0 = r[c], s1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < c; k++) {
+                const double m = (FACT == FACT_SYTRF) ? a[c][k] * dd[k] : a[c][k];
+                if (k & 1) s1 -= x[k] * m;
+                else s0 -= x[k] * m;
+            }
+            const double xc = (s0 + s1) * iv[c];
+            x[c] = (lane > jb + c) ? xc : ((lane == jb + c) ? dd[c] : r[c]);
+        }
+        double pv[8];  // published: POTRF L(i, c); SYTRF D(c) L(i, c); the pivot on the diagonal
+#pragma unroll
+        for (int c = 0; c < 8; c++) pv[c] = (FACT == FACT_SYTRF && lane != jb + c) ? x[c] * dd[c] : x[c];
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            if (jb + c < nb) {
+                if (lane < nb) W[lane * DG_LD + jb + c] = x[c];
+                Pub[(jb + c) * DG_BLD + lane] = pv[c];
+                if (lane == c) Pub[(jb + c) * DG_BLD + 32] = iv[c];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 8; c += 2) *reinterpret_cast<double2 *>(Xr + lane * 8 + c) = make_double2(pv[c], pv[c + 1]);
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence_block();
+            *prog = min(jb + 8, nb);
+        }
+        // rank-8 update of the rest of the row (lower part: columns jb + j <= lane)
+#pragma unroll
+        for (int j = 8; j < 32; j++) {
+            if (lane >= jb + j) {
+                const double *xr = Xr + (jb + j) * 8;
+                double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < 8; c += 2) {
+                    const double2 t = *reinterpret_cast<const double2 *>(xr + c);
+                    s0 += x[c] * t.x;
+                    s1 += x[c + 1] * t.y;
+                }
+                r[j] -= s0 + s1;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 24; j++) r[j] = r[j + 8];
+#pragma unroll
+        for (int j = 24; j < 32; j++) r[j] = 0.0;
+        __syncwarp();  // D8 and Xr are rewritten by the next block
+    }
+    return np;
+}
+
+template <int FACT>
+__device__ __forceinline__ int dg_factor32(double *W, int nb, double crit, double *Pub, volatile int *prog) {
+    if (FACT != FACT_GETRF) return dg_factor32_sym<FACT>(W, nb, crit, Pub, prog, Pub + 32 * DG_BLD);
+    return (nb == 32) ? dg_factor32_impl<FACT, true>(W, 32, crit, Pub, prog)
+                      : dg_factor32_impl<FACT, false>(W, nb, crit, Pub, prog);
+}
+
+// One warp, next to the factorization of the top block: Z = T_jj^{-1} (side 0;
+// side 1: GETRF's L^T) to shared memory (row major, ld DG_LD) and to `gZ`
+// (32 x 32 row major), identity beyond nb.  With M = T^T lower triangular
+// (POTRF L, SYTRF L D, GETRF U^T, or L for side 1), Z = (M^{-1})^T: lane j
+// forms column j of M^{-1} by forward substitution, row i as soon as the
+// factorization has published step i (M(i, k) = Pub[k][i], side 1 Pub[i][k]),
+// so the inverse ends one step after the factorization.  A wait that runs
+// past its bound records PGPU_STATUS_TIMEOUT in `status` and stops waiting.
+template <typename T, int FACT>
+__device__ __forceinline__ void dg_inverse_pipe(const double *Pub, int nb, int side, const volatile int *prog,
+                                                double *Z, T *gZ, int *status) {
+    const int lane = threadIdx.x & 31;
+    const bool lower_l = FACT == FACT_GETRF && side == 1;
+    double y[32];
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+        if (i < nb) {
+            for (int spins = 0; ok && *prog <= i;)
+                if (++spins > DG_SPIN) ok = false;
+            __threadfence_block();
+            const double rinv = lower_l ? 1.0 : Pub[i * DG_BLD + 32];
+            double a0 = (i == lane) ? 1.0 : 0.0, a1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < i; k++) {
+                const double m = lower_l ? Pub[i * DG_BLD + k] : Pub[k * DG_BLD + i];
+                if (k & 1) a1 -= m * y[k];
+                else a0 -= m * y[k];
+            }
+            y[i] = (a0 + a1) * rinv;
+        } else {
+            y[i] = (i == lane) ? 1.0 : 0.0;
+        }
+    }
+    if (!ok && lane == 0) atomicExch(status, PGPU_STATUS_TIMEOUT);
+#pragma unroll
+    for (int i = 0; i < 32; i++) Z[lane * DG_LD + i] = y[i];
+    __syncwarp();
+#pragma unroll 4
+    for (int i = 0; i < 32; i++) gZ[i * 32 + lane] = (T)Z[i * DG_LD + lane];
 }
 
 // CTA-wide transfer of a rows x cols region in 8 x 4 sub-tiles: lane (g, t4)
@@ -1263,9 +1428,9 @@ __global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *W = reinterpret_cast<double *>(smem_raw);  // (nc - jb) x 32 panel, row major, ld DG_LD
     __shared__ double Z0[32 * DG_LD], Z1[32 * DG_LD];
-    __shared__ double Sx[8][8 * DG_LD];
-    __shared__ double dsh[32], Ls[32];
-    __shared__ int npiv;
+    __shared__ __align__(16) double Sx[8][8 * DG_LD];  // also the published steps of the top block's factorization
+    __shared__ double dsh[32];
+    __shared__ int npiv, prog;
     const int k = list[blockIdx.x];
     const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
     const int st = s.cb_stride[k];
@@ -1287,15 +1452,19 @@ __global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__
         dg_copy<4>(
             m, 32, [&](int r, int c) { return (c < nb) ? (double)Ap[r + (size_t)c * st] : 0.0; },
             [&](int r, int c, double v) { W[r * DG_LD + c] = v; });
+        if (tid == 0) prog = 0;
         __syncthreads();
-        // 2. factor the top block (warp 0), one row per lane in registers
+        // 2. factor the top block (warp 0), one row per lane in registers; its inverse(s)
+        //    one step behind (warps 1 and 2)
         if (warp == 0) {
-            const int np = dg_factor32<FACT>(W, nb, fp.criterion, Ls);
+            const int np = dg_factor32<FACT>(W, nb, fp.criterion, &Sx[0][0], &prog);
             if (lane == 0 && np) npiv += np;
+        } else if (warp == 1) {
+            dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 0, &prog, Z0, gZ + (size_t)(jb / 32) * 1024, fp.status);
+        } else if (FACT == FACT_GETRF && warp == 2) {
+            dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 1, &prog, Z1, gZ + (size_t)(nzb + jb / 32) * 1024, fp.status);
         }
         __syncthreads();
-        if (warp == 0) dg_inverse<T, FACT>(W, nb, 0, Z0, gZ + (size_t)(jb / 32) * 1024);
-        if (FACT == FACT_GETRF && warp == 1) dg_inverse<T, FACT>(W, nb, 1, Z1, gZ + (size_t)(nzb + jb / 32) * 1024);
         if (FACT == FACT_SYTRF && tid < 32) dsh[tid] = (tid < nb) ? W[tid * DG_LD + tid] : 0.0;
         __syncthreads();
         // 3. rows below the block (and the U strip of GETRF), 8 rows per warp
@@ -1456,9 +1625,9 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *Wl = reinterpret_cast<double *>(smem_raw);  // this CTA's panels, one after the other
     __shared__ double Zs[2][32 * DG_LD];                 // inverted top blocks of the last panel factored here
-    __shared__ double Sx[8][8 * DG_LD];
-    __shared__ double Tb[32 * DG_LD], Ls[32];            // the top block being factored
-    __shared__ int npiv;
+    __shared__ __align__(16) double Sx[8][8 * DG_LD];  // also the published steps of the top block's factorization
+    __shared__ double Tb[32 * DG_LD];                    // the top block being factored
+    __shared__ int npiv, prog;
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
     const int k = list[blockIdx.x / DC];
@@ -1503,14 +1672,17 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
             double *W = Wl + poff(p);
             double *Wt = W + (32 * p - lop) * DG_LD;  // top block
             for (int e = tid; e < nb * DG_LD; e += blockDim.x) Tb[e] = Wt[e];  // the panel has nb rows left at its top
+            if (tid == 0) prog = 0;
             __syncthreads();
             if (warp == 0) {
-                const int n = dg_factor32<FACT>(Tb, nb, fp.criterion, Ls);
+                const int n = dg_factor32<FACT>(Tb, nb, fp.criterion, &Sx[0][0], &prog);
                 if (lane == 0 && n) npiv += n;
+            } else if (warp == 1) {
+                dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 0, &prog, Zs[0], gZ + (size_t)p * 1024, fp.status);
+            } else if (FACT == FACT_GETRF && warp == 2) {
+                dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 1, &prog, Zs[1], gZ + (size_t)(np + p) * 1024, fp.status);
             }
             __syncthreads();
-            if (warp == 0) dg_inverse<T, FACT>(Tb, nb, 0, Zs[0], gZ + (size_t)p * 1024);
-            if (FACT == FACT_GETRF && warp == 1) dg_inverse<T, FACT>(Tb, nb, 1, Zs[1], gZ + (size_t)(np + p) * 1024);
             for (int e = tid; e < nb * DG_LD; e += blockDim.x) Wt[e] = Tb[e];
             __syncthreads();
             const int r0 = 32 * p + 32;  // rows below the top block
@@ -1653,7 +1825,6 @@ constexpr int TC_GROUP = 128 * TC_CH;               // bytes of 8 rows x TC_BK c
 constexpr int TC_PIECE = (TC_BM / 8) * TC_GROUP;    // one term of a 128-row operand block
 constexpr int TC_STAGE = 6 * TC_PIECE;              // A0 A1 A2 B0 B1 B2
 constexpr int TC_SPIN = 1 << 20;                    // try_wait rounds before giving up
-constexpr int PGPU_STATUS_TIMEOUT = 3;
 
 __host__ __device__ inline int split_nkb(int nc) { return (nc + TC_BK - 1) / TC_BK; }
 __host__ __device__ inline int split_ng(int st) { return (st + 7) / 8 + 16; }

@@ -1089,10 +1089,9 @@ __device__ __forceinline__ double dg_t(const double *W, int a, int b, int side) 
 // reciprocal square root: d = a rsqrt(a), 1 / d = rsqrt(a).
 template <int FACT>
 __device__ __forceinline__ void dg_pivot(double a, double crit, int &np, double &d, double &inv) {
-    if (fabs(a) < crit) {
-        a = (FACT == FACT_POTRF || a >= 0.0) ? crit : -crit;
-        np++;
-    }
+    const bool rep = fabs(a) < crit;  // selects rather than a branch: this sits on the step's critical path
+    np += rep ? 1 : 0;
+    a = rep ? ((FACT == FACT_POTRF || a >= 0.0) ? crit : -crit) : a;
     if (FACT == FACT_POTRF) {
         const double rs = rsqrt(a);
         d = a * rs;
@@ -1189,7 +1188,9 @@ __device__ __forceinline__ int dg_factor32_impl(double *W, int nbr, double crit,
 // (Pub as above; Blk + 64 keeps row r's 8 values contiguous for the update)
 // and updates the rest of its row; the row then moves 8 places left, so the
 // loop over the blocks runs rolled with static register indices.  `Blk`: 320
-// doubles, 16-byte aligned.
+// doubles, 16-byte aligned.  Block b is announced by an arrival at named
+// barrier 1 + b (64 threads: this warp and the inverse warp, which waits there)
+// instead of through *prog.
 template <int FACT>
 __device__ __noinline__ int dg_factor32_sym(double *W, int nb, double crit, double *Pub, volatile int *prog,
                                             double *Blk) {
@@ -1220,12 +1221,9 @@ __device__ __noinline__ int dg_factor32_sym(double *W, int nb, double crit, doub
         double dd[8], iv[8];
 #pragma unroll
         for (int c = 0; c < 8; c++) {
-            if (jb + c < nb) {
-                dg_pivot<FACT>(a[c][c], crit, np, dd[c], iv[c]);
-            } else {  // padding beyond nb: identity
-                dd[c] = 1.0;
-                iv[c] = 1.0;
-            }
+            int npc = 0;
+            dg_pivot<FACT>((jb + c < nb) ? a[c][c] : 1.0, crit, npc, dd[c], iv[c]);  // identity beyond nb
+            np += (jb + c < nb) ? npc : 0;
             double uc[8], lc[8];
 #pragma unroll
             for (int i = c + 1; i < 8; i++) {
@@ -1243,47 +1241,45 @@ __device__ __noinline__ int dg_factor32_sym(double *W, int nb, double crit, doub
         double x[8];
 #pragma unroll
         for (int c = 0; c < 8; c++) {
-            double s0 = r[c], s1 = 0.0;
+            // every term but the last is ready before x[c - 1]: one FMA and one product per column
+            double sc = r[c];
 #pragma unroll
-            for (int k = 0; k < c; k++) {
-                const double m = (FACT == FACT_SYTRF) ? a[c][k] * dd[k] : a[c][k];
-                if (k & 1) s1 -= x[k] * m;
-                else s0 -= x[k] * m;
-            }
-            const double xc = (s0 + s1) * iv[c];
+            for (int k = 0; k < c; k++) sc -= x[k] * ((FACT == FACT_SYTRF) ? a[c][k] * dd[k] : a[c][k]);
+            const double xc = sc * iv[c];
             x[c] = (lane > jb + c) ? xc : ((lane == jb + c) ? dd[c] : r[c]);
         }
         double pv[8];  // published: POTRF L(i, c); SYTRF D(c) L(i, c); the pivot on the diagonal
 #pragma unroll
         for (int c = 0; c < 8; c++) pv[c] = (FACT == FACT_SYTRF && lane != jb + c) ? x[c] * dd[c] : x[c];
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
-            if (jb + c < nb) {
-                if (lane < nb) W[lane * DG_LD + jb + c] = x[c];
-                Pub[(jb + c) * DG_BLD + lane] = pv[c];
-                if (lane == c) Pub[(jb + c) * DG_BLD + 32] = iv[c];
-            }
+        for (int c = 0; c < 8; c++) {  // rows jb + c <= 31 of Pub exist even beyond nb (never read there)
+            if (lane < nb && jb + c < nb) W[lane * DG_LD + jb + c] = x[c];
+            Pub[(jb + c) * DG_BLD + lane] = pv[c];
+            if (lane == c) Pub[(jb + c) * DG_BLD + 32] = iv[c];
         }
 #pragma unroll
         for (int c = 0; c < 8; c += 2) *reinterpret_cast<double2 *>(Xr + lane * 8 + c) = make_double2(pv[c], pv[c + 1]);
         __syncwarp();
-        if (lane == 0) {
-            __threadfence_block();
-            *prog = min(jb + 8, nb);
-        }
-        // rank-8 update of the rest of the row (lower part: columns jb + j <= lane)
+        // block published: release the inverse warp(s) waiting at named barrier 1 + jb / 8
+        asm volatile("bar.arrive %0, 64;" ::"r"(1 + jb / 8) : "memory");
+        // rank-8 update of the rest of the row (lower part: columns jb + j <= lane), by
+        // groups of 8 columns that exist; no branch inside a group, so its columns overlap
 #pragma unroll
-        for (int j = 8; j < 32; j++) {
-            if (lane >= jb + j) {
-                const double *xr = Xr + (jb + j) * 8;
-                double s0 = 0.0, s1 = 0.0;
+        for (int g = 8; g < 32; g += 8) {
+            if (jb + g < 32) {
 #pragma unroll
-                for (int c = 0; c < 8; c += 2) {
-                    const double2 t = *reinterpret_cast<const double2 *>(xr + c);
-                    s0 += x[c] * t.x;
-                    s1 += x[c + 1] * t.y;
+                for (int j = g; j < g + 8; j++) {
+                    const double *xr = Xr + (jb + j) * 8;
+                    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                    for (int c = 0; c < 8; c += 2) {
+                        const double2 t = *reinterpret_cast<const double2 *>(xr + c);
+                        s0 += x[c] * t.x;
+                        s1 += x[c + 1] * t.y;
+                    }
+                    const double nv = r[j] - (s0 + s1);
+                    r[j] = (lane >= jb + j) ? nv : r[j];
                 }
-                r[j] -= s0 + s1;
             }
         }
 #pragma unroll
@@ -1308,8 +1304,9 @@ __device__ __forceinline__ int dg_factor32(double *W, int nb, double crit, doubl
 // (POTRF L, SYTRF L D, GETRF U^T, or L for side 1), Z = (M^{-1})^T: lane j
 // forms column j of M^{-1} by forward substitution, row i as soon as the
 // factorization has published step i (M(i, k) = Pub[k][i], side 1 Pub[i][k]),
-// so the inverse ends one step after the factorization.  A wait that runs
-// past its bound records PGPU_STATUS_TIMEOUT in `status` and stops waiting.
+// so the inverse ends one step after the factorization.  POTRF / SYTRF wait at
+// the named barrier of each 8-row block; GETRF polls *prog, and a wait that
+// runs past its bound records PGPU_STATUS_TIMEOUT in `status` and stops waiting.
 template <typename T, int FACT>
 __device__ __forceinline__ void dg_inverse_pipe(const double *Pub, int nb, int side, const volatile int *prog,
                                                 double *Z, T *gZ, int *status) {
@@ -1320,9 +1317,13 @@ __device__ __forceinline__ void dg_inverse_pipe(const double *Pub, int nb, int s
 #pragma unroll
     for (int i = 0; i < 32; i++) {
         if (i < nb) {
-            for (int spins = 0; ok && *prog <= i;)
-                if (++spins > DG_SPIN) ok = false;
-            __threadfence_block();
+            if (FACT != FACT_GETRF) {  // POTRF / SYTRF: block i / 8 announced at a named barrier
+                if ((i & 7) == 0) asm volatile("bar.sync %0, 64;" ::"r"(1 + i / 8) : "memory");
+            } else {
+                for (int spins = 0; ok && *prog <= i;)
+                    if (++spins > DG_SPIN) ok = false;
+                __threadfence_block();
+            }
             const double rinv = lower_l ? 1.0 : Pub[i * DG_BLD + 32];
             double a0 = (i == lane) ? 1.0 : 0.0, a1 = 0.0;
 #pragma unroll

@@ -276,6 +276,92 @@ def run_cpu_baseline(args, sample_small: bool):
                 berr=backward_error(Af, x, b), iters=it)
 
 
+def run_adjoint(reps: int = 20, ndir: int = 20) -> dict:
+    """Adjoint of the solve on the variable-coefficient 2D diffusion (512x512,
+    k = exp(GRF), seed 2): loss 0.5||x - x_obs||^2 with x_obs the solution for an
+    independent field (seed 12) plus 1% Gaussian noise.  Times one forward solve
+    against one backward pass (transposed solve + sampled outer product over the
+    pattern) with CUDA events, and checks the gradient against central finite
+    differences along `ndir` random directions of (values, b)."""
+    import torch
+    from pastix_b200 import gen
+    from pastix_b200 import pastix as px
+    from pastix_b200.autograd import SparseSolver, solve
+
+    A, grid, fact = gen.workload("grf512")
+    s = grid[0]
+    solver = SparseSolver(A, fact, grid=grid)
+    n = A.shape[0]
+    rng = np.random.default_rng(2)
+    vals = torch.tensor(solver.spm.values, device="cuda")
+    b = torch.tensor(rng.standard_normal(n), device="cuda")
+    # observations: the solution for an independent field, plus 1% noise
+    A_obs = gen.diffusion5_grf(s, s, np.exp(gen.grf_2d(s, s, 16.0, 1.0, 12)))
+    obs = SparseSolver(A_obs, fact, grid=grid)
+    obs.factorize(torch.tensor(obs.spm.values, device="cuda"))
+    x_obs = obs.solve(b)
+    x_obs = x_obs + 0.01 * x_obs.abs().mean() * torch.tensor(rng.standard_normal(n), device="cuda")
+    px.finalize(obs.pd)
+
+    solver.factorize(vals)
+    x = solver.solve(b)
+    g = x - x_obs
+    st = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    t_fwd = timed(lambda: solver.solve(b))
+    t_bwd = timed(lambda: solver.sampled_outer(solver.solve(g, transposed=True), x))
+
+    def fwd_total():
+        solver.factorize(vals)
+        solver.solve(b)
+    t_fact_solve = timed(fwd_total)
+
+    # gradient through torch.autograd, then central differences
+    v = vals.clone().requires_grad_(True)
+    bb = b.clone().requires_grad_(True)
+    xs = solve(v, bb, solver)
+    loss = 0.5 * ((xs - x_obs) ** 2).sum()
+    loss.backward()
+    gv, gb = v.grad, bb.grad
+    drng = np.random.default_rng(20)
+
+    def central(h, dv, db):
+        # (f(+h) - f(-h)) / 2h with the loss difference written as a product, so
+        # that the large loss does not cancel: 0.5 (x+ - x-) . (x+ + x- - 2 x_obs)
+        with torch.no_grad():
+            xp = solve(vals + h * dv, b + h * db, solver)
+            xm = solve(vals - h * dv, b - h * db, solver)
+            return (0.5 * ((xp - xm) * (xp + xm - 2 * x_obs)).sum()).item() / (2 * h)
+
+    worst = 0.0
+    for _ in range(ndir):
+        dv = torch.tensor(drng.standard_normal(vals.numel()), device="cuda") * vals.abs()
+        db = torch.tensor(drng.standard_normal(n), device="cuda")
+        # Richardson extrapolation of the central difference (h, h/2) cancels the
+        # h^2 term, which dominates at this contrast of k = exp(GRF)
+        h = 1e-6
+        fd = (4.0 * central(h / 2, dv, db) - central(h, dv, db)) / 3.0
+        an = (gv * dv).sum().item() + (gb * db).sum().item()
+        worst = max(worst, abs(fd - an) / max(abs(an), 1e-300))
+    px.finalize(solver.pd)
+    return {"workload": "grf512: 2D 5-point diffusion 512x512 (n=262144), k=exp(GRF l=16 var=1 seed 2), LL^T",
+            "forward_solve_ms": t_fwd, "adjoint_ms": t_bwd, "adjoint_over_solve": t_bwd / t_fwd,
+            "factor_plus_solve_ms": t_fact_solve, "fd_directions": ndir, "fd_max_rel_err": worst,
+            "fd_rule": "central differences h=1e-6 and 5e-7, Richardson-extrapolated"}
+
+
 def run_probe(s: int, mixed: bool = False) -> int:
     import torch
     from pastix_b200 import gen
@@ -414,6 +500,8 @@ def main():
         "e2e": {"value": mixed["e2e"], "unit": "s", "h2d_bytes_per_step": mixed["h2d"],
                 "d2h_bytes_per_step": mixed["d2h"], "berr": mixed["e2e_berr"]},
     }
+    if rank == 0 and ws == 1:
+        line["adjoint"] = run_adjoint()
     if rank == 0 and not args.no_cpu_baseline and ws == 1:
         cb = run_cpu_baseline(args, sample_small=args.cpu_sample_grid < 100)
         scale = WORKLOADS[args.workload][0][0] ** 3 / n

@@ -327,6 +327,20 @@ int pgpu_solve_device_static(pastix_data_t *pastix_data, pastix_int_t nrhs, doub
  * big update tiles, BF16 split of FP32 panels),
  * the summed device milliseconds and the launch counts. */
 int pgpu_profile(pastix_data_t *pastix_data, int enable);
+
+/* CUDA graphs of the fixed launch sequences (no counterpart in the reference,
+ * whose numerical phase is scheduled by threads, sopalin/pastix_task_sopalin.c:51-58).
+ * With graphs on (the default) the FP64 factorization's per-level launches
+ * (pastix_subtask_sopalin) and the two sweeps of each solve (both precisions)
+ * are captured into one CUDA graph on first use and replayed by a single
+ * cudaGraphLaunch afterwards (FP32 factorizations launch kernel by kernel:
+ * measured faster than their graph); a graph is keyed by the precision, the factorization kind and
+ * every device buffer its launches name, and is dropped when the analysis
+ * changes.  The static-pivot threshold is read from device memory, so a
+ * replay with new matrix values is exact.  pgpu_graphs(pd, 0) drops the
+ * graphs and launches kernel by kernel; per-launch profiling (pgpu_profile
+ * with enable = 1) also launches kernel by kernel. */
+int pgpu_graphs(pastix_data_t *pastix_data, int enable);
 int pgpu_profile_get(pastix_data_t *pastix_data, double *ms, long long *launches, int nclass);
 
 #ifdef __cplusplus

@@ -76,7 +76,8 @@ struct DevStruct {
 
 // Per-call scalars for the factorization kernels.
 struct FactParams {
-    double criterion;           // static pivoting threshold (eps * ||A||_F)
+    const double *criterion;    // static pivoting threshold (eps * ||A||_F), in device memory so that
+                                // a captured launch sequence stays valid when the values change
     int *nbpivots;              // device counter
     int *status;                // device status word (0 = fine)
 };

@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(256) k_panel_small(DevStruct s, const int *__r
     for (int c = 0; c < nc; c++) {
         if (tid == 0) {
             int np = npiv;
-            P[c + c * st] = static_pivot<T, FACT>(P[c + c * st], fp.criterion, np);
+            P[c + c * st] = static_pivot<T, FACT>(P[c + c * st], __ldg(fp.criterion), np);
             npiv = np;
         }
         __syncthreads();
@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__re
 #pragma unroll
             for (int c = 0; c < 32; c++) {
                 if (c < nb) {
-                    const T d = static_pivot<T, FACT>(__shfl_sync(0xffffffffu, r[c], c), fp.criterion, np);
+                    const T d = static_pivot<T, FACT>(__shfl_sync(0xffffffffu, r[c], c), __ldg(fp.criterion), np);
                     const T inv = T(1) / d;
                     const T u = r[c];
                     if (lane == c) r[c] = d;
@@ -1458,7 +1458,7 @@ __global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__
         // 2. factor the top block (warp 0), one row per lane in registers; its inverse(s)
         //    one step behind (warps 1 and 2)
         if (warp == 0) {
-            const int np = dg_factor32<FACT>(W, nb, fp.criterion, &Sx[0][0], &prog);
+            const int np = dg_factor32<FACT>(W, nb, __ldg(fp.criterion), &Sx[0][0], &prog);
             if (lane == 0 && np) npiv += np;
         } else if (warp == 1) {
             dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 0, &prog, Z0, gZ + (size_t)(jb / 32) * 1024, fp.status);
@@ -1676,7 +1676,7 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
             if (tid == 0) prog = 0;
             __syncthreads();
             if (warp == 0) {
-                const int n = dg_factor32<FACT>(Tb, nb, fp.criterion, &Sx[0][0], &prog);
+                const int n = dg_factor32<FACT>(Tb, nb, __ldg(fp.criterion), &Sx[0][0], &prog);
                 if (lane == 0 && n) npiv += n;
             } else if (warp == 1) {
                 dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 0, &prog, Zs[0], gZ + (size_t)p * 1024, fp.status);

@@ -334,6 +334,11 @@ def spmv_device(pd: Data, alpha: float, x, beta: float, y) -> None:
                                                             C.c_void_p(_torch_stream().cuda_stream)))
 
 
+def graphs(pd: Data, enable: bool) -> None:
+    """Replay the factorization and solve launch sequences as CUDA graphs (default on)."""
+    _check("pgpu_graphs", _lib.load().pgpu_graphs(pd.ptr, int(enable)))
+
+
 def profile(pd: Data, enable: bool) -> None:
     _check("pgpu_profile", _lib.load().pgpu_profile(pd.ptr, int(enable)))
 

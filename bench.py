@@ -143,6 +143,56 @@ def solve_bytes(info) -> float:
     return 2.0 * 8.0 * float(info["coefnbr"])
 
 
+def time_solves(pd, n, info, mode, S) -> dict:
+    """Device time of one solve (1 and 16 right-hand sides, pgpu_solve_device)
+    and of one residual SpMV (pgpu_spmv_device) with the resident factors, and
+    their algorithmic HBM bytes: per sweep the factor panels once
+    (sizeof(T) * coefnbr) plus the right-hand sides read and written; the SpMV
+    reads the permuted CSR (8-byte values, 4-byte column indices, 4-byte row
+    pointers), x, and reads and writes y."""
+    import torch
+    from pastix_b200 import pastix as px
+    fs = 4 if mode == "mixed" else 8
+    out = {}
+    g = torch.Generator(device="cuda").manual_seed(9)
+    for nrhs in (1, 16):
+        B0 = torch.rand(n, nrhs, dtype=torch.float64, device="cuda", generator=g).t().contiguous().t()
+        B = B0.clone()
+        ts = []
+        for rep in range(8):
+            B.copy_(B0)  # in-place solves: start every repetition from the same right-hand sides
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            px.solve_device(pd, B if nrhs > 1 else B[:, 0])
+            e1.record()
+            torch.cuda.synchronize()
+            if rep >= 2:
+                ts.append(e0.elapsed_time(e1))
+        ms = float(np.median(ts))
+        # two sweeps; the FP32 path also casts the FP64 right-hand sides in and out
+        byts = 2.0 * (fs * info["coefnbr"] + 2.0 * n * nrhs * fs) + 2.0 * n * nrhs * 8 * 2
+        out[f"nrhs{nrhs}_ms"] = ms
+        out[f"nrhs{nrhs}_gbs"] = byts / (ms / 1e3) / 1e9
+    if mode == "fp64":
+        x = torch.rand(n, dtype=torch.float64, device="cuda", generator=g)
+        y = torch.zeros_like(x)
+        nnz = int(S.full().nnz)
+        for _ in range(3):
+            px.spmv_device(pd, 1.0, x, 0.0, y)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            px.spmv_device(pd, 1.0, x, 0.0, y)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 20
+        byts = nnz * (8 + 4) + 4 * (n + 1) + 24 * n
+        out["spmv_ms"] = ms
+        out["spmv_gbs"] = byts / (ms / 1e3) / 1e9
+    return out
+
+
 def run_b200(args, ws, rank, local):
     import torch
     from pastix_b200 import gen
@@ -215,6 +265,7 @@ def run_b200(args, ws, rank, local):
         px.profile(pd, False)
         results[mode]["profile"] = prof
         results[mode]["info"] = {k: info[k] for k in ("cb_lcol", "cb_fcol", "cb_stride", "coefnbr")}
+        results[mode]["solve"] = time_solves(pd, n, info, mode, S)
         if mode == "mixed":
             # e2e through the C ABI with host buffers
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -500,6 +551,15 @@ def main():
         "e2e": {"value": mixed["e2e"], "unit": "s", "h2d_bytes_per_step": mixed["h2d"],
                 "d2h_bytes_per_step": mixed["d2h"], "berr": mixed["e2e_berr"]},
     }
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    hbm_src = "measured copy (MEASURED_PEAKS.json)" if peaks.get("hbm_gbs") else "fallback 6650 GB/s"
+    line["solve"] = {"fp32_factor": mixed["solve"], "fp64_factor": {k: v for k, v in fp64["solve"].items()
+                                                                   if not k.startswith("spmv")},
+                     "peak_gbs": hbm, "peak_source": hbm_src,
+                     "frac_nrhs1_fp32": mixed["solve"]["nrhs1_gbs"] / hbm,
+                     "frac_nrhs16_fp64": fp64["solve"]["nrhs16_gbs"] / hbm}
+    line["spmv"] = {"ms": fp64["solve"]["spmv_ms"], "gbs": fp64["solve"]["spmv_gbs"], "peak_gbs": hbm,
+                    "frac": fp64["solve"]["spmv_gbs"] / hbm}
     if rank == 0 and ws == 1:
         line["adjoint"] = run_adjoint()
     if rank == 0 and not args.no_cpu_baseline and ws == 1:

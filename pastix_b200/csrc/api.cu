@@ -72,10 +72,10 @@ template <typename T>
 void launch_bwd_update(const DevStruct &, const RowTile *, int, int, const T *, T *, int, int, cudaStream_t);
 template <typename T>
 void launch_fwd_diag_inv(const DevStruct &, const int *, int, int, const T *, const T *, int, int, const T *, T *,
-                         int, int, const float *, const int64_t *, cudaStream_t);
+                         int, int, const float *, const int64_t *, int, cudaStream_t);
 template <typename T>
 void launch_bwd_diag_inv(const DevStruct &, const int *, int, int, const T *, const T *, int, int, const T *, T *,
-                         int, int, const float *, const int64_t *, cudaStream_t);
+                         int, int, const float *, const int64_t *, int, cudaStream_t);
 template <typename T>
 void launch_bwd_diag(const DevStruct &, const int *, int, int, const T *, int, T *, int, int, cudaStream_t);
 template <typename T>
@@ -167,6 +167,7 @@ struct LevelLists {
     int diag_maxnc;         // widest cblk of the large list
     size_t small_smem_elems, diag_smem_elems, trsm_smem_elems;
     int small_maxst;        // tallest narrow cblk (tables of the fused updates)
+    int ntinv;              // wide cblks with a kept full triangular inverse (FP32 factors)
 };
 
 struct Device {
@@ -879,6 +880,8 @@ static int build_maps_and_lists(pastix_data_t *pd) {
                     pd->dense_slabs.push_back(pgpu::DenseSlab{src, img, (int)nc, (int)nc, (int)nc, (int)r});
             }
         }
+        L.ntinv = 0;
+        for (int i = L.large0; i < (int)pd->large_list.size(); i++) L.ntinv += pd->ti_off[pd->large_list[i]] >= 0;
         L.tt1 = (int)pd->trsm_tc_tiles.size();
         L.ds1 = (int)pd->dense_slabs.size();
         L.tr32_1 = (int)pd->trsm_tiles32.size();
@@ -1465,7 +1468,8 @@ static void sweep_forward(pastix_data_t *pd, const T *P, int unit, int zside, in
         });
         launch_cls(pd, PC_FWD_DIAG, lv.large1 - lv.large0, [&] {
             pgpu::launch_fwd_diag_inv<T>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0, lv.maxnc, P, Dinv,
-                                         zside, scaled, Ld, Y, ldy, nrhs, tinv_of<T>(d), d.ti_off.p, d.stream);
+                                         zside, scaled, Ld, Y, ldy, nrhs, tinv_of<T>(d), d.ti_off.p, lv.ntinv,
+                                         d.stream);
         });
         launch_cls(pd, PC_FWD_UPDATE, lv.st1 - lv.st0, [&] {
             pgpu::launch_fwd_update<T>(d.ds, d.solve_tiles.p + lv.st0, lv.st1 - lv.st0, lv.maxnc, P, Y, ldy, nrhs,
@@ -1491,7 +1495,8 @@ static void sweep_backward(pastix_data_t *pd, const T *P, int unit, int zside, i
         });
         launch_cls(pd, PC_BWD_DIAG, lv.large1 - lv.large0, [&] {
             pgpu::launch_bwd_diag_inv<T>(d.ds, d.large_list.p + lv.large0, lv.large1 - lv.large0, lv.maxnc, P, Dinv,
-                                         zside, scaled, Ld, Y, ldy, nrhs, tinv_of<T>(d), d.ti_off.p, d.stream);
+                                         zside, scaled, Ld, Y, ldy, nrhs, tinv_of<T>(d), d.ti_off.p, lv.ntinv,
+                                         d.stream);
         });
     }
 }

@@ -19,6 +19,8 @@
 // substitution by one warp per right-hand side.
 #include "device.cuh"
 
+#include <cooperative_groups.h>
+
 namespace pgpu {
 
 constexpr int ST_R = 64, ST_C = 64;  // solve update tile: panel rows x panel columns
@@ -147,75 +149,121 @@ __global__ void __launch_bounds__(256) k_bwd_diag(DevStruct s, const int *__rest
 // ---------------------------------------------------------------------------
 // Diagonal steps with the full inverse of the block's triangular factor, kept
 // (transposed, FP32) by the FP32 factorization for its TRSM: Pt = T^{-T},
-// column major nc x nc.  Forward: y <- S Pt y; backward: x <- Pt^T S x (S = D
-// for LDL^T, else I) -- the blocked steps below, as one dense product each, so
-// a cblk's diagonal step is a single parallel pass instead of a chain of
-// 32-column blocks.  One right-hand side; y in shared memory; result to out.
-// Forward: the 8 warps split the columns of Pt, lanes take rows (coalesced),
-// 48 loads in flight per thread; partial sums meet in shared memory.
-template <typename T>
-__device__ __forceinline__ void tinv_fwd_gemv(const float *Pt, int nc, const T *Dl, int st, const T *y, T *out) {
-    __shared__ float part[8][384];
+// column major nc x nc, lower triangular.  Forward: y <- S Pt y; backward:
+// x <- Pt^T S x (S = D for LDL^T, else I) -- the blocked steps of
+// solve_cblk_ztrsmsp_forward / _backward as one dense product.  One right-hand
+// side.  A cluster of TC CTAs shares one cblk: every CTA copies y_k to its
+// shared memory, the cluster barrier then guarantees that all copies are made
+// before any CTA overwrites y_k in place, and 32-row (forward) or 32-column
+// (backward) blocks of Pt go round robin to the CTAs, so each reads about
+// 1/TC of the inverse instead of one CTA reading all of it while the level's
+// other SMs wait.
+constexpr int TC = 8;
+
+template <typename T, int RC>
+__global__ void __cluster_dims__(TC, 1, 1) __launch_bounds__(256)
+    k_fwd_diag_tinv(DevStruct s, const int *__restrict__ list, int zside, int scaled, const T *Ldiag, T *Y, int ldy,
+                    int nrhs, const float *__restrict__ tinv, const int64_t *__restrict__ ti_off) {
+    __shared__ float ys[RC][384];
+    __shared__ float part[8][RC][33];
+    const int k = list[blockIdx.x / TC];
+    const int64_t off = ti_off[k];
+    if (off < 0) return;  // the whole cluster leaves: k_fwd_diag_inv takes this cblk
+    cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int fc = s.cb_fcol[k];
+    const int nc = s.cb_lcol[k] - fc + 1;
+    const int st = s.cb_stride[k];
+    const int j0 = blockIdx.y * RC, nr = min(RC, nrhs - j0);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int kper = (nc + 7) / 8, k0 = warp * kper, k1 = min(nc, k0 + kper);
-    float acc[12];
+    for (int e = tid; e < nc * RC; e += blockDim.x) {
+        const int i = e % nc, j = e / nc;
+        ys[j][i] = j < nr ? (float)Y[fc + i + (size_t)(j0 + j) * ldy] : 0.f;
+    }
+    cluster.sync();
+    const float *Pt = tinv + off + (size_t)zside * nc * nc;
+    for (int cb = rank * 32; cb < nc; cb += TC * 32) {
+        const int c = cb + lane;
+        const int kend = min(nc, cb + 32);  // Pt is lower triangular: columns past the block are zero
+        float acc[RC];
 #pragma unroll
-    for (int i = 0; i < 12; i++) acc[i] = 0.f;
-    for (int kk = k0; kk < k1; kk += 4) {
-        float p[4][12];
+        for (int j = 0; j < RC; j++) acc[j] = 0.f;
+        if (c < nc) {
+#pragma unroll 8
+            for (int kk = warp; kk < kend; kk += 8) {
+                const float pv = Pt[c + (size_t)kk * nc];
+#pragma unroll
+                for (int j = 0; j < RC; j++) acc[j] += pv * ys[j][kk];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < RC; j++) part[warp][j][lane] = acc[j];
+        __syncthreads();
+        for (int o = tid; o < 32 * RC; o += blockDim.x) {
+            const int l = o & 31, j = o >> 5, cc = cb + l;
+            if (cc < nc && j < nr) {
+                float v = 0.f;
+#pragma unroll
+                for (int w = 0; w < 8; w++) v += part[w][j][l];
+                if (scaled) v *= (float)Ldiag[s.cb_coef[k] + cc + (size_t)cc * st];
+                Y[fc + cc + (size_t)(j0 + j) * ldy] = (T)v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int RC>
+__global__ void __cluster_dims__(TC, 1, 1) __launch_bounds__(256)
+    k_bwd_diag_tinv(DevStruct s, const int *__restrict__ list, int zside, int scaled, const T *Ldiag, T *Y, int ldy,
+                    int nrhs, const float *__restrict__ tinv, const int64_t *__restrict__ ti_off) {
+    __shared__ float xs[RC][384];
+    const int k = list[blockIdx.x / TC];
+    const int64_t off = ti_off[k];
+    if (off < 0) return;  // the whole cluster leaves: k_bwd_diag_inv takes this cblk
+    cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int fc = s.cb_fcol[k];
+    const int nc = s.cb_lcol[k] - fc + 1;
+    const int st = s.cb_stride[k];
+    const int j0 = blockIdx.y * RC, nr = min(RC, nrhs - j0);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < nc * RC; e += blockDim.x) {
+        const int i = e % nc, j = e / nc;
+        float v = j < nr ? (float)Y[fc + i + (size_t)(j0 + j) * ldy] : 0.f;
+        if (scaled) v *= (float)Ldiag[s.cb_coef[k] + i + (size_t)i * st];
+        xs[j][i] = v;
+    }
+    cluster.sync();
+    const float *Pt = tinv + off + (size_t)zside * nc * nc;
+    // x_c = sum_{r >= c} Pt[r, c] xs[r]: four columns per warp, lanes over the rows (coalesced)
+    for (int cb = rank * 32; cb < nc; cb += TC * 32) {
+        const int c0 = cb + 4 * warp;
+        float acc[4][RC];
 #pragma unroll
         for (int u = 0; u < 4; u++)
 #pragma unroll
-            for (int i = 0; i < 12; i++) {
-                const int c = lane + 32 * i;
-                p[u][i] = (c < nc && kk + u < k1) ? Pt[c + (size_t)(kk + u) * nc] : 0.f;
+            for (int j = 0; j < RC; j++) acc[u][j] = 0.f;
+        for (int r = c0 + lane; r < nc; r += 32) {
+            float pv[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) pv[u] = (c0 + u < nc && r >= c0 + u) ? Pt[r + (size_t)(c0 + u) * nc] : 0.f;
+#pragma unroll
+            for (int j = 0; j < RC; j++) {
+                const float xr = xs[j][r];
+#pragma unroll
+                for (int u = 0; u < 4; u++) acc[u][j] += pv[u] * xr;
             }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const float yk = (kk + u < k1) ? (float)y[kk + u] : 0.f;
-#pragma unroll
-            for (int i = 0; i < 12; i++) acc[i] += p[u][i] * yk;
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < 12; i++)
-        if (lane + 32 * i < nc) part[warp][lane + 32 * i] = acc[i];
-    __syncthreads();
-    for (int c = tid; c < nc; c += blockDim.x) {
-        float v = 0.f;
-#pragma unroll
-        for (int w = 0; w < 8; w++) v += part[w][c];
-        if (Dl) v *= (float)Dl[c + (size_t)c * st];
-        out[c] = (T)v;
-    }
-}
-// Backward: 4 outputs per warp at a time, lanes over the rows of Pt's columns
-// (coalesced), shuffle reductions.
-template <typename T>
-__device__ __forceinline__ void tinv_bwd_gemv(const float *Pt, int nc, const T *Dl, int st, const T *y, T *out) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    float xv[12];
-#pragma unroll
-    for (int i = 0; i < 12; i++) {
-        const int c = lane + 32 * i;
-        xv[i] = (c < nc) ? (float)y[c] * (Dl ? (float)Dl[c + (size_t)c * st] : 1.f) : 0.f;
-    }
-    for (int kb = 4 * warp; kb < nc; kb += 32) {
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int i = 0; i < 12; i++) {
-            const int c = lane + 32 * i;
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-                acc[u] += ((c < nc && kb + u < nc) ? Pt[c + (size_t)(kb + u) * nc] : 0.f) * xv[i];
         }
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            float v = acc[u];
+        for (int u = 0; u < 4; u++)
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0 && kb + u < nc) out[kb + u] = (T)v;
-        }
+            for (int j = 0; j < RC; j++) {
+                float v = acc[u][j];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0 && c0 + u < nc && j < nr) Y[fc + c0 + u + (size_t)(j0 + j) * ldy] = (T)v;
+            }
     }
 }
 
@@ -240,15 +288,10 @@ __global__ void __launch_bounds__(256) k_fwd_diag_inv(DevStruct s, const int *__
     const int nzb = (nc + 31) / 32;
     const T *gZ = dinv + s.cb_dinv[k] + (size_t)(zside ? nzb : 0) * 1024;
     const int tid = threadIdx.x, nt = blockDim.x;
+    if (tinv != nullptr && ti_off[k] >= 0) return;  // k_fwd_diag_tinv applies the kept full inverse
     for (int e = tid; e < nc * nr; e += nt) {
         int i = e % nc, j = e / nc;
         y[i + j * nc] = Y[(fc + i) + (size_t)(j0 + j) * ldy];
-    }
-    if (RC == 1 && tinv != nullptr && ti_off[k] >= 0) {  // full inverse kept by the FP32 factorization
-        __syncthreads();
-        tinv_fwd_gemv<T>(tinv + ti_off[k] + (size_t)zside * nc * nc, nc, scaled ? Dl : nullptr, st, y,
-                         Y + fc + (size_t)j0 * ldy);
-        return;
     }
     for (int jb = 0; jb < nc; jb += 32) {
         const int nb = min(32, nc - jb);
@@ -321,16 +364,12 @@ __global__ void __launch_bounds__(256) k_bwd_diag_inv(DevStruct s, const int *__
     const int nzb = (nc + 31) / 32;
     const T *gZ = dinv + s.cb_dinv[k] + (size_t)(zside ? nzb : 0) * 1024;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    if (tinv != nullptr && ti_off[k] >= 0) return;  // k_bwd_diag_tinv applies the kept full inverse
     for (int e = tid; e < nc * nr; e += nt) {
         int i = e % nc, j = e / nc;
         y[i + j * nc] = Y[(fc + i) + (size_t)(j0 + j) * ldy];
     }
     __syncthreads();
-    if (RC == 1 && tinv != nullptr && ti_off[k] >= 0) {
-        tinv_bwd_gemv<T>(tinv + ti_off[k] + (size_t)zside * nc * nc, nc, scaled ? Dl : nullptr, st, y,
-                         Y + fc + (size_t)j0 * ldy);
-        return;
-    }
     for (int b = nzb - 1; b >= 0; b--) {
         const int jb = b * 32;
         const int nb = min(32, nc - jb);
@@ -413,12 +452,14 @@ __global__ void __launch_bounds__(256) k_fwd_update(DevStruct s, const RowTile *
     for (int j = 0; j < RC; j++) acc[j] = T(0);
     if (r < rows) {
         const T *Pr = P + s.cb_coef[k] + tl.r0 + r + (size_t)c0 * st;
-        const int cb = g * 16, ce = min(ncol, cb + 16);
-        for (int c = cb; c < ce; c++) {
-            const T p = Pr[(size_t)c * st];
+        const int cb = g * 16;
+        T p[16];  // all 16 loads issued before the products
 #pragma unroll
-            for (int j = 0; j < RC; j++) acc[j] += p * yk[c + j * ST_C];
-        }
+        for (int u = 0; u < 16; u++) p[u] = (cb + u < ncol) ? Pr[(size_t)(cb + u) * st] : T(0);
+#pragma unroll
+        for (int u = 0; u < 16; u++)
+#pragma unroll
+            for (int j = 0; j < RC; j++) acc[j] += p[u] * yk[cb + u + j * ST_C];
     }
 #pragma unroll
     for (int j = 0; j < RC; j++) part[g][r + j * ST_R] = acc[j];
@@ -449,7 +490,7 @@ __global__ void __launch_bounds__(256) k_bwd_update(DevStruct s, const RowTile *
     const int rows = min(ST_R, st - tl.r0);
     const int j0 = blockIdx.y * RC;
     const int nr = min(RC, nrhs - j0);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const int *ridx = s.rowidx + s.cb_rowidx[k] + tl.r0;
     for (int e = tid; e < ST_R * RC; e += 256) {
         int i = e % ST_R, j = e / ST_R;
@@ -457,24 +498,45 @@ __global__ void __launch_bounds__(256) k_bwd_update(DevStruct s, const RowTile *
     }
     __syncthreads();
     const T *Pk = P + s.cb_coef[k] + tl.r0 + (size_t)c0 * st;
-    for (int c = warp; c < ncol; c += 8) {  // warp per column, lanes over the 64 rows
-        T acc[RC];
+    if constexpr (RC == 1) {
+        // thread (row r, 16-column group g): 16 independent coalesced loads, the
+        // products P[r, c] x[r] staged in shared memory (row stride 65: no bank
+        // conflicts on either side), then one thread per column sums its 64 rows
+        __shared__ T prod[ST_C * (ST_R + 1)];
+        const int r = tid % ST_R, g = tid / ST_R, cb = 16 * g;
+        const T xv = xr[r];
+        T p[16];
 #pragma unroll
-        for (int j = 0; j < RC; j++) acc[j] = T(0);
+        for (int u = 0; u < 16; u++) p[u] = (r < rows && cb + u < ncol) ? Pk[r + (size_t)(cb + u) * st] : T(0);
 #pragma unroll
-        for (int h = 0; h < ST_R; h += 32) {
-            const int i = h + lane;
-            if (i < rows) {
-                const T p = Pk[i + (size_t)c * st];
-#pragma unroll
-                for (int j = 0; j < RC; j++) acc[j] += p * xr[i + j * ST_R];
-            }
+        for (int u = 0; u < 16; u++) prod[(cb + u) * (ST_R + 1) + r] = p[u] * xv;
+        __syncthreads();
+        if (tid < ncol) {
+            T v = T(0);
+#pragma unroll 16
+            for (int i = 0; i < ST_R; i++) v += prod[tid * (ST_R + 1) + i];
+            atomicAdd(&Y[(fc + c0 + tid) + (size_t)j0 * ldy], -v);
         }
+        return;
+    } else {
+        // out[c, j] = sum_r P[r, c] x[r, j]: the tile staged transposed in shared memory
+        // (16 independent coalesced loads per thread), then 64 columns x RC dot products
+        __shared__ T pt[ST_C * (ST_R + 1)];
+        const int r = tid % ST_R, g = tid / ST_R, cb = 16 * g;
+        T p[16];
 #pragma unroll
-        for (int j = 0; j < RC; j++) {
-            T v = acc[j];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0 && j < nr) atomicAdd(&Y[(fc + c0 + c) + (size_t)(j0 + j) * ldy], -v);
+        for (int u = 0; u < 16; u++) p[u] = (r < rows && cb + u < ncol) ? Pk[r + (size_t)(cb + u) * st] : T(0);
+#pragma unroll
+        for (int u = 0; u < 16; u++) pt[(cb + u) * (ST_R + 1) + r] = p[u];
+        __syncthreads();
+        for (int o = tid; o < ST_C * RC; o += 256) {
+            const int c = o % ST_C, j = o / ST_C;
+            if (c < ncol && j < nr) {
+                T v = T(0);
+#pragma unroll 16
+                for (int i = 0; i < ST_R; i++) v += pt[c * (ST_R + 1) + i] * xr[i + j * ST_R];
+                atomicAdd(&Y[(fc + c0 + c) + (size_t)(j0 + j) * ldy], -v);
+            }
         }
     }
 }
@@ -517,23 +579,38 @@ void launch_bwd_diag(const DevStruct &s, const int *list, int count, int maxnc, 
     const int ZDIM = 1;
     PGPU_RC_DISPATCH(nrhs, k_bwd_diag, count, (size_t)maxnc * sizeof(T), s, list, P, unit, Y, ldy, nrhs);
 }
+// ntinv: how many cblks of the list have a kept full inverse (FP32 factors);
+// those go to the 8-CTA cluster kernels, the rest to the blocked kernels, and
+// a kernel with no cblk of its own is not launched.
 template <typename T>
 void launch_fwd_diag_inv(const DevStruct &s, const int *list, int count, int maxnc, const T *P, const T *dinv,
                          int zside, int scaled, const T *Ld, T *Y, int ldy, int nrhs, const float *tinv,
-                         const int64_t *ti_off, cudaStream_t st) {
+                         const int64_t *ti_off, int ntinv, cudaStream_t st) {
     if (count <= 0) return;
+    if (tinv == nullptr) ntinv = 0;
     const int ZDIM = 1;
-    PGPU_RC_DISPATCH(nrhs, k_fwd_diag_inv, count, (size_t)maxnc * sizeof(T), s, list, P, dinv, zside, scaled, Ld,
-                     Y, ldy, nrhs, tinv, ti_off);
+    if (ntinv > 0) {
+        if (nrhs == 1) k_fwd_diag_tinv<T, 1><<<count * TC, 256, 0, st>>>(s, list, zside, scaled, Ld, Y, ldy, nrhs, tinv, ti_off);
+        else k_fwd_diag_tinv<T, 8><<<dim3(count * TC, (nrhs + 7) / 8), 256, 0, st>>>(s, list, zside, scaled, Ld, Y, ldy, nrhs, tinv, ti_off);
+    }
+    if (ntinv < count)
+        PGPU_RC_DISPATCH(nrhs, k_fwd_diag_inv, count, (size_t)maxnc * sizeof(T), s, list, P, dinv, zside, scaled, Ld,
+                         Y, ldy, nrhs, tinv, ti_off);
 }
 template <typename T>
 void launch_bwd_diag_inv(const DevStruct &s, const int *list, int count, int maxnc, const T *P, const T *dinv,
                          int zside, int scaled, const T *Ld, T *Y, int ldy, int nrhs, const float *tinv,
-                         const int64_t *ti_off, cudaStream_t st) {
+                         const int64_t *ti_off, int ntinv, cudaStream_t st) {
     if (count <= 0) return;
+    if (tinv == nullptr) ntinv = 0;
     const int ZDIM = 1;
-    PGPU_RC_DISPATCH(nrhs, k_bwd_diag_inv, count, (size_t)maxnc * sizeof(T), s, list, P, dinv, zside, scaled, Ld,
-                     Y, ldy, nrhs, tinv, ti_off);
+    if (ntinv > 0) {
+        if (nrhs == 1) k_bwd_diag_tinv<T, 1><<<count * TC, 256, 0, st>>>(s, list, zside, scaled, Ld, Y, ldy, nrhs, tinv, ti_off);
+        else k_bwd_diag_tinv<T, 8><<<dim3(count * TC, (nrhs + 7) / 8), 256, 0, st>>>(s, list, zside, scaled, Ld, Y, ldy, nrhs, tinv, ti_off);
+    }
+    if (ntinv < count)
+        PGPU_RC_DISPATCH(nrhs, k_bwd_diag_inv, count, (size_t)maxnc * sizeof(T), s, list, P, dinv, zside, scaled, Ld,
+                         Y, ldy, nrhs, tinv, ti_off);
 }
 template <typename T>
 void launch_fwd_update(const DevStruct &s, const RowTile *tiles, int count, int maxnc, const T *P, T *Y, int ldy,
@@ -562,10 +639,10 @@ int solve_rows_per_tile() { return ST_R; }
     template void launch_bwd_diag<T>(const DevStruct &, const int *, int, int, const T *, int, T *, int, int,     \
                                      cudaStream_t);                                                              \
     template void launch_fwd_diag_inv<T>(const DevStruct &, const int *, int, int, const T *, const T *, int,     \
-                                         int, const T *, T *, int, int, const float *, const int64_t *,          \
+                                         int, const T *, T *, int, int, const float *, const int64_t *, int,     \
                                          cudaStream_t);                                                          \
     template void launch_bwd_diag_inv<T>(const DevStruct &, const int *, int, int, const T *, const T *, int,     \
-                                         int, const T *, T *, int, int, const float *, const int64_t *,          \
+                                         int, const T *, T *, int, int, const float *, const int64_t *, int,     \
                                          cudaStream_t);                                                          \
     template void launch_fwd_update<T>(const DevStruct &, const RowTile *, int, int, const T *, T *, int, int,    \
                                        cudaStream_t);                                                            \

@@ -341,6 +341,26 @@ int pgpu_profile(pastix_data_t *pastix_data, int enable);
  * graphs and launches kernel by kernel; per-launch profiling (pgpu_profile
  * with enable = 1) also launches kernel by kernel. */
 int pgpu_graphs(pastix_data_t *pastix_data, int enable);
+
+/* Bucket boundaries of the supernode update tiles (no counterpart in the
+ * reference, whose update GEMM is one BLAS call per blok,
+ * kernels/core_zgemmsp.c:404-474).  FP64 factors: an update task whose facing
+ * blok has at least dmma_n rows and whose source cblk is at least dmma_k wide
+ * runs as 128 x 64 DMMA tiles, any other as 64 x 64 FMA tiles (defaults 32,
+ * 32).  FP32 factors: a task whose source is at least tc_k (>= 32) wide runs on
+ * tcgen05 with split BF16 operands, narrower ones as FMA tiles (default 32).
+ * Setting them rebuilds the launch lists: the next pastix_task_numfact /
+ * pgpu_numfact_device refactorizes.  pgpu_get_tuning returns the three values. */
+int pgpu_set_tuning(pastix_data_t *pastix_data, pastix_int_t dmma_n, pastix_int_t dmma_k, pastix_int_t tc_k);
+int pgpu_get_tuning(const pastix_data_t *pastix_data, pastix_int_t *vals);
+
+/* Autotuner of those bucket boundaries for the analysed matrix: each candidate
+ * (FP64: dmma_n in {8, 16, 32, 64} x dmma_k in {16, 32}; FP32: tc_k in
+ * {32, 48, 64, 96}) is applied and timed on a factorization of the given
+ * device values (spm value order, as pgpu_numfact_device); the fastest stays
+ * in effect and the matrix is left factorized with it.  chosen (if not NULL)
+ * receives {dmma_n, dmma_k, tc_k}. */
+int pgpu_autotune(pastix_data_t *pastix_data, const double *values_dev, pastix_int_t *chosen);
 int pgpu_profile_get(pastix_data_t *pastix_data, double *ms, long long *launches, int nclass);
 
 #ifdef __cplusplus

@@ -31,7 +31,7 @@ EXPORTS = [
     "pgpu_solver_info", "pgpu_get_coeftab", "pgpu_solve_device", "pgpu_solve_transposed_device",
     "pgpu_numfact_device", "pgpu_sampled_outer", "pgpu_spmv_device", "pgpu_device_status",
     "pgpu_stream", "pgpu_solve_refine_device", "pgpu_profile", "pgpu_profile_get", "pgpu_set_symbol",
-    "pgpu_solve_device_static", "pgpu_graphs",
+    "pgpu_solve_device_static", "pgpu_graphs", "pgpu_set_tuning", "pgpu_get_tuning", "pgpu_autotune",
 ]
 
 # kernel classes of pgpu_profile_get, in order
@@ -125,6 +125,9 @@ def load() -> C.CDLL:
         "pgpu_solve_refine_device": (C.c_int, [P, pastix_int_t, VP, pastix_int_t, VP, pastix_int_t]),
         "pgpu_profile": (C.c_int, [P, C.c_int]),
         "pgpu_graphs": (C.c_int, [P, C.c_int]),
+        "pgpu_set_tuning": (C.c_int, [P, pastix_int_t, pastix_int_t, pastix_int_t]),
+        "pgpu_get_tuning": (C.c_int, [P, PINT]),
+        "pgpu_autotune": (C.c_int, [P, VP, PINT]),
         "pgpu_profile_get": (C.c_int, [P, PDBL, C.POINTER(C.c_longlong), C.c_int]),
         "pgpu_set_symbol": (C.c_int, [P, C.POINTER(spmatrix_t), PINT, pastix_int_t, PINT, PINT, PINT, pastix_int_t,
                                       PINT, PINT, PINT]),

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -118,7 +119,6 @@ enum : int {
 namespace {
 
 constexpr idx_t SMALL_PANEL_ELEMS = 4096;  // st*nc below which a cblk is factored in one CTA's smem
-constexpr idx_t TC_MIN_K = 32;             // FP32 factors: tasks whose source is this wide go to tcgen05
 
 template <typename X>
 struct DBuf {  // owning device buffer
@@ -274,6 +274,11 @@ struct pastix_data_s {
     int mixed = 0;
     double anorm = 0.0;
     double crit_host = 0.0;  // source of the threshold's copy to the device
+    // bucket boundaries of the update tiles (pgpu_set_tuning / pgpu_autotune):
+    // FP64 tasks with blok height >= tune_dmma_n and source width >= tune_dmma_k take
+    // 128 x 64 DMMA tiles, the others 64 x 64 SIMT tiles; FP32 tasks whose source is
+    // at least tune_tc_k wide take tcgen05 tiles (split BF16 terms), the others SIMT
+    int tune_dmma_n = 32, tune_dmma_k = 32, tune_tc_k = 32;
     Device dev;
     // launch accounting: per kernel class, launches always counted, device time when profiling
     bool prof_on = false;
@@ -790,7 +795,7 @@ static int build_maps_and_lists(pastix_data_t *pd) {
     pd->split_slabs.clear();
     for (const auto &tk : sv.tasks) {
         const idx_t K = sv.cb_lcol[tk.src] - sv.cb_fcol[tk.src] + 1;
-        if (K >= TC_MIN_K && K * sv.cb_stride[tk.src] > SMALL_PANEL_ELEMS && pd->sp_off[tk.src] < 0)
+        if (K >= pd->tune_tc_k && K * sv.cb_stride[tk.src] > SMALL_PANEL_ELEMS && pd->sp_off[tk.src] < 0)
             pd->sp_off[tk.src] = 0;
     }
     for (idx_t k = 0; k < sv.cblknbr; k++) {
@@ -899,8 +904,8 @@ static int build_maps_and_lists(pastix_data_t *pd) {
             const auto &tk = sv.tasks[t];
             const idx_t K = sv.cb_lcol[tk.src] - sv.cb_fcol[tk.src] + 1;
             if (K * sv.cb_stride[tk.src] <= SMALL_PANEL_ELEMS) continue;  // done by k_panel_small
-            const bool big = tk.n >= 32 && K >= 32;       // FP64: DMMA tiles
-            const bool tc = K >= TC_MIN_K;                // FP32: tcgen05 tiles
+            const bool big = tk.n >= pd->tune_dmma_n && K >= pd->tune_dmma_k;  // FP64: DMMA tiles
+            const bool tc = K >= pd->tune_tc_k;                                // FP32: tcgen05 tiles
             const idx_t BM = big ? 128 : 64, BN = 64;
             auto &list = big ? pd->upd_big_tiles : pd->upd_tiles;
             for (int side = 0; side < (fk == pgpu::FACT_GETRF ? 2 : 1); side++) {
@@ -2192,6 +2197,80 @@ extern "C" int pgpu_solve_refine_device(pastix_data_t *pd, pastix_int_t nrhs, co
     launch_cls(pd, PC_VEC, 1, [&] { pgpu::launch_permute<double, double>((int)n, (int)nrhs, d.perm.p, 0, xp.p, n, X, ldx, d.stream); });
     CUDA_TRY(cudaStreamSynchronize(d.stream));
     pd->dparm[DPARM_REFINE_TIME] = now_s() - t0;
+    return PASTIX_SUCCESS;
+}
+
+// Rebuild the launch lists after a change of the tile buckets; the device
+// copy and every captured graph are rebuilt on the next numerical step.
+static int retune(pastix_data_t *pd, int dmma_n, int dmma_k, int tc_k) {
+    if (pd->dev.ready) CUDA_TRY(cudaStreamSynchronize(pd->dev.stream));
+    pd->tune_dmma_n = dmma_n;
+    pd->tune_dmma_k = dmma_k;
+    pd->tune_tc_k = tc_k;
+    int rc = build_maps_and_lists(pd);
+    if (rc) return rc;
+    pd->dev.ready = false;
+    pd->steps &= ~(STEP_CSC2BCSC | STEP_BCSC2CTAB | STEP_NUMFACT);
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pgpu_set_tuning(pastix_data_t *pd, pastix_int_t dmma_n, pastix_int_t dmma_k, pastix_int_t tc_k) {
+    if (!pd || !(pd->steps & STEP_ANALYSE)) return PASTIX_ERR_BADPARAMETER;
+    if (dmma_n < 1 || dmma_k < 1 || tc_k < 32) return PASTIX_ERR_BADPARAMETER;  // tcgen05 tiles need K >= 32
+    return retune(pd, (int)dmma_n, (int)dmma_k, (int)tc_k);
+}
+
+extern "C" int pgpu_get_tuning(const pastix_data_t *pd, pastix_int_t *vals) {
+    if (!pd || !vals) return PASTIX_ERR_BADPARAMETER;
+    vals[0] = pd->tune_dmma_n;
+    vals[1] = pd->tune_dmma_k;
+    vals[2] = pd->tune_tc_k;
+    return PASTIX_SUCCESS;
+}
+
+// Autotuner of the update tile buckets: for the factor precision in use, every
+// candidate bucket boundary is applied (launch lists rebuilt), the matrix is
+// factorized from the device values twice and the faster run's device time
+// kept; the fastest candidate stays in effect, with the factorization done.
+extern "C" int pgpu_autotune(pastix_data_t *pd, const double *values_dev, pastix_int_t *chosen) {
+    if (!pd || !values_dev || !(pd->steps & STEP_ANALYSE)) return PASTIX_ERR_BADPARAMETER;
+    if (pd->prof_on) {
+        perr("pgpu_autotune: not available while pgpu_profile timing is enabled");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    pd->mixed = pd->iparm[IPARM_MIXED] ? 1 : 0;
+    std::vector<std::array<int, 3>> cands;
+    if (pd->mixed) {
+        for (int tk : {32, 48, 64, 96}) cands.push_back({pd->tune_dmma_n, pd->tune_dmma_k, tk});
+    } else {
+        for (int n : {8, 16, 32, 64})
+            for (int k : {16, 32}) cands.push_back({n, k, pd->tune_tc_k});
+    }
+    double best = 1e300;
+    std::array<int, 3> arg{pd->tune_dmma_n, pd->tune_dmma_k, pd->tune_tc_k};
+    for (const auto &c : cands) {
+        int rc = retune(pd, c[0], c[1], c[2]);
+        if (rc) return rc;
+        double t = 1e300;
+        for (int rep = 0; rep < 3; rep++) {  // the first run also allocates and captures
+            rc = pgpu_numfact_device(pd, values_dev);
+            if (rc) return rc;
+            if (rep) t = std::min(t, pd->dparm[DPARM_FACT_TIME]);
+        }
+        if (t < best) {
+            best = t;
+            arg = c;
+        }
+    }
+    int rc = retune(pd, arg[0], arg[1], arg[2]);
+    if (rc) return rc;
+    rc = pgpu_numfact_device(pd, values_dev);
+    if (rc) return rc;
+    if (chosen) {
+        chosen[0] = arg[0];
+        chosen[1] = arg[1];
+        chosen[2] = arg[2];
+    }
     return PASTIX_SUCCESS;
 }
 

@@ -334,6 +334,27 @@ def spmv_device(pd: Data, alpha: float, x, beta: float, y) -> None:
                                                             C.c_void_p(_torch_stream().cuda_stream)))
 
 
+def set_tuning(pd: Data, dmma_n: int, dmma_k: int, tc_k: int) -> None:
+    """Bucket boundaries of the update tiles (see pgpu_set_tuning)."""
+    _check("pgpu_set_tuning", _lib.load().pgpu_set_tuning(pd.ptr, dmma_n, dmma_k, tc_k))
+
+
+def get_tuning(pd: Data) -> tuple:
+    v = np.zeros(3, dtype=np.int64)
+    _check("pgpu_get_tuning", _lib.load().pgpu_get_tuning(pd.ptr, v.ctypes.data_as(PINT)))
+    return tuple(int(x) for x in v)
+
+
+def autotune(pd: Data, values) -> tuple:
+    """Time the candidate update-tile buckets on factorizations of `values` (CUDA
+    float64 tensor, spm order); the fastest stays in effect.  Returns
+    (dmma_n, dmma_k, tc_k)."""
+    _torch_stream().synchronize()
+    v = np.zeros(3, dtype=np.int64)
+    _check("pgpu_autotune", _lib.load().pgpu_autotune(pd.ptr, C.c_void_p(values.data_ptr()), v.ctypes.data_as(PINT)))
+    return tuple(int(x) for x in v)
+
+
 def graphs(pd: Data, enable: bool) -> None:
     """Replay the factorization and solve launch sequences as CUDA graphs (default on)."""
     _check("pgpu_graphs", _lib.load().pgpu_graphs(pd.ptr, int(enable)))

@@ -109,3 +109,17 @@ def test_numeric_without_gpu_fails_loudly(lib):
     with pytest.raises(px.PastixError) as e:
         px.task_numfact(pd, S)
     assert e.value.code == px.error.INTERNAL
+
+
+def test_tuning_rejects_bad_values(lib):
+    """pgpu_set_tuning checks its bucket boundaries (host only, no GPU needed)."""
+    from conftest import analyse
+    from pastix_b200 import gen
+    from pastix_b200 import pastix as px
+    pd, S, info = analyse(gen.laplacian7(8, 8, 8), (8, 8, 8), "POTRF")
+    assert px.get_tuning(pd) == (32, 32, 32)
+    assert lib.pgpu_set_tuning(pd.ptr, 0, 32, 32) == px.error.BADPARAMETER
+    assert lib.pgpu_set_tuning(pd.ptr, 32, 32, 16) == px.error.BADPARAMETER
+    assert px.get_tuning(pd) == (32, 32, 32)
+    px.set_tuning(pd, 16, 16, 48)  # rebuilds the launch lists on the host
+    assert px.get_tuning(pd) == (16, 16, 48)

@@ -221,6 +221,10 @@ def run_b200(args, ws, rank, local):
         t0 = time.time()
         px.analyze_grid(pd, S, *grid)
         t_an = time.time() - t0
+        # one-time setup outside the timed region: bucket boundaries of the update tiles
+        t0 = time.time()
+        tuning = px.autotune(pd, vals)
+        t_tune = time.time() - t0
         info = px.solver_info(pd)
         x = torch.zeros_like(b)
         stream = torch.cuda.ExternalStream(px.stream_ptr(pd))
@@ -257,7 +261,9 @@ def run_b200(args, ws, rank, local):
         results[mode] = dict(t=t, berr=berr, fwd=float(np.linalg.norm(xh - xt) / np.linalg.norm(xt)),
                              fact_time=float(dp[px.dparm.fact_time]), iters=int(ip[px.iparm.nbiter]),
                              npiv=int(ip[px.iparm.static_pivoting]), launches=launches / args.steps,
-                             analyze_s=t_an, clocks=clocks, thflops=info["thflops"])
+                             analyze_s=t_an, clocks=clocks, thflops=info["thflops"],
+                             tuning={"dmma_min_rows": tuning[0], "dmma_min_width": tuning[1],
+                                     "tcgen05_min_width": tuning[2], "autotune_s": t_tune})
         # profiled pass (per-class device times) for the roofline of the dominant kernel
         px.profile(pd, True)
         step()
@@ -535,9 +541,10 @@ def main():
         "dtype": "f32+f64" if best == "mixed" else "f64", "data": "synthetic", "config": config,
         "path": best,
         "fp32_refine": {"s": mixed["t"], "berr": mixed["berr"], "fwd_err": mixed["fwd"], "cg_iters": mixed["iters"],
-                        "factor_s": mixed["fact_time"]},
+                        "factor_s": mixed["fact_time"], "tuning": mixed["tuning"]},
         "fp64": {"s": fp64["t"], "berr": fp64["berr"], "fwd_err": fp64["fwd"], "refine_iters": fp64["iters"],
-                 "factor_s": fp64["fact_time"], "factor_tflops": fp64["thflops"] / fp64["fact_time"] / 1e12},
+                 "factor_s": fp64["fact_time"], "factor_tflops": fp64["thflops"] / fp64["fact_time"] / 1e12,
+                 "tuning": fp64["tuning"]},
         "factor_tflops_fp32": mixed["thflops"] / mixed["fact_time"] / 1e12,
         "static_pivots": fp64["npiv"],
         "roofline": roof,

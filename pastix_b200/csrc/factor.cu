@@ -1910,6 +1910,11 @@ __device__ __forceinline__ void split_bf16x3(float a, uint32_t &t0, uint32_t &t1
 
 // Split 128-row slabs of FP32 panels into their BF16 image.  `scale` multiplies
 // column c by the diagonal entry D[c][c] of the panel (the L D operand of LDL^T).
+// CTAs per 128-row slab in k_split / k_split_dense: the slab's 8-column chunks
+// are spread over them, so that the few tall panels of the upper levels are
+// converted by many SMs instead of one CTA walking ~40 chunks in sequence.
+constexpr int SPLIT_CTAS = 8;
+
 __global__ void __launch_bounds__(256) k_split(DevStruct s, const SplitSlab *__restrict__ slabs, const float *P,
                                                const float *Dp, const int64_t *__restrict__ sp_off,
                                                unsigned char *img, int scale) {
@@ -1923,9 +1928,11 @@ __global__ void __launch_bounds__(256) k_split(DevStruct s, const SplitSlab *__r
     unsigned char *out = img + sp_off[k];
     const int rows = min(128, 8 * ((st + 7) / 8) - sl.r0);  // whole row groups of the panel
     const int nch = TC_CH * nkb;                             // 8-column chunks
-    const int items = 128 * nch;
+    // the slab's chunks go round robin to the gridDim.y CTAs of the slab
+    const int G = gridDim.y, nq = (nch - (int)blockIdx.y + G - 1) / G;
+    const int items = 128 * max(nq, 0);
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int r = it & 127, ch = it >> 7;
+        const int r = it & 127, ch = (int)blockIdx.y + (it >> 7) * G;
         if (r >= rows) continue;
         const int pr = sl.r0 + r;
         float v[8];
@@ -2060,8 +2067,9 @@ __global__ void __launch_bounds__(256) k_split_dense(const DenseSlab *__restrict
     unsigned char *out = img + sl.img;
     const int rows = min(128, 8 * ((sl.rows + 7) / 8) - sl.r0);
     const int nch = TC_CH * nkb;
-    for (int it = threadIdx.x; it < 128 * nch; it += blockDim.x) {
-        const int r = it & 127, ch = it >> 7;
+    const int G = gridDim.y, nq = (nch - (int)blockIdx.y + G - 1) / G;  // chunks round robin over the slab's CTAs
+    for (int it = threadIdx.x; it < 128 * max(nq, 0); it += blockDim.x) {
+        const int r = it & 127, ch = (int)blockIdx.y + (it >> 7) * G;
         if (r >= rows) continue;
         const int pr = sl.r0 + r;
         float v[8];
@@ -2468,7 +2476,7 @@ void launch_trinv(const DevStruct &s, const int *list, int count, int maxnzb, co
 
 void launch_split_dense(const DenseSlab *slabs, int count, const float *src, unsigned char *img, cudaStream_t st) {
     if (count <= 0) return;
-    k_split_dense<<<count, 256, 0, st>>>(slabs, src, img);
+    k_split_dense<<<dim3(count, SPLIT_CTAS), 256, 0, st>>>(slabs, src, img);
 }
 
 template <int FACT>
@@ -2484,7 +2492,7 @@ void launch_trsm_tc(const DevStruct &s, const UpdTile *tiles, int count, float *
 void launch_split(const DevStruct &s, const SplitSlab *slabs, int count, const float *P, const float *D,
                   const int64_t *sp_off, unsigned char *img, int scale, cudaStream_t st) {
     if (count <= 0) return;
-    k_split<<<count, 256, 0, st>>>(s, slabs, P, D, sp_off, img, scale);
+    k_split<<<dim3(count, SPLIT_CTAS), 256, 0, st>>>(s, slabs, P, D, sp_off, img, scale);
 }
 
 long long split_image_bytes(int nc, int st) { return split_bytes(nc, st); }

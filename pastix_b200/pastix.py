@@ -306,11 +306,23 @@ def numfact_device(pd: Data, values) -> None:
     _check("pgpu_numfact_device", _lib.load().pgpu_numfact_device(pd.ptr, C.c_void_p(values.data_ptr())))
 
 
+def _ld(B) -> int:
+    """Leading dimension of a column-major n or n x nrhs CUDA tensor (the
+    stride of a single column is arbitrary in torch, so it is not read)."""
+    if B.dim() == 1 or B.shape[1] == 1:
+        if B.dim() == 2 and B.stride(0) != 1 and B.shape[0] > 1:
+            raise ValueError("right-hand sides must be column major (unit stride down a column)")
+        return B.shape[0]
+    if B.stride(0) != 1:
+        raise ValueError("right-hand sides must be column major (unit stride down a column)")
+    return B.stride(1)
+
+
 def solve_device(pd: Data, B, transposed: bool = False) -> None:
     """In-place solve of a CUDA float64 tensor B (n or n x nrhs, column-major storage)."""
     n = B.shape[0]
     nrhs = 1 if B.dim() == 1 else B.shape[1]
-    ld = n if B.dim() == 1 else B.stride(1)
+    ld = _ld(B)
     fn = _lib.load().pgpu_solve_transposed_device if transposed else _lib.load().pgpu_solve_device
     _check("pgpu_solve_device", fn(pd.ptr, nrhs, C.c_void_p(B.data_ptr()), ld,
                                    C.c_void_p(_torch_stream().cuda_stream)))
@@ -318,10 +330,8 @@ def solve_device(pd: Data, B, transposed: bool = False) -> None:
 
 def solve_refine_device(pd: Data, B, X) -> None:
     """X <- refined solution of A X = B (CUDA float64 tensors, column-major)."""
-    n = B.shape[0]
     nrhs = 1 if B.dim() == 1 else B.shape[1]
-    ldb = n if B.dim() == 1 else B.stride(1)
-    ldx = n if X.dim() == 1 else X.stride(1)
+    ldb, ldx = _ld(B), _ld(X)
     _torch_stream().synchronize()
     _check("pgpu_solve_refine_device",
            _lib.load().pgpu_solve_refine_device(pd.ptr, nrhs, C.c_void_p(B.data_ptr()), ldb,

@@ -32,6 +32,7 @@ EXPORTS = [
     "pgpu_numfact_device", "pgpu_sampled_outer", "pgpu_spmv_device", "pgpu_device_status",
     "pgpu_stream", "pgpu_solve_refine_device", "pgpu_profile", "pgpu_profile_get", "pgpu_set_symbol",
     "pgpu_solve_device_static", "pgpu_graphs", "pgpu_set_tuning", "pgpu_get_tuning", "pgpu_autotune",
+    "pgpu_refine_block",
 ]
 
 # kernel classes of pgpu_profile_get, in order
@@ -125,6 +126,7 @@ def load() -> C.CDLL:
         "pgpu_solve_refine_device": (C.c_int, [P, pastix_int_t, VP, pastix_int_t, VP, pastix_int_t]),
         "pgpu_profile": (C.c_int, [P, C.c_int]),
         "pgpu_graphs": (C.c_int, [P, C.c_int]),
+        "pgpu_refine_block": (C.c_int, [P, C.c_int]),
         "pgpu_set_tuning": (C.c_int, [P, pastix_int_t, pastix_int_t, pastix_int_t]),
         "pgpu_get_tuning": (C.c_int, [P, PINT]),
         "pgpu_autotune": (C.c_int, [P, VP, PINT]),

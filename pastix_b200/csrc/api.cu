@@ -91,6 +91,13 @@ void launch_axpy(int64_t, double, const double *, double *, cudaStream_t);
 void launch_xpby(int64_t, const double *, double, double *, cudaStream_t);
 void launch_scal(int64_t, double, double *, cudaStream_t);
 void launch_gemv(int64_t, int, const double *, const double *, double *, cudaStream_t);
+void launch_spmm(int, int, const int *, const int *, const double *, double, const double *, int64_t, double, double *,
+                 int64_t, cudaStream_t);
+void launch_dots_cols(int64_t, int, int, const double *, int64_t, int64_t, const double *, int64_t, int, double *,
+                      cudaStream_t);
+void launch_axpy_cols(int64_t, int, const double *, const double *, int64_t, double *, int64_t, cudaStream_t);
+void launch_scal_cols(int64_t, int, const double *, int, double *, int64_t, cudaStream_t);
+void launch_gemv_cols(int64_t, int, int, const double *, int64_t, const double *, double *, int64_t, cudaStream_t);
 template <typename TS, typename TD>
 void launch_permute(int, int, const int64_t *, int, const TS *, int64_t, TD *, int64_t, cudaStream_t);
 template <typename TS, typename TD>
@@ -204,7 +211,7 @@ struct Device {
     DBuf<double> part, scal; // reduction partials, scalars
     DBuf<double> w1, w2;     // permuted double work vectors
     DBuf<float> wf;          // float work for mixed precision
-    DBuf<double> ws[12];     // grow-only work areas (no allocation in the steady state)
+    DBuf<double> ws[16];     // grow-only work areas (no allocation in the steady state)
     pgpu::DevStruct ds{};
 };
 
@@ -288,6 +295,8 @@ struct pastix_data_s {
     // executable CUDA graphs of the fixed launch sequences (declared after `dev`, so destroyed first)
     bool use_graphs = true;
     GraphCache graphs;
+    // GMRES refinement of several right-hand sides as one block (pgpu_refine_block)
+    bool refine_block = true;
 };
 
 // Run one launch of kernel class `cls` with `count` blocks through `fn`, on
@@ -310,7 +319,8 @@ static inline void launch_cls(pastix_data_t *pd, int cls, long long count, Fn &&
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
-enum : int { WS_SOLVE = 0, WS_ORDER, WS_GMV, WS_GMW, WS_GMG, WS_VEC, WS_BP, WS_XP, WS_RB, WS_RX };
+enum : int { WS_SOLVE = 0, WS_ORDER, WS_GMV, WS_GMW, WS_GMG, WS_VEC, WS_BP, WS_XP, WS_RB, WS_RX, WS_BGV, WS_BGS,
+             WS_SPSV };
 
 // Persistent device work area `slot` of at least `count` doubles (grown, never shrunk).
 static double *work(Device &d, int slot, size_t count) {
@@ -1805,7 +1815,17 @@ struct Refiner {
     void copy(const double *a, double *b) { cudaMemcpyAsync(b, a, n * 8, cudaMemcpyDeviceToDevice, d.stream); }
     void axpy(double a, const double *x, double *y) { pgpu::launch_axpy(n, a, x, y, d.stream); }
     void scal(double a, double *x) { pgpu::launch_scal(n, a, x, d.stream); }
-    int spsv(double *x) { return precond ? solve_perm_d(pd, 0, x, (int)n, 1) : 0; }
+    // M^{-1} x in place, solved in one fixed work vector so that the captured
+    // solve graph is the same for every Krylov vector
+    int spsv(double *x) {
+        if (!precond) return 0;
+        double *s = work(d, WS_SPSV, (size_t)n);
+        if (!s) return PASTIX_ERR_OUTOFMEMORY;
+        cudaMemcpyAsync(s, x, n * 8, cudaMemcpyDeviceToDevice, d.stream);
+        int rc = solve_perm_d(pd, 0, s, (int)n, 1);
+        cudaMemcpyAsync(x, s, n * 8, cudaMemcpyDeviceToDevice, d.stream);
+        return rc;
+    }
 };
 
 // GMRES(im), right preconditioned (refinement/z_refine_gmres.c:49-371)
@@ -2000,6 +2020,173 @@ static int refine_sr(Refiner &R, double *x, const double *b, double eps, int ite
 }  // namespace
 
 // Refinement of permuted device vectors x (in/out) for rhs b (one column each).
+// GMRES(im) on a block of nb columns at once (permuted numbering): one Krylov
+// process per column, exactly the steps of refine_gmres (right
+// preconditioning, modified Gram-Schmidt, Givens rotations, per-column
+// convergence test and iteration count), with every vector operation applied
+// to the whole block -- one multi-column preconditioner solve, one SpMV pass
+// per 8 columns, column-wise dots kept on the device -- and one host
+// synchronization per iteration for the Givens step.  Columns that have
+// converged keep their iterate; their Krylov vectors are carried along unused.
+static int refine_gmres_block(pastix_data_t *pd, double *X, int64_t ldx, const double *B, int64_t ldb, int nb,
+                              double eps, int itermax, int im, std::vector<int> &iters) {
+    Device &d = pd->dev;
+    const int64_t n = pd->n;
+    const int im1 = im + 1;
+    const int64_t blk = n * nb;  // one Krylov index for all columns
+    double *V = work(d, WS_BGV, (size_t)blk * (2 * im + 2));
+    double *sc = work(d, WS_BGS, (size_t)(im + 2) * nb * 2);
+    if (!V || !sc) return PASTIX_ERR_OUTOFMEMORY;
+    double *W = V + (size_t)blk * im1;     // preconditioned directions W_0 .. W_{im-1}
+    double *Sb = W + (size_t)blk * im;     // the block solved by the preconditioner (one captured graph)
+    double *hdev = sc;                     // (im + 2) x nb: Gram-Schmidt coefficients, norms
+    double *fdev = sc + (size_t)(im + 2) * nb;
+    auto spmm = [&](double alpha, const double *x, int64_t lx, double beta, double *y, int64_t ly) {
+        launch_cls(pd, PC_SPMV, 1, [&] {
+            pgpu::launch_spmm((int)n, nb, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha, x, lx, beta, y, ly,
+                              d.stream);
+        });
+    };
+    auto col_norms = [&](const double *A, int64_t lda, std::vector<double> &out) -> int {
+        pgpu::launch_dots_cols(n, nb, 1, A, 0, lda, A, lda, 1, hdev, d.stream);
+        out.resize(nb);
+        CUDA_TRY(cudaMemcpyAsync(out.data(), hdev, nb * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+        CUDA_TRY(cudaStreamSynchronize(d.stream));
+        return PASTIX_SUCCESS;
+    };
+    std::vector<double> normb, normx, resid, hh((size_t)(im + 2) * nb), fac(nb), ycoef((size_t)im * nb);
+    int rc = col_norms(B, ldb, normb);
+    if (rc) return rc;
+    for (auto &v : normb)
+        if (v == 0.) v = 1;
+    std::vector<std::vector<double>> H(nb, std::vector<double>((size_t)im * im1)), G(nb, std::vector<double>(im1)),
+        gc(nb, std::vector<double>(im)), gs(nb, std::vector<double>(im));
+    std::vector<char> done(nb, 0), act(nb, 0);
+    std::vector<int> m(nb, 0);
+    iters.assign(nb, 0);
+    for (;;) {
+        // V_0 = B - A X, the residual of every column
+        for (int c = 0; c < nb; c++)
+            CUDA_TRY(cudaMemcpyAsync(V + c * n, B + c * ldb, n * sizeof(double), cudaMemcpyDeviceToDevice, d.stream));
+        spmm(-1.0, X, ldx, 1.0, V, n);
+        rc = col_norms(V, n, resid);
+        if (rc) return rc;
+        bool any = false;
+        for (int c = 0; c < nb; c++) {
+            if (!done[c] && (resid[c] / normb[c] <= eps || iters[c] >= itermax)) done[c] = 1;
+            act[c] = !done[c];
+            any |= act[c];
+            fac[c] = act[c] ? 1.0 / resid[c] : 0.0;
+            G[c][0] = resid[c];
+            m[c] = 0;
+        }
+        if (!any) break;
+        CUDA_TRY(cudaMemcpyAsync(fdev, fac.data(), nb * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+        pgpu::launch_scal_cols(n, nb, fdev, 0, V, n, d.stream);
+        for (int i = 0; i < im; i++) {
+            double *Vi = V + (size_t)i * blk, *Wi = W + (size_t)i * blk, *Vn = Vi + blk;
+            CUDA_TRY(cudaMemcpyAsync(Sb, Vi, (size_t)blk * sizeof(double), cudaMemcpyDeviceToDevice, d.stream));
+            rc = solve_perm_d(pd, 0, Sb, (int)n, nb);
+            if (rc) return rc;
+            CUDA_TRY(cudaMemcpyAsync(Wi, Sb, (size_t)blk * sizeof(double), cudaMemcpyDeviceToDevice, d.stream));
+            spmm(1.0, Wi, n, 0.0, Vn, n);
+            for (int j = 0; j <= i; j++) {  // modified Gram-Schmidt, coefficients kept on the device
+                double *hj = hdev + (size_t)j * nb;
+                pgpu::launch_dots_cols(n, nb, 1, V + (size_t)j * blk, 0, n, Vn, n, 0, hj, d.stream);
+                pgpu::launch_axpy_cols(n, nb, hj, V + (size_t)j * blk, n, Vn, n, d.stream);
+            }
+            double *hn = hdev + (size_t)(i + 1) * nb;
+            pgpu::launch_dots_cols(n, nb, 1, Vn, 0, n, Vn, n, 1, hn, d.stream);
+            pgpu::launch_scal_cols(n, nb, hn, 1, Vn, n, d.stream);
+            CUDA_TRY(cudaMemcpyAsync(hh.data(), hdev, (size_t)(i + 2) * nb * sizeof(double), cudaMemcpyDeviceToHost,
+                                     d.stream));
+            CUDA_TRY(cudaStreamSynchronize(d.stream));
+            bool more = false;
+            for (int c = 0; c < nb; c++) {
+                if (!act[c]) continue;
+                double *Hi = H[c].data() + (size_t)i * im1;
+                for (int j = 0; j <= i + 1; j++) Hi[j] = hh[(size_t)j * nb + c];
+                for (int j = 0; j < i; j++) {
+                    double t = Hi[j];
+                    Hi[j] = gc[c][j] * t + gs[c][j] * Hi[j + 1];
+                    Hi[j + 1] = gc[c][j] * Hi[j + 1] - gs[c][j] * t;
+                }
+                double t = std::sqrt(Hi[i] * Hi[i] + Hi[i + 1] * Hi[i + 1]);
+                if (std::fabs(t) <= eps) t = eps;
+                gc[c][i] = Hi[i] / t;
+                gs[c][i] = Hi[i + 1] / t;
+                G[c][i + 1] = -gs[c][i] * G[c][i];
+                G[c][i] = gc[c][i] * G[c][i];
+                Hi[i] = gc[c][i] * Hi[i] + gs[c][i] * Hi[i + 1];
+                iters[c]++;
+                m[c] = i + 1;
+                if (i + 1 >= im || std::fabs(G[c][i + 1]) / normb[c] <= eps || iters[c] >= itermax) act[c] = 0;
+                more |= act[c];
+            }
+            if (!more) break;
+        }
+        // X += W y with y = H^{-1} G per column (upper triangular, m[c] columns)
+        std::fill(ycoef.begin(), ycoef.end(), 0.0);
+        int mmax = 0;
+        for (int c = 0; c < nb; c++) {
+            const int mc = m[c];
+            mmax = std::max(mmax, mc);
+            std::vector<double> y(G[c].begin(), G[c].begin() + mc);
+            for (int r = mc - 1; r >= 0; r--) {
+                double t = y[r];
+                for (int q = r + 1; q < mc; q++) t -= H[c][(size_t)q * im1 + r] * y[q];
+                y[r] = t / H[c][(size_t)r * im1 + r];
+            }
+            for (int r = 0; r < mc; r++) ycoef[(size_t)r * nb + c] = y[r];
+        }
+        if (mmax > 0) {
+            CUDA_TRY(cudaMemcpyAsync(hdev, ycoef.data(), (size_t)mmax * nb * sizeof(double), cudaMemcpyHostToDevice,
+                                     d.stream));
+            pgpu::launch_gemv_cols(n, nb, mmax, W, blk, hdev, X, ldx, d.stream);
+        }
+        for (int c = 0; c < nb; c++)
+            if (iters[c] >= itermax) done[c] = 1;  // as refine_gmres: no residual test after the last cycle
+    }
+    CUDA_TRY(cudaStreamSynchronize(d.stream));
+    return PASTIX_SUCCESS;
+}
+
+static int refine_perm(pastix_data_t *pd, double *x, const double *b, int &iters);
+
+// Refinement of nrhs permuted columns: GMRES in blocks of columns (as many as
+// a quarter of the free device memory holds, at most 256) when several right-hand
+// sides are refined, one column at a time otherwise (the reference's loop,
+// refinement/pastix_task_refine.c:121-164).
+static int refine_columns(pastix_data_t *pd, double *X, int64_t ldx, const double *B, int64_t ldb, int nrhs,
+                          pastix_int_t &maxit) {
+    maxit = 0;
+    const int method = (int)pd->iparm[IPARM_REFINEMENT];
+    const bool gm = method != PastixRefineCG && method != PastixRefineSR && method != PastixRefineBiCGSTAB;
+    if (nrhs > 1 && gm && pd->refine_block) {
+        const int im = (int)std::max<pastix_int_t>(1, pd->iparm[IPARM_GMRES_IM]);
+        size_t fr = 0, tot = 0;
+        CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+        const size_t per_col = (size_t)pd->n * (2 * im + 2) * sizeof(double) + (size_t)pd->n * 12;
+        const int cap = (int)std::max<size_t>(1, std::min<size_t>(256, fr / 4 / std::max<size_t>(1, per_col)));
+        for (int c0 = 0; c0 < nrhs; c0 += cap) {
+            const int nb = std::min(cap, nrhs - c0);
+            std::vector<int> it;
+            int rc = refine_gmres_block(pd, X + (size_t)c0 * ldx, ldx, B + (size_t)c0 * ldb, ldb, nb,
+                                        pd->dparm[DPARM_EPSILON_REFINEMENT], (int)pd->iparm[IPARM_ITERMAX], im, it);
+            if (rc) return rc;
+            for (int v : it) maxit = std::max<pastix_int_t>(maxit, v);
+        }
+        return PASTIX_SUCCESS;
+    }
+    for (int j = 0; j < nrhs; j++) {
+        int it = 0;
+        int rc = refine_perm(pd, X + (size_t)j * ldx, B + (size_t)j * ldb, it);
+        if (rc) return rc;
+        maxit = std::max<pastix_int_t>(maxit, it);
+    }
+    return PASTIX_SUCCESS;
+}
+
 static int refine_perm(pastix_data_t *pd, double *x, const double *b, int &iters) {
     Refiner R(pd);
     double eps = pd->dparm[DPARM_EPSILON_REFINEMENT];
@@ -2019,12 +2206,10 @@ extern "C" int pastix_subtask_refine(pastix_data_t *pd, pastix_rhs_t Bp, pastix_
     CUDA_TRY(cudaSetDevice(pd->dev.dev));
     double t0 = now_s();
     pd->iparm[IPARM_NBITER] = 0;
-    for (pastix_int_t j = 0; j < Bp->n; j++) {
-        int it = 0;
-        int rc = refine_perm(pd, (double *)Xp->b + j * Xp->ld, (const double *)Bp->b + j * Bp->ld, it);
-        if (rc) return rc;
-        pd->iparm[IPARM_NBITER] = std::max<pastix_int_t>(pd->iparm[IPARM_NBITER], it);
-    }
+    pastix_int_t maxit = 0;
+    int rc = refine_columns(pd, (double *)Xp->b, Xp->ld, (const double *)Bp->b, Bp->ld, (int)Bp->n, maxit);
+    if (rc) return rc;
+    pd->iparm[IPARM_NBITER] = maxit;
     CUDA_TRY(cudaStreamSynchronize(pd->dev.stream));
     pd->dparm[DPARM_REFINE_TIME] = now_s() - t0;
     return PASTIX_SUCCESS;
@@ -2188,12 +2373,10 @@ extern "C" int pgpu_solve_refine_device(pastix_data_t *pd, pastix_int_t nrhs, co
     if (pd->dparm[DPARM_EPSILON_REFINEMENT] < 0.) pd->dparm[DPARM_EPSILON_REFINEMENT] = 1e-12;
     double t0 = now_s();
     pd->iparm[IPARM_NBITER] = 0;
-    for (pastix_int_t j = 0; j < nrhs; j++) {
-        int it = 0;
-        rc = refine_perm(pd, xp.p + j * n, bp.p + j * n, it);
-        if (rc) return rc;
-        pd->iparm[IPARM_NBITER] = std::max<pastix_int_t>(pd->iparm[IPARM_NBITER], it);
-    }
+    pastix_int_t maxit = 0;
+    rc = refine_columns(pd, xp.p, n, bp.p, n, (int)nrhs, maxit);
+    if (rc) return rc;
+    pd->iparm[IPARM_NBITER] = maxit;
     launch_cls(pd, PC_VEC, 1, [&] { pgpu::launch_permute<double, double>((int)n, (int)nrhs, d.perm.p, 0, xp.p, n, X, ldx, d.stream); });
     CUDA_TRY(cudaStreamSynchronize(d.stream));
     pd->dparm[DPARM_REFINE_TIME] = now_s() - t0;
@@ -2271,6 +2454,12 @@ extern "C" int pgpu_autotune(pastix_data_t *pd, const double *values_dev, pastix
         chosen[1] = arg[1];
         chosen[2] = arg[2];
     }
+    return PASTIX_SUCCESS;
+}
+
+extern "C" int pgpu_refine_block(pastix_data_t *pd, int enable) {
+    if (!pd) return PASTIX_ERR_BADPARAMETER;
+    pd->refine_block = enable != 0;
     return PASTIX_SUCCESS;
 }
 

@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include <algorithm>
+
 namespace pgpu {
 
 // SpMV with a group of G lanes per row.
@@ -129,6 +131,132 @@ __global__ void k_sampled(int64_t nnz, const int *__restrict__ erow, const int *
 static inline int nblk(int64_t n, int t = 256) {
     int64_t b = (n + t - 1) / t;
     return (int)(b < 148 * 32 ? (b < 1 ? 1 : b) : 148 * 32);
+}
+
+// ---------------------------------------------------------------------------
+// Column-batched vector kernels of the batched GMRES (one Krylov process per
+// right-hand side, all columns advanced together; refinement/z_refine_gmres.c
+// applied to a block of columns).  A block of nb columns has leading
+// dimension ld; per-column scalars live in device memory, so a Gram-Schmidt
+// step needs no host round trip.
+// ---------------------------------------------------------------------------
+constexpr int SPMM_CB = 8;  // columns per CTA row of k_spmm (A read once per 8 columns)
+
+// Y[:, c] = alpha A X[:, c] + beta Y[:, c] for the CTA's SPMM_CB columns.
+template <int G>
+__global__ void k_spmm(int n, int nb, const int *__restrict__ rowptr, const int *__restrict__ col,
+                       const double *__restrict__ val, double alpha, const double *__restrict__ X, int64_t ldx,
+                       double beta, double *__restrict__ Y, int64_t ldy) {
+    const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int lane = threadIdx.x % G;
+    const int c0 = blockIdx.y * SPMM_CB;
+    double acc[SPMM_CB];
+#pragma unroll
+    for (int c = 0; c < SPMM_CB; c++) acc[c] = 0.0;
+    if (gid < n) {
+        const int b = rowptr[gid], e = rowptr[gid + 1];
+        for (int p = b + lane; p < e; p += G) {
+            const double a = val[p];
+            const int64_t j = col[p];
+#pragma unroll
+            for (int c = 0; c < SPMM_CB; c++)
+                if (c0 + c < nb) acc[c] += a * X[j + (int64_t)(c0 + c) * ldx];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < SPMM_CB; c++)
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o, G);
+    if (lane == 0 && gid < n) {
+#pragma unroll
+        for (int c = 0; c < SPMM_CB; c++) {
+            if (c0 + c >= nb) break;
+            double *y = Y + gid + (int64_t)(c0 + c) * ldy;
+            *y = alpha * acc[c] + (beta == 0.0 ? 0.0 : beta * *y);
+        }
+    }
+}
+
+// out[j * nb + c] = sum_i A_j[i, c] B[i, c] for the J blocks A_j = A + j * sA
+// (sqrt of it when do_sqrt); one CTA per (column, block), fixed-order
+// reductions (deterministic).
+__global__ void k_dots_cols(int64_t n, int nb, const double *__restrict__ A, int64_t sA, int64_t lda,
+                            const double *__restrict__ B, int64_t ldb, int do_sqrt, double *__restrict__ out) {
+    __shared__ double sh[32];
+    const int c = blockIdx.x, j = blockIdx.y;
+    const double *a = A + (int64_t)j * sA + (int64_t)c * lda;
+    const double *b = B + (int64_t)c * ldb;
+    double acc = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) acc += a[i] * b[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = (threadIdx.x < blockDim.x / 32) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) out[(int64_t)j * nb + c] = do_sqrt ? sqrt(v) : v;
+    }
+}
+
+// Y[:, c] -= s[c] X[:, c]
+__global__ void k_axpy_cols(int64_t n, int nb, const double *__restrict__ s, const double *__restrict__ X,
+                            int64_t ldx, double *__restrict__ Y, int64_t ldy) {
+    const int c = blockIdx.y;
+    const double f = s[c];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        Y[i + c * ldy] -= f * X[i + c * ldx];
+}
+
+// X[:, c] *= f[c] (inverse = 0), or X[:, c] /= f[c] where f[c] > 1e-50 (inverse = 1)
+__global__ void k_scal_cols(int64_t n, int nb, const double *__restrict__ f, int inverse, double *__restrict__ X,
+                            int64_t ldx) {
+    const int c = blockIdx.y;
+    double g = f[c];
+    if (inverse) {
+        if (!(g > 1e-50)) return;
+        g = 1.0 / g;
+    }
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        X[i + c * ldx] *= g;
+}
+
+// X[:, c] += sum_{j < m} W_j[:, c] y[j * nb + c], W_j = W + j * sW (ld n)
+__global__ void k_gemv_cols(int64_t n, int nb, int m, const double *__restrict__ W, int64_t sW,
+                            const double *__restrict__ y, double *__restrict__ X, int64_t ldx) {
+    const int c = blockIdx.y;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int j = 0; j < m; j++) acc += W[(int64_t)j * sW + (int64_t)c * n + i] * y[(int64_t)j * nb + c];
+        X[i + c * ldx] += acc;
+    }
+}
+
+void launch_spmm(int n, int nb, const int *rowptr, const int *col, const double *val, double alpha, const double *X,
+                 int64_t ldx, double beta, double *Y, int64_t ldy, cudaStream_t st) {
+    if (n <= 0 || nb <= 0) return;
+    const int G = 4;
+    dim3 grid((unsigned)(((int64_t)n * G + 255) / 256), (unsigned)((nb + SPMM_CB - 1) / SPMM_CB));
+    k_spmm<G><<<grid, 256, 0, st>>>(n, nb, rowptr, col, val, alpha, X, ldx, beta, Y, ldy);
+}
+void launch_dots_cols(int64_t n, int nb, int nblk, const double *A, int64_t sA, int64_t lda, const double *B,
+                      int64_t ldb, int do_sqrt, double *out, cudaStream_t st) {
+    if (nb <= 0 || nblk <= 0) return;
+    k_dots_cols<<<dim3(nb, nblk), 1024, 0, st>>>(n, nb, A, sA, lda, B, ldb, do_sqrt, out);
+}
+static dim3 cols_grid(int64_t n, int nb) {
+    const int64_t bx = std::min<int64_t>((n + 255) / 256, std::max<int64_t>(1, 148 * 8 / std::max(1, nb)));
+    return dim3((unsigned)std::max<int64_t>(1, bx), (unsigned)nb);
+}
+void launch_axpy_cols(int64_t n, int nb, const double *s, const double *X, int64_t ldx, double *Y, int64_t ldy,
+                      cudaStream_t st) {
+    if (nb > 0) k_axpy_cols<<<cols_grid(n, nb), 256, 0, st>>>(n, nb, s, X, ldx, Y, ldy);
+}
+void launch_scal_cols(int64_t n, int nb, const double *f, int inverse, double *X, int64_t ldx, cudaStream_t st) {
+    if (nb > 0) k_scal_cols<<<cols_grid(n, nb), 256, 0, st>>>(n, nb, f, inverse, X, ldx);
+}
+void launch_gemv_cols(int64_t n, int nb, int m, const double *W, int64_t sW, const double *y, double *X, int64_t ldx,
+                      cudaStream_t st) {
+    if (nb > 0 && m > 0) k_gemv_cols<<<cols_grid(n, nb), 256, 0, st>>>(n, nb, m, W, sW, y, X, ldx);
 }
 
 void launch_spmv(int n, int64_t nnz, const int *rowptr, const int *col, const double *val, double alpha,

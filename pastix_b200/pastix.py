@@ -365,6 +365,11 @@ def autotune(pd: Data, values) -> tuple:
     return tuple(int(x) for x in v)
 
 
+def refine_block(pd: Data, enable: bool) -> None:
+    """GMRES refinement of several right-hand sides as one block (default on)."""
+    _check("pgpu_refine_block", _lib.load().pgpu_refine_block(pd.ptr, int(enable)))
+
+
 def graphs(pd: Data, enable: bool) -> None:
     """Replay the factorization and solve launch sequences as CUDA graphs (default on)."""
     _check("pgpu_graphs", _lib.load().pgpu_graphs(pd.ptr, int(enable)))

@@ -89,3 +89,48 @@ def test_mixed_ldlt(lib):
     A, grid, _ = gen.workload("el48", small=True)
     Af, b, x, ip, dp = _solve_refine(A, mtxtype.Symmetric, "SYTRF", px.refine.GMRES, mixed=True, grid=grid)
     assert backward_error(Af, x[:, 0], b[:, 0]) <= 1e-12
+
+
+def _refine_both(A, kind, fact, grid, nrhs, mixed):
+    """pastix_task_refine on nrhs columns with the GMRES block (default) and
+    with the column loop, from the same factors and the same first solve."""
+    ip, dp = px.initParam()
+    ip[px.iparm.factorization] = {"POTRF": 0, "SYTRF": 1, "GETRF": 2}[fact]
+    ip[px.iparm.refinement] = px.refine.GMRES
+    ip[px.iparm.mixed] = 1 if mixed else 0
+    dp[px.dparm.epsilon_refinement] = 1e-12
+    pd = px.init(ip, dp)
+    S = spmatrix(A, kind)
+    px.analyze_grid(pd, S, *grid)
+    px.task_numfact(pd, S)
+    Af = S.full()
+    xt = np.asfortranarray(np.random.default_rng(8).uniform(-1, 1, (A.shape[0], nrhs)))
+    b = np.asfortranarray(Af @ xt)
+    x0 = b.copy(order="F")
+    px.task_solve(pd, S, x0)
+    out = {}
+    for block in (True, False):
+        px.refine_block(pd, block)
+        x = x0.copy(order="F")
+        px.task_refine(pd, S, b, x)
+        out[block] = (x, int(ip[px.iparm.nbiter]))
+    return Af, b, out
+
+
+@pytest.mark.parametrize("name,kind,fact,nrhs", [("cd64", mtxtype.General, "GETRF", 5),
+                                                  ("el48", mtxtype.Symmetric, "SYTRF", 9)])
+def test_gmres_block_matches_columns(lib, name, kind, fact, nrhs):
+    """The GMRES block runs the per-column GMRES of z_refine_gmres.c for every
+    column at once: each column converges (backward error 1e-12) with the same
+    iteration count as the column loop (one apart at most: the multi-column
+    FP32 solve rounds differently) and to the same solution."""
+    A, grid, _ = gen.workload(name, small=True)
+    Af, b, out = _refine_both(A, kind, fact, grid, nrhs, mixed=True)
+    (xb, itb), (xc, itc) = out[True], out[False]
+    for j in range(nrhs):
+        assert backward_error(Af, xb[:, j], b[:, j]) <= 1e-12
+        assert backward_error(Af, xc[:, j], b[:, j]) <= 1e-12
+    assert abs(itb - itc) <= 1
+    # two solutions with backward error 1e-12 differ by up to cond(A) x 1e-12;
+    # the shifted indefinite elasticity matrix has cond ~1e4-1e5
+    assert np.linalg.norm(xb - xc) / np.linalg.norm(xc) <= (1e-9 if fact == "GETRF" else 1e-7)

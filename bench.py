@@ -272,6 +272,24 @@ def run_b200(args, ws, rank, local):
         results[mode]["profile"] = prof
         results[mode]["info"] = {k: info[k] for k in ("cb_lcol", "cb_fcol", "cb_stride", "coefnbr")}
         results[mode]["solve"] = time_solves(pd, n, info, mode, S)
+        # 16 right-hand sides (b = A x_true, x_true ~ U[-1,1] seed 1): time to backward error 1e-12 of all
+        xt16 = gen.rhs_uniform(n, 16, seed)
+        b16h = np.asfortranarray(Af @ xt16)
+        B16 = torch.from_numpy(np.ascontiguousarray(b16h.T)).cuda().t()
+        X16 = torch.zeros(16, n, dtype=torch.float64, device="cuda").t()
+        t16 = []
+        for rep in range(4):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            px.numfact_device(pd, vals)
+            px.solve_refine_device(pd, B16, X16)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if rep:
+                t16.append(e0.elapsed_time(e1) / 1e3)
+        X16h = X16.cpu().numpy()
+        results[mode]["rhs16"] = {"s": float(np.median(t16)), "iters": int(ip[px.iparm.nbiter]),
+                                  "berr_max": max(backward_error(Af, X16h[:, j], b16h[:, j]) for j in range(16))}
         if mode == "mixed":
             # e2e through the C ABI with host buffers
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -651,6 +669,8 @@ def main():
                  "factor_s": fp64["fact_time"], "factor_tflops": fp64["thflops"] / fp64["fact_time"] / 1e12,
                  "tuning": fp64["tuning"]},
         "factor_tflops_fp32": mixed["thflops"] / mixed["fact_time"] / 1e12,
+        "rhs16": {"fp32_refine": mixed["rhs16"], "fp64": fp64["rhs16"],
+                  "note": "factor + solve + refinement of 16 right-hand sides (block CG) to backward error 1e-12"},
         "static_pivots": fp64["npiv"],
         "roofline": roof,
         "roofline_fp64": {"kernel": "k_update_dmma + k_update", "achieved": ach64, "peak": peak64,

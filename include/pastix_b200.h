@@ -342,14 +342,16 @@ int pgpu_profile(pastix_data_t *pastix_data, int enable);
  * with enable = 1) also launches kernel by kernel. */
 int pgpu_graphs(pastix_data_t *pastix_data, int enable);
 
-/* GMRES refinement of several right-hand sides as one block (default on): the
- * per-column GMRES of refinement/z_refine_gmres.c (same steps, iterates and
- * stopping test per column) advanced for all columns together, so that each
+/* GMRES and CG refinement of several right-hand sides as one block (default
+ * on): the per-column GMRES of refinement/z_refine_gmres.c, or the per-column
+ * CG of refinement/z_refine_grad.c (same steps, iterates and stopping test per
+ * column), advanced for all columns together, so that each
  * preconditioner application is one multi-column solve instead of one solve
  * per column (the reference refines the columns one after the other,
  * refinement/pastix_task_refine.c:121-164).  enable = 0 restores the column
  * loop.  Blocks hold as many columns as a quarter of the free device memory
- * allows (2 im + 2 vectors each), at most 256. */
+ * allows (GMRES: 2 im + 2 vectors each, CG: 5), at most 256; BiCGStab and
+ * simple refinement keep the column loop. */
 int pgpu_refine_block(pastix_data_t *pastix_data, int enable);
 
 /* Bucket boundaries of the supernode update tiles (no counterpart in the

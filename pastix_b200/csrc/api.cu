@@ -98,6 +98,7 @@ void launch_dots_cols(int64_t, int, int, const double *, int64_t, int64_t, const
 void launch_axpy_cols(int64_t, int, const double *, const double *, int64_t, double *, int64_t, cudaStream_t);
 void launch_scal_cols(int64_t, int, const double *, int, double *, int64_t, cudaStream_t);
 void launch_gemv_cols(int64_t, int, int, const double *, int64_t, const double *, double *, int64_t, cudaStream_t);
+void launch_xpby_cols(int64_t, int, const double *, const double *, double *, cudaStream_t);
 template <typename TS, typename TD>
 void launch_permute(int, int, const int64_t *, int, const TS *, int64_t, TD *, int64_t, cudaStream_t);
 template <typename TS, typename TD>
@@ -2151,17 +2152,124 @@ static int refine_gmres_block(pastix_data_t *pd, double *X, int64_t ldx, const d
     return PASTIX_SUCCESS;
 }
 
+// Preconditioned CG on a block of nb columns (permuted numbering): the steps
+// of refine_cg for every column at once -- one multi-column preconditioner
+// solve and one SpMV pass per 8 columns per iteration; per-column alpha and
+// beta from column-wise dots (one host round trip each); a column that has
+// converged gets alpha = beta = 0, so its iterate stays where it stopped.
+static int refine_cg_block(pastix_data_t *pd, double *X, int64_t ldx, const double *B, int64_t ldb, int nb, double eps,
+                           int itermax, std::vector<int> &iters) {
+    Device &d = pd->dev;
+    const int64_t n = pd->n;
+    const int64_t blk = n * nb;
+    double *Rb = work(d, WS_BGV, (size_t)blk * 5);
+    double *sc = work(d, WS_BGS, (size_t)nb * 4);
+    if (!Rb || !sc) return PASTIX_ERR_OUTOFMEMORY;
+    double *Pb = Rb + blk, *Zb = Pb + blk, *Qb = Zb + blk, *Sb = Qb + blk;
+    double *d0 = sc, *d1 = sc + nb, *fa = sc + 2 * nb, *fb = sc + 3 * nb;
+    auto spmm = [&](double alpha, const double *x, int64_t lx, double beta, double *y) {
+        launch_cls(pd, PC_SPMV, 1, [&] {
+            pgpu::launch_spmm((int)n, nb, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha, x, lx, beta, y, n,
+                              d.stream);
+        });
+    };
+    auto fetch = [&](const double *src, std::vector<double> &out) -> int {
+        out.resize(nb);
+        CUDA_TRY(cudaMemcpyAsync(out.data(), src, nb * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+        CUDA_TRY(cudaStreamSynchronize(d.stream));
+        return PASTIX_SUCCESS;
+    };
+    auto precond = [&]() -> int {  // Z = M^{-1} R, solved in one fixed block
+        CUDA_TRY(cudaMemcpyAsync(Sb, Rb, (size_t)blk * sizeof(double), cudaMemcpyDeviceToDevice, d.stream));
+        int rc = solve_perm_d(pd, 0, Sb, (int)n, nb);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(Zb, Sb, (size_t)blk * sizeof(double), cudaMemcpyDeviceToDevice, d.stream));
+        return PASTIX_SUCCESS;
+    };
+    std::vector<double> normb, resid, rz, pq, rzn, a(nb), bcoef(nb);
+    pgpu::launch_dots_cols(n, nb, 1, B, 0, ldb, B, ldb, 1, d0, d.stream);
+    int rc = fetch(d0, normb);
+    if (rc) return rc;
+    for (auto &v : normb)
+        if (v == 0.) v = 1;
+    for (int c = 0; c < nb; c++)
+        CUDA_TRY(cudaMemcpyAsync(Rb + c * n, B + c * ldb, n * sizeof(double), cudaMemcpyDeviceToDevice, d.stream));
+    spmm(-1.0, X, ldx, 1.0, Rb);
+    pgpu::launch_dots_cols(n, nb, 1, Rb, 0, n, Rb, n, 1, d0, d.stream);
+    if ((rc = fetch(d0, resid))) return rc;
+    std::vector<char> act(nb);
+    bool any = false;
+    iters.assign(nb, 0);
+    for (int c = 0; c < nb; c++) {
+        act[c] = resid[c] / normb[c] > eps && itermax > 0;
+        any |= act[c];
+    }
+    if (!any) return PASTIX_SUCCESS;
+    if ((rc = precond())) return rc;
+    CUDA_TRY(cudaMemcpyAsync(Pb, Zb, (size_t)blk * sizeof(double), cudaMemcpyDeviceToDevice, d.stream));
+    pgpu::launch_dots_cols(n, nb, 1, Rb, 0, n, Zb, n, 0, d0, d.stream);
+    if ((rc = fetch(d0, rz))) return rc;
+    for (int it = 1; any; it++) {
+        spmm(1.0, Pb, n, 0.0, Qb);
+        pgpu::launch_dots_cols(n, nb, 1, Qb, 0, n, Pb, n, 0, d1, d.stream);
+        if ((rc = fetch(d1, pq))) return rc;
+        for (int c = 0; c < nb; c++) a[c] = act[c] ? rz[c] / pq[c] : 0.0;
+        std::vector<double> na(nb);
+        for (int c = 0; c < nb; c++) na[c] = -a[c];
+        CUDA_TRY(cudaMemcpyAsync(fa, na.data(), nb * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+        CUDA_TRY(cudaMemcpyAsync(fb, a.data(), nb * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+        pgpu::launch_axpy_cols(n, nb, fa, Pb, n, X, ldx, d.stream);  // X += alpha P
+        pgpu::launch_axpy_cols(n, nb, fb, Qb, n, Rb, n, d.stream);   // R -= alpha Q
+        pgpu::launch_dots_cols(n, nb, 1, Rb, 0, n, Rb, n, 1, d0, d.stream);
+        if ((rc = fetch(d0, resid))) return rc;
+        any = false;
+        for (int c = 0; c < nb; c++) {
+            if (!act[c]) continue;
+            iters[c] = it;
+            if (resid[c] / normb[c] <= eps || it >= itermax) act[c] = 0;
+            any |= act[c];
+        }
+        if (!any) break;
+        if ((rc = precond())) return rc;
+        pgpu::launch_dots_cols(n, nb, 1, Rb, 0, n, Zb, n, 0, d0, d.stream);
+        if ((rc = fetch(d0, rzn))) return rc;
+        for (int c = 0; c < nb; c++) {
+            bcoef[c] = act[c] ? rzn[c] / rz[c] : 0.0;
+            if (act[c]) rz[c] = rzn[c];
+        }
+        CUDA_TRY(cudaMemcpyAsync(fa, bcoef.data(), nb * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+        pgpu::launch_xpby_cols(n, nb, Zb, fa, Pb, d.stream);  // P = Z + beta P
+    }
+    CUDA_TRY(cudaStreamSynchronize(d.stream));
+    return PASTIX_SUCCESS;
+}
+
 static int refine_perm(pastix_data_t *pd, double *x, const double *b, int &iters);
 
-// Refinement of nrhs permuted columns: GMRES in blocks of columns (as many as
-// a quarter of the free device memory holds, at most 256) when several right-hand
-// sides are refined, one column at a time otherwise (the reference's loop,
-// refinement/pastix_task_refine.c:121-164).
+// Refinement of nrhs permuted columns: GMRES or CG in blocks of columns (as
+// many as a quarter of the free device memory holds, at most 256) when several
+// right-hand sides are refined, one column at a time otherwise (the
+// reference's loop, refinement/pastix_task_refine.c:121-164).
 static int refine_columns(pastix_data_t *pd, double *X, int64_t ldx, const double *B, int64_t ldb, int nrhs,
                           pastix_int_t &maxit) {
     maxit = 0;
     const int method = (int)pd->iparm[IPARM_REFINEMENT];
     const bool gm = method != PastixRefineCG && method != PastixRefineSR && method != PastixRefineBiCGSTAB;
+    if (nrhs > 1 && method == PastixRefineCG && pd->refine_block) {
+        size_t fr = 0, tot = 0;
+        CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+        const size_t per_col = (size_t)pd->n * 5 * sizeof(double) + (size_t)pd->n * 12;
+        const int cap = (int)std::max<size_t>(1, std::min<size_t>(256, fr / 4 / std::max<size_t>(1, per_col)));
+        for (int c0 = 0; c0 < nrhs; c0 += cap) {
+            const int nb = std::min(cap, nrhs - c0);
+            std::vector<int> it;
+            int rc = refine_cg_block(pd, X + (size_t)c0 * ldx, ldx, B + (size_t)c0 * ldb, ldb, nb,
+                                     pd->dparm[DPARM_EPSILON_REFINEMENT], (int)pd->iparm[IPARM_ITERMAX], it);
+            if (rc) return rc;
+            for (int v : it) maxit = std::max<pastix_int_t>(maxit, v);
+        }
+        return PASTIX_SUCCESS;
+    }
     if (nrhs > 1 && gm && pd->refine_block) {
         const int im = (int)std::max<pastix_int_t>(1, pd->iparm[IPARM_GMRES_IM]);
         size_t fr = 0, tot = 0;

@@ -231,6 +231,15 @@ __global__ void k_gemv_cols(int64_t n, int nb, int m, const double *__restrict__
     }
 }
 
+// P[:, c] = Z[:, c] + beta[c] P[:, c]
+__global__ void k_xpby_cols(int64_t n, int nb, const double *__restrict__ Z, const double *__restrict__ beta,
+                            double *__restrict__ P) {
+    const int c = blockIdx.y;
+    const double b = beta[c];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        P[i + c * n] = Z[i + c * n] + b * P[i + c * n];
+}
+
 void launch_spmm(int n, int nb, const int *rowptr, const int *col, const double *val, double alpha, const double *X,
                  int64_t ldx, double beta, double *Y, int64_t ldy, cudaStream_t st) {
     if (n <= 0 || nb <= 0) return;
@@ -253,6 +262,9 @@ void launch_axpy_cols(int64_t n, int nb, const double *s, const double *X, int64
 }
 void launch_scal_cols(int64_t n, int nb, const double *f, int inverse, double *X, int64_t ldx, cudaStream_t st) {
     if (nb > 0) k_scal_cols<<<cols_grid(n, nb), 256, 0, st>>>(n, nb, f, inverse, X, ldx);
+}
+void launch_xpby_cols(int64_t n, int nb, const double *Z, const double *beta, double *P, cudaStream_t st) {
+    if (nb > 0) k_xpby_cols<<<cols_grid(n, nb), 256, 0, st>>>(n, nb, Z, beta, P);
 }
 void launch_gemv_cols(int64_t n, int nb, int m, const double *W, int64_t sW, const double *y, double *X, int64_t ldx,
                       cudaStream_t st) {

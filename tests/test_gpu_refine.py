@@ -91,12 +91,12 @@ def test_mixed_ldlt(lib):
     assert backward_error(Af, x[:, 0], b[:, 0]) <= 1e-12
 
 
-def _refine_both(A, kind, fact, grid, nrhs, mixed):
-    """pastix_task_refine on nrhs columns with the GMRES block (default) and
-    with the column loop, from the same factors and the same first solve."""
+def _refine_both(A, kind, fact, grid, nrhs, mixed, method=px.refine.GMRES):
+    """pastix_task_refine on nrhs columns as one block (default) and with the
+    column loop, from the same factors and the same first solve."""
     ip, dp = px.initParam()
     ip[px.iparm.factorization] = {"POTRF": 0, "SYTRF": 1, "GETRF": 2}[fact]
-    ip[px.iparm.refinement] = px.refine.GMRES
+    ip[px.iparm.refinement] = method
     ip[px.iparm.mixed] = 1 if mixed else 0
     dp[px.dparm.epsilon_refinement] = 1e-12
     pd = px.init(ip, dp)
@@ -117,15 +117,19 @@ def _refine_both(A, kind, fact, grid, nrhs, mixed):
     return Af, b, out
 
 
-@pytest.mark.parametrize("name,kind,fact,nrhs", [("cd64", mtxtype.General, "GETRF", 5),
-                                                  ("el48", mtxtype.Symmetric, "SYTRF", 9)])
-def test_gmres_block_matches_columns(lib, name, kind, fact, nrhs):
-    """The GMRES block runs the per-column GMRES of z_refine_gmres.c for every
-    column at once: each column converges (backward error 1e-12) with the same
-    iteration count as the column loop (one apart at most: the multi-column
-    FP32 solve rounds differently) and to the same solution."""
+@pytest.mark.parametrize("name,kind,fact,nrhs,method", [
+    ("cd64", mtxtype.General, "GETRF", 5, px.refine.GMRES),
+    ("el48", mtxtype.Symmetric, "SYTRF", 9, px.refine.GMRES),
+    ("lap100", mtxtype.Symmetric, "POTRF", 6, px.refine.CG),
+    ("grf512", mtxtype.Symmetric, "POTRF", 3, px.refine.CG)])
+def test_block_refinement_matches_columns(lib, name, kind, fact, nrhs, method):
+    """The refinement block runs the per-column GMRES (z_refine_gmres.c) or CG
+    (z_refine_grad.c) for every column at once: each column converges
+    (backward error 1e-12) with the same iteration count as the column loop
+    (one apart at most: the multi-column FP32 solve rounds differently) and to
+    the same solution."""
     A, grid, _ = gen.workload(name, small=True)
-    Af, b, out = _refine_both(A, kind, fact, grid, nrhs, mixed=True)
+    Af, b, out = _refine_both(A, kind, fact, grid, nrhs, mixed=True, method=method)
     (xb, itb), (xc, itc) = out[True], out[False]
     for j in range(nrhs):
         assert backward_error(Af, xb[:, j], b[:, j]) <= 1e-12

@@ -369,8 +369,9 @@ int pgpu_get_tuning(const pastix_data_t *pastix_data, pastix_int_t *vals);
 /* Autotuner of those bucket boundaries for the analysed matrix: each candidate
  * (FP64: dmma_n in {8, 16, 32, 64} x dmma_k in {16, 32}; FP32: tc_k in
  * {32, 48, 64, 96}) is applied and timed on a factorization of the given
- * device values (spm value order, as pgpu_numfact_device); the fastest stays
- * in effect and the matrix is left factorized with it.  chosen (if not NULL)
+ * device values (spm value order, as pgpu_numfact_device); the buckets in
+ * effect are kept unless a candidate is at least 2 % faster, and the matrix is
+ * left factorized with the buckets chosen.  chosen (if not NULL)
  * receives {dmma_n, dmma_k, tc_k}. */
 int pgpu_autotune(pastix_data_t *pastix_data, const double *values_dev, pastix_int_t *chosen);
 int pgpu_profile_get(pastix_data_t *pastix_data, double *ms, long long *launches, int nclass);

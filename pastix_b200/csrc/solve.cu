@@ -151,21 +151,31 @@ __global__ void __launch_bounds__(256) k_bwd_diag(DevStruct s, const int *__rest
 // (transposed, FP32) by the FP32 factorization for its TRSM: Pt = T^{-T},
 // column major nc x nc, lower triangular.  Forward: y <- S Pt y; backward:
 // x <- Pt^T S x (S = D for LDL^T, else I) -- the blocked steps of
-// solve_cblk_ztrsmsp_forward / _backward as one dense product.  One right-hand
-// side.  A cluster of TC CTAs shares one cblk: every CTA copies y_k to its
-// shared memory, the cluster barrier then guarantees that all copies are made
-// before any CTA overwrites y_k in place, and 32-row (forward) or 32-column
-// (backward) blocks of Pt go round robin to the CTAs, so each reads about
-// 1/TC of the inverse instead of one CTA reading all of it while the level's
-// other SMs wait.
+// solve_cblk_ztrsmsp_forward / _backward as one dense product, for RC
+// right-hand sides.  A cluster of TC CTAs shares one cblk: every CTA copies
+// y_k to its shared memory, and the lower triangle of Pt is cut into 32 x 32
+// tiles spread over the cluster's 8 * TC warps (at most two each, 32
+// independent coalesced loads per lane), so that no warp walks a long row or
+// column alone.  Partial sums go by distributed-shared-memory atomics to the
+// CTA that owns the 32 outputs (block b -> CTA b % TC); a second cluster
+// barrier orders every partial before the owners overwrite y_k in place.
 constexpr int TC = 8;
+
+// Tile t of the lower triangle of an nch x nch block grid, row by row:
+// (i, jc) with jc <= i and t = i (i + 1) / 2 + jc.
+__device__ __forceinline__ void tri_tile(int t, int &i, int &jc) {
+    i = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
+    while ((i + 1) * (i + 2) / 2 <= t) i++;
+    while (i * (i + 1) / 2 > t) i--;
+    jc = t - i * (i + 1) / 2;
+}
 
 template <typename T, int RC>
 __global__ void __cluster_dims__(TC, 1, 1) __launch_bounds__(256)
     k_fwd_diag_tinv(DevStruct s, const int *__restrict__ list, int zside, int scaled, const T *Ldiag, T *Y, int ldy,
                     int nrhs, const float *__restrict__ tinv, const int64_t *__restrict__ ti_off) {
     __shared__ float ys[RC][384];
-    __shared__ float part[8][RC][33];
+    __shared__ float acc[RC][384];
     const int k = list[blockIdx.x / TC];
     const int64_t off = ti_off[k];
     if (off < 0) return;  // the whole cluster leaves: k_fwd_diag_inv takes this cblk
@@ -176,40 +186,60 @@ __global__ void __cluster_dims__(TC, 1, 1) __launch_bounds__(256)
     const int st = s.cb_stride[k];
     const int j0 = blockIdx.y * RC, nr = min(RC, nrhs - j0);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int e = tid; e < nc * RC; e += blockDim.x) {
-        const int i = e % nc, j = e / nc;
-        ys[j][i] = j < nr ? (float)Y[fc + i + (size_t)(j0 + j) * ldy] : 0.f;
+    const int npad = 32 * ((nc + 31) / 32);  // whole 32-blocks: the tiles read ys up to npad
+    for (int e = tid; e < npad * RC; e += blockDim.x) {
+        const int i = e % npad, j = e / npad;
+        ys[j][i] = (j < nr && i < nc) ? (float)Y[fc + i + (size_t)(j0 + j) * ldy] : 0.f;
+        acc[j][i] = 0.f;
     }
-    cluster.sync();
+    cluster.sync();  // every copy of y_k made, every accumulator cleared
     const float *Pt = tinv + off + (size_t)zside * nc * nc;
-    for (int cb = rank * 32; cb < nc; cb += TC * 32) {
-        const int c = cb + lane;
-        const int kend = min(nc, cb + 32);  // Pt is lower triangular: columns past the block are zero
-        float acc[RC];
+    const int nch = (nc + 31) / 32, ntile = nch * (nch + 1) / 2;
+    for (int t = rank * 8 + warp; t < ntile; t += TC * 8) {
+        int i, jc;
+        tri_tile(t, i, jc);
+        const int r = 32 * i + lane, c0 = 32 * jc;
+        float a[RC];
 #pragma unroll
-        for (int j = 0; j < RC; j++) acc[j] = 0.f;
-        if (c < nc) {
-#pragma unroll 8
-            for (int kk = warp; kk < kend; kk += 8) {
-                const float pv = Pt[c + (size_t)kk * nc];
+        for (int j = 0; j < RC; j++) a[j] = 0.f;
+        if (r < nc) {
+            float p[32];
 #pragma unroll
-                for (int j = 0; j < RC; j++) acc[j] += pv * ys[j][kk];
+            for (int u = 0; u < 32; u++) p[u] = (c0 + u < nc) ? Pt[r + (size_t)(c0 + u) * nc] : 0.f;
+#pragma unroll
+            for (int u = 0; u < 32; u++)
+#pragma unroll
+                for (int j = 0; j < RC; j++) a[j] += p[u] * ys[j][c0 + u];
+            float *dst = cluster.map_shared_rank(&acc[0][0], i % TC);
+#pragma unroll
+            for (int j = 0; j < RC; j++)
+                if (j < nr) atomicAdd(dst + j * 384 + r, a[j]);
+        }
+    }
+    cluster.sync();  // every partial sum in place
+    for (int cb = rank * 32; cb < nc; cb += TC * 32)
+        for (int e = tid; e < 32 * RC; e += blockDim.x) {
+            const int l = e & 31, j = e >> 5, c = cb + l;
+            if (c < nc && j < nr) {
+                float v = acc[j][c];
+                if (scaled) v *= (float)Ldiag[s.cb_coef[k] + c + (size_t)c * st];
+                Y[fc + c + (size_t)(j0 + j) * ldy] = (T)v;
             }
         }
+}
+
+// Sum over the 32 lanes of v[u] for every u at once (butterfly transpose
+// reduction, 31 shuffles): on return lane l holds in v[0] the sum of v[l].
+__device__ __forceinline__ void lane_sums32(float (&v)[32], int lane) {
 #pragma unroll
-        for (int j = 0; j < RC; j++) part[warp][j][lane] = acc[j];
-        __syncthreads();
-        for (int o = tid; o < 32 * RC; o += blockDim.x) {
-            const int l = o & 31, j = o >> 5, cc = cb + l;
-            if (cc < nc && j < nr) {
-                float v = 0.f;
+    for (int sft = 16; sft >= 1; sft >>= 1) {
+        const bool upper = (lane & sft) != 0;
 #pragma unroll
-                for (int w = 0; w < 8; w++) v += part[w][j][l];
-                if (scaled) v *= (float)Ldiag[s.cb_coef[k] + cc + (size_t)cc * st];
-                Y[fc + cc + (size_t)(j0 + j) * ldy] = (T)v;
-            }
+        for (int u = 0; u < sft; u++) {
+            const float send = upper ? v[u] : v[u + sft];
+            const float keep = upper ? v[u + sft] : v[u];
+            v[u] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
         }
-        __syncthreads();
     }
 }
 
@@ -218,6 +248,7 @@ __global__ void __cluster_dims__(TC, 1, 1) __launch_bounds__(256)
     k_bwd_diag_tinv(DevStruct s, const int *__restrict__ list, int zside, int scaled, const T *Ldiag, T *Y, int ldy,
                     int nrhs, const float *__restrict__ tinv, const int64_t *__restrict__ ti_off) {
     __shared__ float xs[RC][384];
+    __shared__ float acc[RC][384];
     const int k = list[blockIdx.x / TC];
     const int64_t off = ti_off[k];
     if (off < 0) return;  // the whole cluster leaves: k_bwd_diag_inv takes this cblk
@@ -228,43 +259,44 @@ __global__ void __cluster_dims__(TC, 1, 1) __launch_bounds__(256)
     const int st = s.cb_stride[k];
     const int j0 = blockIdx.y * RC, nr = min(RC, nrhs - j0);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int e = tid; e < nc * RC; e += blockDim.x) {
-        const int i = e % nc, j = e / nc;
-        float v = j < nr ? (float)Y[fc + i + (size_t)(j0 + j) * ldy] : 0.f;
-        if (scaled) v *= (float)Ldiag[s.cb_coef[k] + i + (size_t)i * st];
+    const int npad = 32 * ((nc + 31) / 32);
+    for (int e = tid; e < npad * RC; e += blockDim.x) {
+        const int i = e % npad, j = e / npad;
+        float v = (j < nr && i < nc) ? (float)Y[fc + i + (size_t)(j0 + j) * ldy] : 0.f;
+        if (scaled && i < nc) v *= (float)Ldiag[s.cb_coef[k] + i + (size_t)i * st];
         xs[j][i] = v;
+        acc[j][i] = 0.f;
     }
     cluster.sync();
     const float *Pt = tinv + off + (size_t)zside * nc * nc;
-    // x_c = sum_{r >= c} Pt[r, c] xs[r]: four columns per warp, lanes over the rows (coalesced)
-    for (int cb = rank * 32; cb < nc; cb += TC * 32) {
-        const int c0 = cb + 4 * warp;
-        float acc[4][RC];
+    // x_c = sum_{r >= c} Pt[r, c] xs[r]: tile (row block i, column block jc <= i), lanes over the rows
+    const int nch = (nc + 31) / 32, ntile = nch * (nch + 1) / 2;
+    for (int t = rank * 8 + warp; t < ntile; t += TC * 8) {
+        int i, jc;
+        tri_tile(t, i, jc);
+        const int r = 32 * i + lane, c0 = 32 * jc;
+        float p[32];
 #pragma unroll
-        for (int u = 0; u < 4; u++)
+        for (int u = 0; u < 32; u++)
+            p[u] = (r < nc && c0 + u < nc && r >= c0 + u) ? Pt[r + (size_t)(c0 + u) * nc] : 0.f;
+        float *dst = cluster.map_shared_rank(&acc[0][0], jc % TC);
 #pragma unroll
-            for (int j = 0; j < RC; j++) acc[u][j] = 0.f;
-        for (int r = c0 + lane; r < nc; r += 32) {
-            float pv[4];
+        for (int j = 0; j < RC; j++) {
+            if (j >= nr) break;
+            const float xr = r < nc ? xs[j][r] : 0.f;
+            float v[32];
 #pragma unroll
-            for (int u = 0; u < 4; u++) pv[u] = (c0 + u < nc && r >= c0 + u) ? Pt[r + (size_t)(c0 + u) * nc] : 0.f;
-#pragma unroll
-            for (int j = 0; j < RC; j++) {
-                const float xr = xs[j][r];
-#pragma unroll
-                for (int u = 0; u < 4; u++) acc[u][j] += pv[u] * xr;
-            }
+            for (int u = 0; u < 32; u++) v[u] = p[u] * xr;
+            lane_sums32(v, lane);
+            if (c0 + lane < nc) atomicAdd(dst + j * 384 + c0 + lane, v[0]);
         }
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-#pragma unroll
-            for (int j = 0; j < RC; j++) {
-                float v = acc[u][j];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0 && c0 + u < nc && j < nr) Y[fc + c0 + u + (size_t)(j0 + j) * ldy] = (T)v;
-            }
     }
+    cluster.sync();  // every partial sum in place
+    for (int cb = rank * 32; cb < nc; cb += TC * 32)
+        for (int e = tid; e < 32 * RC; e += blockDim.x) {
+            const int l = e & 31, j = e >> 5, c = cb + l;
+            if (c < nc && j < nr) Y[fc + c + (size_t)(j0 + j) * ldy] = (T)acc[j][c];
+        }
 }
 
 template <typename T, int RC>

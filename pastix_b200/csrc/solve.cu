@@ -228,6 +228,118 @@ __global__ void __cluster_dims__(TC, 1, 1) __launch_bounds__(256)
         }
 }
 
+// Groups of 8 right-hand sides: 8 products per loaded element make the work
+// compute-heavy enough that 32-row (forward) or 32-column (backward) blocks
+// round robin over the cluster's CTAs, with no cross-CTA partial sums, beat the
+// tiled kernels (whose remote atomics grow with the number of right-hand
+// sides); a single right-hand side uses the tiled kernels.
+template <typename T, int RC>
+__global__ void __cluster_dims__(TC, 1, 1) __launch_bounds__(256)
+    k_fwd_diag_tinv_rr(DevStruct s, const int *__restrict__ list, int zside, int scaled, const T *Ldiag, T *Y, int ldy,
+                    int nrhs, const float *__restrict__ tinv, const int64_t *__restrict__ ti_off) {
+    __shared__ float ys[RC][384];
+    __shared__ float part[8][RC][33];
+    const int k = list[blockIdx.x / TC];
+    const int64_t off = ti_off[k];
+    if (off < 0) return;  // the whole cluster leaves: k_fwd_diag_inv takes this cblk
+    cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int fc = s.cb_fcol[k];
+    const int nc = s.cb_lcol[k] - fc + 1;
+    const int st = s.cb_stride[k];
+    const int j0 = blockIdx.y * RC, nr = min(RC, nrhs - j0);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < nc * RC; e += blockDim.x) {
+        const int i = e % nc, j = e / nc;
+        ys[j][i] = j < nr ? (float)Y[fc + i + (size_t)(j0 + j) * ldy] : 0.f;
+    }
+    cluster.sync();
+    const float *Pt = tinv + off + (size_t)zside * nc * nc;
+    for (int cb = rank * 32; cb < nc; cb += TC * 32) {
+        const int c = cb + lane;
+        const int kend = min(nc, cb + 32);  // Pt is lower triangular: columns past the block are zero
+        float acc[RC];
+#pragma unroll
+        for (int j = 0; j < RC; j++) acc[j] = 0.f;
+        if (c < nc) {
+#pragma unroll 8
+            for (int kk = warp; kk < kend; kk += 8) {
+                const float pv = Pt[c + (size_t)kk * nc];
+#pragma unroll
+                for (int j = 0; j < RC; j++) acc[j] += pv * ys[j][kk];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < RC; j++) part[warp][j][lane] = acc[j];
+        __syncthreads();
+        for (int o = tid; o < 32 * RC; o += blockDim.x) {
+            const int l = o & 31, j = o >> 5, cc = cb + l;
+            if (cc < nc && j < nr) {
+                float v = 0.f;
+#pragma unroll
+                for (int w = 0; w < 8; w++) v += part[w][j][l];
+                if (scaled) v *= (float)Ldiag[s.cb_coef[k] + cc + (size_t)cc * st];
+                Y[fc + cc + (size_t)(j0 + j) * ldy] = (T)v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int RC>
+__global__ void __cluster_dims__(TC, 1, 1) __launch_bounds__(256)
+    k_bwd_diag_tinv_rr(DevStruct s, const int *__restrict__ list, int zside, int scaled, const T *Ldiag, T *Y, int ldy,
+                    int nrhs, const float *__restrict__ tinv, const int64_t *__restrict__ ti_off) {
+    __shared__ float xs[RC][384];
+    const int k = list[blockIdx.x / TC];
+    const int64_t off = ti_off[k];
+    if (off < 0) return;  // the whole cluster leaves: k_bwd_diag_inv takes this cblk
+    cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int fc = s.cb_fcol[k];
+    const int nc = s.cb_lcol[k] - fc + 1;
+    const int st = s.cb_stride[k];
+    const int j0 = blockIdx.y * RC, nr = min(RC, nrhs - j0);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < nc * RC; e += blockDim.x) {
+        const int i = e % nc, j = e / nc;
+        float v = j < nr ? (float)Y[fc + i + (size_t)(j0 + j) * ldy] : 0.f;
+        if (scaled) v *= (float)Ldiag[s.cb_coef[k] + i + (size_t)i * st];
+        xs[j][i] = v;
+    }
+    cluster.sync();
+    const float *Pt = tinv + off + (size_t)zside * nc * nc;
+    // x_c = sum_{r >= c} Pt[r, c] xs[r]: four columns per warp, lanes over the rows (coalesced)
+    for (int cb = rank * 32; cb < nc; cb += TC * 32) {
+        const int c0 = cb + 4 * warp;
+        float acc[4][RC];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int j = 0; j < RC; j++) acc[u][j] = 0.f;
+        for (int r = c0 + lane; r < nc; r += 32) {
+            float pv[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) pv[u] = (c0 + u < nc && r >= c0 + u) ? Pt[r + (size_t)(c0 + u) * nc] : 0.f;
+#pragma unroll
+            for (int j = 0; j < RC; j++) {
+                const float xr = xs[j][r];
+#pragma unroll
+                for (int u = 0; u < 4; u++) acc[u][j] += pv[u] * xr;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int j = 0; j < RC; j++) {
+                float v = acc[u][j];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0 && c0 + u < nc && j < nr) Y[fc + c0 + u + (size_t)(j0 + j) * ldy] = (T)v;
+            }
+    }
+}
+
 // Sum over the 32 lanes of v[u] for every u at once (butterfly transpose
 // reduction, 31 shuffles): on return lane l holds in v[0] the sum of v[l].
 __device__ __forceinline__ void lane_sums32(float (&v)[32], int lane) {
@@ -623,7 +735,7 @@ void launch_fwd_diag_inv(const DevStruct &s, const int *list, int count, int max
     const int ZDIM = 1;
     if (ntinv > 0) {
         if (nrhs == 1) k_fwd_diag_tinv<T, 1><<<count * TC, 256, 0, st>>>(s, list, zside, scaled, Ld, Y, ldy, nrhs, tinv, ti_off);
-        else k_fwd_diag_tinv<T, 8><<<dim3(count * TC, (nrhs + 7) / 8), 256, 0, st>>>(s, list, zside, scaled, Ld, Y, ldy, nrhs, tinv, ti_off);
+        else k_fwd_diag_tinv_rr<T, 8><<<dim3(count * TC, (nrhs + 7) / 8), 256, 0, st>>>(s, list, zside, scaled, Ld, Y, ldy, nrhs, tinv, ti_off);
     }
     if (ntinv < count)
         PGPU_RC_DISPATCH(nrhs, k_fwd_diag_inv, count, (size_t)maxnc * sizeof(T), s, list, P, dinv, zside, scaled, Ld,
@@ -638,7 +750,7 @@ void launch_bwd_diag_inv(const DevStruct &s, const int *list, int count, int max
     const int ZDIM = 1;
     if (ntinv > 0) {
         if (nrhs == 1) k_bwd_diag_tinv<T, 1><<<count * TC, 256, 0, st>>>(s, list, zside, scaled, Ld, Y, ldy, nrhs, tinv, ti_off);
-        else k_bwd_diag_tinv<T, 8><<<dim3(count * TC, (nrhs + 7) / 8), 256, 0, st>>>(s, list, zside, scaled, Ld, Y, ldy, nrhs, tinv, ti_off);
+        else k_bwd_diag_tinv_rr<T, 8><<<dim3(count * TC, (nrhs + 7) / 8), 256, 0, st>>>(s, list, zside, scaled, Ld, Y, ldy, nrhs, tinv, ti_off);
     }
     if (ntinv < count)
         PGPU_RC_DISPATCH(nrhs, k_bwd_diag_inv, count, (size_t)maxnc * sizeof(T), s, list, P, dinv, zside, scaled, Ld,

@@ -161,6 +161,16 @@ typedef struct pastix_order_s {
 typedef struct pastix_data_s pastix_data_t;
 typedef struct pastix_rhs_s *pastix_rhs_t;
 
+/* IPARM_IO_STRATEGY values (include/pastix/api.h:228-236).  PastixIOLoad: a
+ * personal ordering is read from the ordering file and the block symbol from
+ * "symbname"; PastixIOSave: both are written ("ordergen", "symbgen") after
+ * ordering and symbolic factorization.  The graph and CSC variants are not
+ * implemented (ignored). */
+typedef enum pastix_io_e {
+    PastixIONo = 0, PastixIOLoad = 1, PastixIOSave = 2, PastixIOLoadGraph = 4, PastixIOSaveGraph = 8,
+    PastixIOLoadCSC = 16, PastixIOSaveCSC = 32
+} pastix_io_t;
+
 /* ---- main API (include/pastix.h:56-125) ---- */
 /* replaces include/pastix.h:89 (pastixInitParam, common/api.c:420) */
 void pastixInitParam(pastix_int_t *iparm, double *dparm);
@@ -232,6 +242,14 @@ int pastixRhsSingleToDouble(const pastix_rhs_t sB, pastix_rhs_t dB);
 /* ---- ordering helpers (include/pastix/order.h) ---- */
 /* replaces order/order_grids.c:307 (pastixOrderGrid); *myorder must point to a struct */
 int pastixOrderGrid(pastix_order_t **myorder, pastix_int_t nx, pastix_int_t ny, pastix_int_t nz);
+/* replaces order/order_io.c:132 (pastixOrderLoad): reads the reference's ordering
+ * text format from $PASTIX_FILE_ORDER or "ordername" into *ordemesh (0-based;
+ * rangtab / treetab NULL for a version-0 file without the elimination tree) */
+int pastixOrderLoad(const pastix_data_t *pastix_data, pastix_order_t *ordemesh);
+/* replaces order/order_io.c:296 (pastixOrderSave): writes *ordemesh in the same
+ * format to "ordergen" (or $PASTIX_FILE_ORDER) in the instance's output
+ * directory "<$PASTIX_OUTPUT_DIR or pastix>-XXXXXX" */
+int pastixOrderSave(pastix_data_t *pastix_data, const pastix_order_t *ordemesh);
 /* replaces order/order.c (pastixOrderExit): frees the arrays of an order filled by this library */
 void pastixOrderExit(pastix_order_t *ordeptr);
 

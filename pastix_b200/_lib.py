@@ -27,7 +27,7 @@ EXPORTS = [
     "pastix_subtask_applyorder", "pastix_subtask_trsm", "pastix_subtask_diag", "pastix_subtask_solve",
     "pastix_subtask_solve_adv", "pastix_subtask_refine",
     "pastixRhsInit", "pastixRhsFinalize", "pastixRhsDoubletoSingle", "pastixRhsSingleToDouble",
-    "pastixOrderGrid", "pastixOrderExit",
+    "pastixOrderGrid", "pastixOrderExit", "pastixOrderLoad", "pastixOrderSave",
     "pgpu_solver_info", "pgpu_get_coeftab", "pgpu_solve_device", "pgpu_solve_transposed_device",
     "pgpu_numfact_device", "pgpu_sampled_outer", "pgpu_spmv_device", "pgpu_device_status",
     "pgpu_stream", "pgpu_solve_refine_device", "pgpu_profile", "pgpu_profile_get", "pgpu_set_symbol",
@@ -113,6 +113,8 @@ def load() -> C.CDLL:
         "pastixRhsFinalize": (C.c_int, [P]),
         "pastixOrderGrid": (C.c_int, [C.POINTER(C.POINTER(pastix_order_t)), pastix_int_t, pastix_int_t, pastix_int_t]),
         "pastixOrderExit": (None, [C.POINTER(pastix_order_t)]),
+        "pastixOrderLoad": (C.c_int, [P, C.POINTER(pastix_order_t)]),
+        "pastixOrderSave": (C.c_int, [P, C.POINTER(pastix_order_t)]),
         "pgpu_solver_info": (C.c_int, [P, C.POINTER(pgpu_solver_info_t)]),
         "pgpu_get_coeftab": (C.c_int, [P, VP, VP]),
         "pgpu_solve_device": (C.c_int, [P, pastix_int_t, VP, pastix_int_t, VP]),

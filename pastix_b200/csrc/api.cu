@@ -27,6 +27,8 @@
 #include <string>
 #include <vector>
 
+#include <unistd.h>
+
 #include "../../include/pastix_b200.h"
 #include "device.cuh"
 #include "symbol.hpp"
@@ -298,6 +300,7 @@ struct pastix_data_s {
     GraphCache graphs;
     // GMRES refinement of several right-hand sides as one block (pgpu_refine_block)
     bool refine_block = true;
+    std::string dir_global;  // per-instance output directory of PastixIOSave (created on first save)
 };
 
 // Run one launch of kernel class `cls` with `count` blocks through `fn`, on
@@ -512,6 +515,216 @@ extern "C" void pastixFinalize(pastix_data_t **pd) {
 }
 
 // ---------------------------------------------------------------------------
+// Analysis files (IPARM_IO_STRATEGY).  The ordering and the block symbolic
+// matrix in the reference's plain-text formats, so that a file written by
+// either library loads in the other:
+//   ordering (order/order_io.c:44-120, 199-258): "1", cblknbr, vertnbr, then
+//     rangtab (cblknbr + 1), permtab (vertnbr), treetab (cblknbr; absent in
+//     version 0), whitespace separated, base = rangtab[0];
+//   symbol (symbol/symbol_io.c:51-180): "1", cblknbr, bloknbr, nodenbr,
+//     baseval, then fcolnum lcolnum bloknum per cblk and frownum lrownum
+//     fcblknm per blok.
+// Loads: the ordering from $PASTIX_FILE_ORDER or "ordername", the symbol from
+// "symbname" (pastix_subtask_order with a personal ordering,
+// pastix_subtask_symbfact); saves: "ordergen" (or $PASTIX_FILE_ORDER) and
+// "symbgen" in a directory "<$PASTIX_OUTPUT_DIR or pastix>-XXXXXX" created
+// once per instance (common/api.c:85-140).
+// ---------------------------------------------------------------------------
+static bool read_ints(FILE *f, idx_t *v, size_t count) {
+    for (size_t i = 0; i < count; i++) {
+        long long x;
+        if (fscanf(f, "%lld", &x) != 1) return false;
+        v[i] = (idx_t)x;
+    }
+    return true;
+}
+
+static int order_read(FILE *f, pgpu::Order &o) {
+    idx_t hdr[3];
+    if (!read_ints(f, hdr, 3) || (hdr[0] != 0 && hdr[0] != 1) || hdr[1] < 0 || hdr[2] < 1 || hdr[1] > hdr[2]) {
+        perr("pastixOrderLoad: bad header");
+        return PASTIX_ERR_FILE;
+    }
+    const idx_t cb = hdr[1], n = hdr[2];
+    o = pgpu::Order{};
+    o.n = n;
+    o.cblknbr = cb;
+    o.rangtab.resize(cb + 1);
+    o.permtab.resize(n);
+    if (!read_ints(f, o.rangtab.data(), cb + 1) || !read_ints(f, o.permtab.data(), n)) {
+        perr("pastixOrderLoad: truncated file");
+        return PASTIX_ERR_FILE;
+    }
+    if (hdr[0] == 1) {
+        o.treetab.resize(cb);
+        if (!read_ints(f, o.treetab.data(), cb)) {
+            perr("pastixOrderLoad: truncated file");
+            return PASTIX_ERR_FILE;
+        }
+    }
+    const idx_t base = o.rangtab[0];
+    for (auto &v : o.rangtab) v -= base;
+    for (auto &v : o.permtab) v -= base;
+    for (auto &v : o.treetab) v = v < 0 ? -1 : v - base;
+    if (o.rangtab[cb] != n) {
+        perr("pastixOrderLoad: rangtab does not cover the %lld vertices", (long long)n);
+        return PASTIX_ERR_FILE;
+    }
+    o.peritab.assign(n, -1);
+    for (idx_t i = 0; i < n; i++) {
+        if (o.permtab[i] < 0 || o.permtab[i] >= n || o.peritab[o.permtab[i]] >= 0) {
+            perr("pastixOrderLoad: permtab is not a permutation");
+            return PASTIX_ERR_FILE;
+        }
+        o.peritab[o.permtab[i]] = i;
+    }
+    if (o.treetab.empty()) {  // version 0 (no elimination tree): supernodes found again from the graph
+        o.rangtab.clear();
+        o.cblknbr = 0;
+    }
+    return PASTIX_SUCCESS;
+}
+
+// Integers 8 to a line, tab separated (intSave / putc of order/order_io.c).
+static void write_ints(FILE *f, const idx_t *v, size_t count) {
+    for (size_t i = 0; i < count; i++) fprintf(f, "%lld%c", (long long)v[i], (i % 8 == 7 || i + 1 == count) ? '\n' : '\t');
+}
+
+static int order_write(FILE *f, const pgpu::Order &o) {
+    if (o.rangtab.empty() || o.treetab.empty() || (idx_t)o.permtab.size() != o.n) {
+        perr("pastixOrderSave: the ordering needs permtab, rangtab and treetab");
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    fprintf(f, "1\n%lld\t%lld\n", (long long)o.cblknbr, (long long)o.n);
+    write_ints(f, o.rangtab.data(), o.cblknbr + 1);
+    write_ints(f, o.permtab.data(), o.n);
+    write_ints(f, o.treetab.data(), o.cblknbr);
+    return ferror(f) ? PASTIX_ERR_FILE : PASTIX_SUCCESS;
+}
+
+static int symbol_read(FILE *f, pgpu::Symbol &sy) {
+    idx_t hdr[5];
+    if (!read_ints(f, hdr, 5) || hdr[0] < 0 || hdr[0] > 1 || hdr[1] < 1 || hdr[2] < hdr[1] || hdr[3] < hdr[1]) {
+        perr("symbol file: bad header");
+        return PASTIX_ERR_FILE;
+    }
+    const idx_t cb = hdr[1], bk = hdr[2], b = hdr[4];
+    sy = pgpu::Symbol{};
+    sy.nodenbr = hdr[3];
+    sy.cblktab.resize(cb + 1);
+    sy.bloktab.resize(bk);
+    for (idx_t k = 0; k < cb; k++) {
+        idx_t v[3];
+        if (!read_ints(f, v, 3) || v[0] > v[1]) { perr("symbol file: bad cblk %lld", (long long)k); return PASTIX_ERR_FILE; }
+        sy.cblktab[k] = pgpu::SymCblk{v[0] - b, v[1] - b, v[2] - b};
+    }
+    sy.cblktab[cb] = pgpu::SymCblk{sy.nodenbr, sy.nodenbr, bk};
+    for (idx_t k = 0; k < cb; k++)
+        if (sy.cblktab[k].bloknum < 0 || sy.cblktab[k].bloknum >= sy.cblktab[k + 1].bloknum) {
+            perr("symbol file: bloknum of cblk %lld out of order", (long long)k);
+            return PASTIX_ERR_FILE;
+        }
+    for (idx_t i = 0; i < bk; i++) {
+        idx_t v[3];
+        if (!read_ints(f, v, 3) || v[0] > v[1] || v[2] - b < 0 || v[2] - b >= cb) {
+            perr("symbol file: bad blok %lld", (long long)i);
+            return PASTIX_ERR_FILE;
+        }
+        sy.bloktab[i] = pgpu::SymBlok{v[0] - b, v[1] - b, 0, v[2] - b};
+    }
+    for (idx_t k = 0; k < cb; k++)  // owning cblk of every blok
+        for (idx_t i = sy.cblktab[k].bloknum; i < sy.cblktab[k + 1].bloknum; i++) sy.bloktab[i].lcblknm = k;
+    return PASTIX_SUCCESS;
+}
+
+static int symbol_write(FILE *f, const pgpu::Symbol &sy) {
+    fprintf(f, "1\n%lld\t%lld\t%lld\t%lld\n", (long long)sy.cblknbr(), (long long)sy.bloknbr(), (long long)sy.nodenbr,
+            0LL);
+    for (idx_t k = 0; k < sy.cblknbr(); k++)
+        fprintf(f, "%lld\t%lld\t%lld\n", (long long)sy.cblktab[k].fcolnum, (long long)sy.cblktab[k].lcolnum,
+                (long long)sy.cblktab[k].bloknum);
+    for (const auto &bl : sy.bloktab)
+        fprintf(f, "%lld\t%lld\t%lld\n", (long long)bl.frownum, (long long)bl.lrownum, (long long)bl.fcblknm);
+    return ferror(f) ? PASTIX_ERR_FILE : PASTIX_SUCCESS;
+}
+
+// "<$PASTIX_OUTPUT_DIR or pastix>-XXXXXX", created on first use (pastix_gendirectories).
+static const char *output_dir(pastix_data_t *pd) {
+    if (pd->dir_global.empty()) {
+        const char *pre = getenv("PASTIX_OUTPUT_DIR");
+        std::string tmpl = std::string(pre && *pre ? pre : "pastix") + "-XXXXXX";
+        std::vector<char> buf(tmpl.begin(), tmpl.end());
+        buf.push_back('\0');
+        if (!mkdtemp(buf.data())) {
+            perr("cannot create the output directory %s", tmpl.c_str());
+            return nullptr;
+        }
+        pd->dir_global = buf.data();
+    }
+    return pd->dir_global.c_str();
+}
+
+static int order_save_file(pastix_data_t *pd, const pgpu::Order &o) {
+    const char *dir = output_dir(pd);
+    if (!dir) return PASTIX_ERR_FILE;
+    const char *env = getenv("PASTIX_FILE_ORDER");
+    const std::string path = std::string(dir) + "/" + (env && *env ? env : "ordergen");
+    FILE *f = fopen(path.c_str(), "w");
+    if (!f) { perr("cannot write %s", path.c_str()); return PASTIX_ERR_FILE; }
+    int rc = order_write(f, o);
+    if (fclose(f) != 0 && rc == PASTIX_SUCCESS) rc = PASTIX_ERR_FILE;
+    return rc;
+}
+
+static int order_load_file(pgpu::Order &o) {
+    const char *env = getenv("PASTIX_FILE_ORDER");
+    const char *path = env && *env ? env : "ordername";
+    FILE *f = fopen(path, "r");
+    if (!f) { perr("pastixOrderLoad: cannot open %s", path); return PASTIX_ERR_FILE; }
+    int rc = order_read(f, o);
+    fclose(f);
+    return rc;
+}
+
+// pastixOrderLoad (order/order_io.c:132): the ordering file of $PASTIX_FILE_ORDER
+// or "ordername" into *ordemesh (arrays allocated here, freed by pastixOrderExit).
+extern "C" int pastixOrderLoad(const pastix_data_t *, pastix_order_t *ordemesh) {
+    if (!ordemesh) return PASTIX_ERR_BADPARAMETER;
+    pgpu::Order o;
+    int rc = order_load_file(o);
+    if (rc) return rc;
+    memset(ordemesh, 0, sizeof(*ordemesh));
+    auto dup = [](const std::vector<idx_t> &v) {
+        pastix_int_t *p = (pastix_int_t *)malloc(std::max<size_t>(1, v.size()) * sizeof(pastix_int_t));
+        if (!v.empty()) memcpy(p, v.data(), v.size() * sizeof(pastix_int_t));
+        return p;
+    };
+    ordemesh->baseval = 0;
+    ordemesh->vertnbr = o.n;
+    ordemesh->cblknbr = o.cblknbr;
+    ordemesh->permtab = dup(o.permtab);
+    ordemesh->peritab = dup(o.peritab);
+    ordemesh->rangtab = o.rangtab.empty() ? nullptr : dup(o.rangtab);
+    ordemesh->treetab = o.treetab.empty() ? nullptr : dup(o.treetab);
+    return PASTIX_SUCCESS;
+}
+
+// pastixOrderSave (order/order_io.c:296): *ordemesh to "<output dir>/ordergen"
+// (or $PASTIX_FILE_ORDER).
+extern "C" int pastixOrderSave(pastix_data_t *pd, const pastix_order_t *ordemesh) {
+    if (!pd || !ordemesh || !ordemesh->permtab || !ordemesh->rangtab || !ordemesh->treetab || ordemesh->vertnbr < 1)
+        return PASTIX_ERR_BADPARAMETER;
+    pgpu::Order o;
+    const idx_t b = ordemesh->baseval;
+    o.n = ordemesh->vertnbr;
+    o.cblknbr = ordemesh->cblknbr;
+    for (idx_t i = 0; i < o.n; i++) o.permtab.push_back(ordemesh->permtab[i] - b);
+    for (idx_t k = 0; k <= o.cblknbr; k++) o.rangtab.push_back(ordemesh->rangtab[k] - b);
+    for (idx_t k = 0; k < o.cblknbr; k++) o.treetab.push_back(ordemesh->treetab[k] < 0 ? -1 : ordemesh->treetab[k] - b);
+    return order_save_file(pd, o);
+}
+
+// ---------------------------------------------------------------------------
 // ordering
 // ---------------------------------------------------------------------------
 extern "C" int pastixOrderGrid(pastix_order_t **myorder, pastix_int_t nx, pastix_int_t ny, pastix_int_t nz) {
@@ -617,7 +830,17 @@ extern "C" int pastix_subtask_order(pastix_data_t *pd, const spmatrix_t *spm, pa
     }
     pgpu::Order &o = pd->order;
     o = pgpu::Order{};
-    if (pd->iparm[IPARM_ORDERING] == PastixOrderPersonal && myorder && myorder->permtab) {
+    const bool personal = pd->iparm[IPARM_ORDERING] == PastixOrderPersonal;
+    if (personal && (pd->iparm[IPARM_IO_STRATEGY] & PastixIOLoad)) {
+        // the ordering file replaces the personal ordering (order/order_compute_personal.c:71-77)
+        rc = order_load_file(o);
+        if (rc) return rc;
+        if (o.n != n) {
+            if (n % o.n != 0) { perr("loaded ordering size mismatch"); return PASTIX_ERR_BADPARAMETER; }
+            pgpu::order_expand_dof(o, n / o.n);  // node ordering of a dof > 1 matrix
+        }
+        pd->user_order = true;
+    } else if (personal && myorder && myorder->permtab) {
         idx_t vn = myorder->vertnbr, ob = myorder->baseval;
         if (vn <= 0 || n % vn != 0) { perr("personal order size mismatch"); return PASTIX_ERR_BADPARAMETER; }
         o.n = vn;
@@ -648,6 +871,10 @@ extern "C" int pastix_subtask_order(pastix_data_t *pd, const spmatrix_t *spm, pa
     if (o.rangtab.empty()) pgpu::order_find_supernodes(o, pd->graph);
     std::string err = pgpu::order_check(o);
     if (!err.empty()) { perr("ordering check failed: %s", err.c_str()); return PASTIX_ERR_BADPARAMETER; }
+    if (pd->iparm[IPARM_IO_STRATEGY] & PastixIOSave) {  // order/pastix_subtask_order.c:485
+        rc = order_save_file(pd, o);
+        if (rc) return rc;
+    }
     pd->steps = STEP_INIT | STEP_ORDERING;
     return PASTIX_SUCCESS;
 }
@@ -658,7 +885,30 @@ extern "C" int pastix_subtask_symbfact(pastix_data_t *pd) {
         return PASTIX_ERR_BADPARAMETER;
     }
     double t0 = now_s();
-    pgpu::symbol_fax(pd->symbol, pd->graph, pd->order);
+    if (pd->iparm[IPARM_IO_STRATEGY] & PastixIOLoad) {  // symbol/pastix_subtask_symbfact.c:156-163
+        FILE *f = fopen("symbname", "r");
+        if (!f) { perr("pastix_subtask_symbfact: cannot open symbname"); return PASTIX_ERR_FILE; }
+        int rc = symbol_read(f, pd->symbol);
+        fclose(f);
+        if (rc) return rc;
+        if (pd->symbol.nodenbr != pd->order.n) {
+            perr("pastix_subtask_symbfact: the symbol file has %lld columns, the matrix %lld",
+                 (long long)pd->symbol.nodenbr, (long long)pd->order.n);
+            return PASTIX_ERR_BADPARAMETER;
+        }
+    } else {
+        pgpu::symbol_fax(pd->symbol, pd->graph, pd->order);
+    }
+    if (pd->iparm[IPARM_IO_STRATEGY] & PastixIOSave) {  // symbol/pastix_subtask_symbfact.c:275-285
+        const char *dir = output_dir(pd);
+        if (!dir) return PASTIX_ERR_FILE;
+        const std::string path = std::string(dir) + "/symbgen";
+        FILE *f = fopen(path.c_str(), "w");
+        if (!f) { perr("cannot write %s", path.c_str()); return PASTIX_ERR_FILE; }
+        int rc = symbol_write(f, pd->symbol);
+        if (fclose(f) != 0 && rc == PASTIX_SUCCESS) rc = PASTIX_ERR_FILE;
+        if (rc) return rc;
+    }
     pd->dparm[DPARM_SYMBFACT_TIME] = now_s() - t0;
     pd->steps |= STEP_SYMBFACT;
     return PASTIX_SUCCESS;

@@ -41,6 +41,10 @@ class factotype(IntEnum):
     LLH = 0; LDLT = 1; LU = 2; LLT = 3; LDLH = 4
 
 
+class io(IntEnum):
+    No = 0; Load = 1; Save = 2; LoadGraph = 4; SaveGraph = 8; LoadCSC = 16; SaveCSC = 32
+
+
 class refine(IntEnum):
     GMRES = 0; CG = 1; SR = 2; BiCGSTAB = 3
 
@@ -125,6 +129,20 @@ def orderGrid(nx: int, ny: int, nz: int):
     n, cb = o.vertnbr, o.cblknbr
     res = tuple(np.ctypeslib.as_array(a, shape=(s,)).copy()
                 for a, s in ((o.permtab, n), (o.peritab, n), (o.rangtab, cb + 1), (o.treetab, cb)))
+    lib.pastixOrderExit(C.byref(o))
+    return res
+
+
+def orderLoad(pd: Data = None):
+    """pastixOrderLoad: the ordering file ($PASTIX_FILE_ORDER or "ordername") as
+    (permtab, peritab, rangtab, treetab) numpy arrays (rangtab / treetab None
+    for a file without the elimination tree)."""
+    lib = _lib.load()
+    o = pastix_order_t()
+    _check("pastixOrderLoad", lib.pastixOrderLoad(pd.ptr if pd is not None else None, C.byref(o)))
+    n, cb = o.vertnbr, o.cblknbr
+    get = lambda a, s: np.ctypeslib.as_array(a, shape=(s,)).copy() if a else None  # noqa: E731
+    res = (get(o.permtab, n), get(o.peritab, n), get(o.rangtab, cb + 1), get(o.treetab, cb))
     lib.pastixOrderExit(C.byref(o))
     return res
 

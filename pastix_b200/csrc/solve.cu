@@ -140,6 +140,100 @@ __global__ void __launch_bounds__(256) k_bwd_diag(DevStruct s, const int *__rest
     }
 }
 
+// One right-hand side: one warp per narrow cblk (width <= 64, since
+// stride * width <= 4096), eight cblks per CTA -- the leaves of the tree are
+// tens of thousands of such cblks, and a CTA each left seven of its warps
+// idle.  y_k lives in two registers per lane (columns lane, 32 + lane); the
+// substitution steps are those of k_fwd_diag / k_bwd_diag.
+template <typename T>
+__device__ __forceinline__ T warp_fwd_block(const T *D, int st, int jb, int nb, int unit, int lane, T v) {
+    const T rd = (!unit && lane < nb) ? T(1) / D[(jb + lane) + (size_t)(jb + lane) * st] : T(1);
+    T drow[32];
+#pragma unroll
+    for (int c = 0; c < 32; c++) drow[c] = (c < lane && lane < nb) ? D[(jb + lane) + (size_t)(jb + c) * st] : T(0);
+#pragma unroll
+    for (int c = 0; c < 32; c++) {
+        if (c < nb) {
+            if (lane == c) v *= rd;
+            const T vc = __shfl_sync(0xffffffffu, v, c);
+            v -= drow[c] * vc;
+        }
+    }
+    return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_bwd_block(const T *D, int st, int jb, int nb, int unit, int lane, T v) {
+    const T rd = (!unit && lane < nb) ? T(1) / D[(jb + lane) + (size_t)(jb + lane) * st] : T(1);
+    T dcol[32];
+#pragma unroll
+    for (int c = 0; c < 32; c++) dcol[c] = (lane < c && c < nb) ? D[(jb + c) + (size_t)(jb + lane) * st] : T(0);
+#pragma unroll
+    for (int c = 31; c >= 0; c--) {
+        if (c < nb) {
+            if (lane == c) v *= rd;
+            const T vc = __shfl_sync(0xffffffffu, v, c);
+            v -= dcol[c] * vc;
+        }
+    }
+    return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwd_diag_w(DevStruct s, const int *__restrict__ list, int count, const T *P,
+                                                     int unit, T *Y) {
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (w >= count) return;  // whole warps
+    const int k = list[w];
+    const int fc = s.cb_fcol[k];
+    const int nc = s.cb_lcol[k] - fc + 1;
+    const int st = s.cb_stride[k];
+    const T *D = P + s.cb_coef[k];
+    T y0 = lane < nc ? Y[fc + lane] : T(0);
+    T y1 = 32 + lane < nc ? Y[fc + 32 + lane] : T(0);
+    y0 = warp_fwd_block<T>(D, st, 0, min(32, nc), unit, lane, y0);
+    if (nc > 32) {  // rows 32 .. nc - 1 of the diagonal block: y1 -= D[32 + lane, 0..31] y0
+        const int r = 32 + lane;
+        T acc = T(0);
+#pragma unroll
+        for (int c = 0; c < 32; c++) {
+            const T yc = __shfl_sync(0xffffffffu, y0, c);
+            if (r < nc) acc += D[r + (size_t)c * st] * yc;
+        }
+        y1 = warp_fwd_block<T>(D, st, 32, nc - 32, unit, lane, y1 - acc);
+    }
+    if (lane < nc) Y[fc + lane] = y0;
+    if (32 + lane < nc) Y[fc + 32 + lane] = y1;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_bwd_diag_w(DevStruct s, const int *__restrict__ list, int count, const T *P,
+                                                     int unit, T *Y) {
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (w >= count) return;
+    const int k = list[w];
+    const int fc = s.cb_fcol[k];
+    const int nc = s.cb_lcol[k] - fc + 1;
+    const int st = s.cb_stride[k];
+    const T *D = P + s.cb_coef[k];
+    T y0 = lane < nc ? Y[fc + lane] : T(0);
+    T y1 = 32 + lane < nc ? Y[fc + 32 + lane] : T(0);
+    if (nc > 32) {  // the last block first, then its contribution to rows 0..31: y0 -= D[32 + c, lane] y1[c]
+        y1 = warp_bwd_block<T>(D, st, 32, nc - 32, unit, lane, y1);
+        T acc = T(0);
+#pragma unroll
+        for (int c = 0; c < 32; c++) {
+            const T yc = __shfl_sync(0xffffffffu, y1, c);
+            if (32 + c < nc) acc += D[(32 + c) + (size_t)lane * st] * yc;
+        }
+        y0 -= acc;
+    }
+    y0 = warp_bwd_block<T>(D, st, 0, min(32, nc), unit, lane, y0);
+    if (lane < nc) Y[fc + lane] = y0;
+    if (32 + lane < nc) Y[fc + 32 + lane] = y1;
+}
+
 // ---------------------------------------------------------------------------
 // Wide cblks: blocked diagonal solves with the inverted 32 x 32 sub-blocks Z
 // (Z = T^{-1}, T the upper factor of the sub-block, see factor.cu):
@@ -713,6 +807,10 @@ template <typename T>
 void launch_fwd_diag(const DevStruct &s, const int *list, int count, int maxnc, const T *P, int unit, T *Y, int ldy,
                      int nrhs, cudaStream_t st) {
     if (count <= 0) return;
+    if (nrhs == 1) {  // narrow cblks (width <= 64): one warp each
+        k_fwd_diag_w<T><<<(count + 7) / 8, 256, 0, st>>>(s, list, count, P, unit, Y);
+        return;
+    }
     const int ZDIM = 1;
     PGPU_RC_DISPATCH(nrhs, k_fwd_diag, count, (size_t)maxnc * sizeof(T), s, list, P, unit, Y, ldy, nrhs);
 }
@@ -720,6 +818,10 @@ template <typename T>
 void launch_bwd_diag(const DevStruct &s, const int *list, int count, int maxnc, const T *P, int unit, T *Y, int ldy,
                      int nrhs, cudaStream_t st) {
     if (count <= 0) return;
+    if (nrhs == 1) {
+        k_bwd_diag_w<T><<<(count + 7) / 8, 256, 0, st>>>(s, list, count, P, unit, Y);
+        return;
+    }
     const int ZDIM = 1;
     PGPU_RC_DISPATCH(nrhs, k_bwd_diag, count, (size_t)maxnc * sizeof(T), s, list, P, unit, Y, ldy, nrhs);
 }

@@ -292,19 +292,24 @@ def run_b200(args, ws, rank, local):
                                   "berr_max": max(backward_error(Af, X16h[:, j], b16h[:, j]) for j in range(16))}
         if mode == "mixed":
             # e2e through the C ABI with host buffers
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            # (each step timed on its own; the median over the steps is reported, the
+            # host side of these calls shares the machine's cores with other jobs)
             xe = np.asfortranarray(b_h.copy())
             px.task_numfact(pd, S)  # warm
             torch.cuda.synchronize()
-            e0.record(stream)
-            for _ in range(max(1, min(args.steps, 3))):
+            te = []
+            for _ in range(max(3, args.steps)):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
                 px.task_numfact(pd, S)
                 xe[:] = b_h
                 px.task_solve(pd, S, xe)
                 px.task_refine(pd, S, b_h, xe)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            results[mode]["e2e"] = e0.elapsed_time(e1) / 1e3 / max(1, min(args.steps, 3))
+                e1.record(stream)
+                torch.cuda.synchronize()
+                te.append(e0.elapsed_time(e1) / 1e3)
+            results[mode]["e2e"] = float(np.median(te))
+            results[mode]["e2e_steps"] = te
             results[mode]["e2e_berr"] = backward_error(Af, xe, b_h)
             results[mode]["h2d"] = 8 * S.nnz + 8 * n + 2 * 8 * n
             results[mode]["d2h"] = 8 * n + 8 * n
@@ -681,7 +686,8 @@ def main():
         "clocks": mixed["clocks"],
         "gpu_launches": int(res[best]["launches"]),
         "e2e": {"value": mixed["e2e"], "unit": "s", "h2d_bytes_per_step": mixed["h2d"],
-                "d2h_bytes_per_step": mixed["d2h"], "berr": mixed["e2e_berr"]},
+                "d2h_bytes_per_step": mixed["d2h"], "berr": mixed["e2e_berr"], "statistic": "median",
+                "steps_s": mixed["e2e_steps"]},
     }
     hbm = peaks.get("hbm_gbs") or 6650.0
     hbm_src = "measured copy (MEASURED_PEAKS.json)" if peaks.get("hbm_gbs") else "fallback 6650 GB/s"

@@ -109,6 +109,18 @@ def dist_setup():
     return ws, rank, local
 
 
+def max_over_ranks(t: float, ws: int, device: str = "cuda") -> float:
+    """The slowest rank's time (replicas: the whole job ends when the last
+    rank does); every rank takes part and receives it."""
+    if ws <= 1:
+        return t
+    import torch
+    import torch.distributed as dist
+    tt = torch.tensor([t], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
 def fp64_peak_tflops(torch) -> float:
     """cuBLAS DGEMM throughput measured in this run (the FP64 roofline denominator)."""
     n = 8192
@@ -252,10 +264,7 @@ def run_b200(args, ws, rank, local):
         t = e0.elapsed_time(e1) / 1e3 / args.steps
         launches = sum(v[1] for v in px.profile_get(pd).values())
         clocks = sampler.stop() if sampler else None
-        if ws > 1:
-            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-            t = float(tt.item())
+        t = max_over_ranks(t, ws)
         xh = x.cpu().numpy()
         berr = backward_error(Af, xh, b_h)
         results[mode] = dict(t=t, berr=berr, fwd=float(np.linalg.norm(xh - xt) / np.linalg.norm(xt)),

@@ -679,31 +679,32 @@ __global__ void __launch_bounds__(256) k_fwd_update(DevStruct s, const RowTile *
     const int j0 = blockIdx.y * RC;
     const int nr = min(RC, nrhs - j0);
     const int tid = threadIdx.x;
+    const int r = tid % ST_R, g = tid / ST_R, cb = 16 * g;  // 4 column groups of 16
+    // the panel tile and the target rows do not depend on y_k: their loads are issued first and
+    // overlap the staging of y_k (one memory round trip per tile instead of three)
+    T p[16];
+    {
+        const T *Pr = P + s.cb_coef[k] + tl.r0 + r + (size_t)c0 * st;
+#pragma unroll
+        for (int u = 0; u < 16; u++) p[u] = (r < rows && cb + u < ncol) ? Pr[(size_t)(cb + u) * st] : T(0);
+    }
+    const int gr = (tid < ST_R && tid < rows) ? s.rowidx[s.cb_rowidx[k] + tl.r0 + tid] : 0;
     for (int e = tid; e < ST_C * RC; e += 256) {
         int c = e % ST_C, j = e / ST_C;
         yk[e] = (c < ncol && j < nr) ? Y[(fc + c0 + c) + (size_t)(j0 + j) * ldy] : T(0);
     }
     __syncthreads();
-    const int r = tid % ST_R, g = tid / ST_R;  // 4 column groups of 16
     T acc[RC];
 #pragma unroll
     for (int j = 0; j < RC; j++) acc[j] = T(0);
-    if (r < rows) {
-        const T *Pr = P + s.cb_coef[k] + tl.r0 + r + (size_t)c0 * st;
-        const int cb = g * 16;
-        T p[16];  // all 16 loads issued before the products
 #pragma unroll
-        for (int u = 0; u < 16; u++) p[u] = (cb + u < ncol) ? Pr[(size_t)(cb + u) * st] : T(0);
+    for (int u = 0; u < 16; u++)
 #pragma unroll
-        for (int u = 0; u < 16; u++)
-#pragma unroll
-            for (int j = 0; j < RC; j++) acc[j] += p[u] * yk[cb + u + j * ST_C];
-    }
+        for (int j = 0; j < RC; j++) acc[j] += p[u] * yk[cb + u + j * ST_C];
 #pragma unroll
     for (int j = 0; j < RC; j++) part[g][r + j * ST_R] = acc[j];
     __syncthreads();
     if (tid < ST_R && tid < rows) {
-        const int gr = s.rowidx[s.cb_rowidx[k] + tl.r0 + tid];
 #pragma unroll
         for (int j = 0; j < RC; j++) {
             if (j >= nr) break;
@@ -730,22 +731,24 @@ __global__ void __launch_bounds__(256) k_bwd_update(DevStruct s, const RowTile *
     const int nr = min(RC, nrhs - j0);
     const int tid = threadIdx.x;
     const int *ridx = s.rowidx + s.cb_rowidx[k] + tl.r0;
+    // thread (row r, 16-column group g): 16 independent coalesced loads of the
+    // panel tile, issued before the gather of x (which needs the row indices
+    // first), so that the two overlap
+    const T *Pk = P + s.cb_coef[k] + tl.r0 + (size_t)c0 * st;
+    const int r = tid % ST_R, g = tid / ST_R, cb = 16 * g;
+    T p[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) p[u] = (r < rows && cb + u < ncol) ? Pk[r + (size_t)(cb + u) * st] : T(0);
     for (int e = tid; e < ST_R * RC; e += 256) {
         int i = e % ST_R, j = e / ST_R;
         xr[e] = (i < rows && j < nr) ? Y[ridx[i] + (size_t)(j0 + j) * ldy] : T(0);
     }
     __syncthreads();
-    const T *Pk = P + s.cb_coef[k] + tl.r0 + (size_t)c0 * st;
     if constexpr (RC == 1) {
-        // thread (row r, 16-column group g): 16 independent coalesced loads, the
-        // products P[r, c] x[r] staged in shared memory (row stride 65: no bank
-        // conflicts on either side), then one thread per column sums its 64 rows
+        // the products P[r, c] x[r] staged in shared memory (row stride 65: no
+        // bank conflicts on either side), then one thread per column sums its 64 rows
         __shared__ T prod[ST_C * (ST_R + 1)];
-        const int r = tid % ST_R, g = tid / ST_R, cb = 16 * g;
         const T xv = xr[r];
-        T p[16];
-#pragma unroll
-        for (int u = 0; u < 16; u++) p[u] = (r < rows && cb + u < ncol) ? Pk[r + (size_t)(cb + u) * st] : T(0);
 #pragma unroll
         for (int u = 0; u < 16; u++) prod[(cb + u) * (ST_R + 1) + r] = p[u] * xv;
         __syncthreads();
@@ -757,13 +760,9 @@ __global__ void __launch_bounds__(256) k_bwd_update(DevStruct s, const RowTile *
         }
         return;
     } else {
-        // out[c, j] = sum_r P[r, c] x[r, j]: the tile staged transposed in shared memory
-        // (16 independent coalesced loads per thread), then 64 columns x RC dot products
+        // out[c, j] = sum_r P[r, c] x[r, j]: the tile staged transposed in shared memory,
+        // then 64 columns x RC dot products
         __shared__ T pt[ST_C * (ST_R + 1)];
-        const int r = tid % ST_R, g = tid / ST_R, cb = 16 * g;
-        T p[16];
-#pragma unroll
-        for (int u = 0; u < 16; u++) p[u] = (r < rows && cb + u < ncol) ? Pk[r + (size_t)(cb + u) * st] : T(0);
 #pragma unroll
         for (int u = 0; u < 16; u++) pt[(cb + u) * (ST_R + 1) + r] = p[u];
         __syncthreads();

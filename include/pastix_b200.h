@@ -332,8 +332,10 @@ int pgpu_solve_refine_device(pastix_data_t *pastix_data, pastix_int_t nrhs, cons
  * event): make it before any stream capture.  The array is shared by every
  * pastix_data_t of the process on that device, so calls that overlap in time
  * (two host threads, or two streams without ordering between them) race on
- * it.  Not available while pgpu_profile timing is on.  Same arguments and
- * stream semantics as pgpu_solve_device (A X = B). */
+ * it.  Not available while pgpu_profile timing is on.  The set-up is cached
+ * per device for the life of the process; after a device reset a call fails
+ * once with PASTIX_ERR_INTERNAL and the next one redoes the set-up.  Same
+ * arguments and stream semantics as pgpu_solve_device (A X = B). */
 #define PGPU_STATIC_SOLVE_ELEMS 1048576
 int pgpu_solve_device_static(pastix_data_t *pastix_data, pastix_int_t nrhs, double *B, pastix_int_t ldb,
                              void *stream);

@@ -21,10 +21,6 @@ HERE = Path(__file__).resolve().parent
 LIB = HERE / "_build" / "liboracle.so"
 I64P = C.POINTER(C.c_int64)
 
-# OpenBLAS shipped in this image (opencv wheel); used only to time the CPU baseline
-OPENBLAS_CANDIDATES = [
-    "/opt/prime-rl/.venv/lib/python3.12/site-packages/opencv_python_headless.libs/libopenblasp-r0-59ffcd50.3.15.so",
-]
 
 
 class ora_symbol_t(C.Structure):
@@ -67,11 +63,10 @@ def use_blas(enable: bool = True) -> bool:
     if not enable:
         lib.ora_unload_blas()
         return False
-    for p in OPENBLAS_CANDIDATES + [os.environ.get("ORACLE_BLAS", "")]:
-        if not p or not Path(p).exists():
-            continue
+    from . import blas
+    for p in blas.candidates():
         # the wheel's OpenBLAS needs its bundled gfortran / quadmath, loaded globally first
-        for dep in sorted(Path(p).parent.glob("libquadmath*.so*")) + sorted(Path(p).parent.glob("libgfortran*.so*")):
+        for dep in blas.runtime_deps(p):
             try:
                 C.CDLL(str(dep), mode=C.RTLD_GLOBAL)
             except OSError:

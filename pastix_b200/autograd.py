@@ -7,6 +7,12 @@ LDL^T), ``grad_b = lambda``, and the value gradient ``-lambda_i x_j`` over the
 stored pattern from one sampled outer-product kernel (pgpu_sampled_outer); no
 refactorization.  Only float64 CUDA tensors are accepted: the library has no
 CPU path.
+
+A solver holds one set of factors.  Each factorization bumps
+``SparseSolver.version``; a forward records the version it solved with, and
+its backward refactorizes from the values it saved when another forward has
+replaced the factors in between, so the gradient always belongs to the
+matrix of its own forward.
 """
 from __future__ import annotations
 
@@ -42,7 +48,8 @@ class SparseSolver:
             px.task_analyze(self.pd, self.spm)
         self.n = self.spm.n
         self.nnz = self.spm.nnz
-        self._factored_version = None
+        self.version = 0  # bumped by every factorization
+
 
     def factorize(self, values: torch.Tensor) -> None:
         _check_cuda(values)
@@ -50,6 +57,7 @@ class SparseSolver:
             raise ValueError(f"values has {values.numel()} entries, the pattern {self.nnz}")
         torch.cuda.current_stream().synchronize()
         px.numfact_device(self.pd, values.contiguous())
+        self.version += 1
 
     def solve(self, b: torch.Tensor, transposed: bool = False) -> torch.Tensor:
         """Device solve with the current factors (no autograd)."""
@@ -88,13 +96,17 @@ class _Solve(torch.autograd.Function):
         solver.factorize(values.detach())
         x = solver.solve(b.detach())
         ctx.solver = solver
-        ctx.save_for_backward(x)
+        ctx.version = solver.version
+        ctx.save_for_backward(x, values.detach())
         return x
 
     @staticmethod
     def backward(ctx, gx):
-        (x,) = ctx.saved_tensors
+        x, values = ctx.saved_tensors
         solver: SparseSolver = ctx.solver
+        if solver.version != ctx.version:
+            # another forward factorized different values since: restore ours
+            solver.factorize(values)
         gx = gx.contiguous()
         lam = solver.solve(gx, transposed=True)
         gvals = None

@@ -578,10 +578,8 @@ static int order_read(FILE *f, pgpu::Order &o) {
         }
         o.peritab[o.permtab[i]] = i;
     }
-    if (o.treetab.empty()) {  // version 0 (no elimination tree): supernodes found again from the graph
-        o.rangtab.clear();
-        o.cblknbr = 0;
-    }
+    // version 0 keeps rangtab without treetab (order/order_io.c:80-85); the
+    // ordering step finds the supernodes again when it needs a tree
     return PASTIX_SUCCESS;
 }
 
@@ -868,7 +866,12 @@ extern "C" int pastix_subtask_order(pastix_data_t *pd, const spmatrix_t *spm, pa
         pgpu::order_nd_graph(o, pd->graph);
         pd->user_order = false;
     }
-    if (o.rangtab.empty()) pgpu::order_find_supernodes(o, pd->graph);
+    if (o.rangtab.empty() || o.treetab.empty()) {  // order/pastix_subtask_order.c:360-364
+        o.rangtab.clear();
+        o.treetab.clear();
+        o.cblknbr = 0;
+        pgpu::order_find_supernodes(o, pd->graph);
+    }
     std::string err = pgpu::order_check(o);
     if (!err.empty()) { perr("ordering check failed: %s", err.c_str()); return PASTIX_ERR_BADPARAMETER; }
     if (pd->iparm[IPARM_IO_STRATEGY] & PastixIOSave) {  // order/pastix_subtask_order.c:485
@@ -891,6 +894,12 @@ extern "C" int pastix_subtask_symbfact(pastix_data_t *pd) {
         int rc = symbol_read(f, pd->symbol);
         fclose(f);
         if (rc) return rc;
+        // structural checks before anything walks the loaded structure
+        std::string err = pgpu::symbol_check(pd->symbol);
+        if (!err.empty()) {
+            perr("pastix_subtask_symbfact: symbol file fails its checks: %s", err.c_str());
+            return PASTIX_ERR_FILE;
+        }
         if (pd->symbol.nodenbr != pd->order.n) {
             perr("pastix_subtask_symbfact: the symbol file has %lld columns, the matrix %lld",
                  (long long)pd->symbol.nodenbr, (long long)pd->order.n);
@@ -2989,7 +2998,14 @@ extern "C" int pgpu_solve_device_static(pastix_data_t *pd, pastix_int_t nrhs, do
     const idx_t n = pd->n;
     cudaStream_t user = (cudaStream_t)stream;
     if (user != d.stream) {
-        CUDA_TRY(cudaEventRecord(slot->ev, user));
+        if (cudaEventRecord(slot->ev, user) != cudaSuccess) {
+            // the cached event (and symbol address) belong to a context that is
+            // gone, e.g. after a device reset: redo the set-up on the next call
+            std::lock_guard<std::mutex> lock(g_static_mutex);
+            slot->ready = false;
+            perr("pgpu_solve_device_static: ordering event unusable (device reset?)");
+            return PASTIX_ERR_INTERNAL;
+        }
         CUDA_TRY(cudaStreamWaitEvent(d.stream, slot->ev, 0));
     }
     pgpu::launch_permute<double, double>((int)n, (int)nrhs, d.perm.p, 1, B, ldb, Y, n, d.stream);

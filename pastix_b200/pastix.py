@@ -135,8 +135,8 @@ def orderGrid(nx: int, ny: int, nz: int):
 
 def orderLoad(pd: Data = None):
     """pastixOrderLoad: the ordering file ($PASTIX_FILE_ORDER or "ordername") as
-    (permtab, peritab, rangtab, treetab) numpy arrays (rangtab / treetab None
-    for a file without the elimination tree)."""
+    (permtab, peritab, rangtab, treetab) numpy arrays (treetab None for a
+    version-0 file, which has no elimination tree)."""
     lib = _lib.load()
     o = pastix_order_t()
     _check("pastixOrderLoad", lib.pastixOrderLoad(pd.ptr if pd is not None else None, C.byref(o)))

@@ -4,7 +4,9 @@ entry points fail loudly without a GPU (no CPU fallback)."""
 from __future__ import annotations
 
 import ctypes as C
+import os
 import re
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -123,3 +125,47 @@ def test_tuning_rejects_bad_values(lib):
     assert px.get_tuning(pd) == (32, 32, 32)
     px.set_tuning(pd, 16, 16, 48)  # rebuilds the launch lists on the host
     assert px.get_tuning(pd) == (16, 16, 48)
+
+
+def _enum_values(text, name):
+    """{member: value} of `typedef enum <name> {...}`, implicit values counted."""
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", "", text)
+    m = re.search(r"typedef enum %s \{(.*?)\}" % name, text, re.S)
+    if m is None:
+        return None
+    out, nxt = {}, 0
+    for item in m.group(1).split(","):
+        item = item.strip()
+        if not item:
+            continue
+        if "=" in item:
+            k, v = (x.strip() for x in item.split("=", 1))
+            nxt = int(v, 0) if re.fullmatch(r"-?(0x)?[0-9a-fA-F]+", v) else out[v]
+        else:
+            k = item
+        out[k] = nxt
+        nxt += 1
+    return out
+
+
+# the reference source tree, where this machine has one
+REF_API = Path(os.environ.get("PASTIX_SOURCE_DIR", "/root/reference")) / "include" / "pastix" / "api.h"
+
+
+@pytest.mark.skipif(not REF_API.exists(), reason="the reference source tree is not on this machine")
+def test_enums_match_the_reference_header():
+    """Every enumeration this header restates has the reference's members and
+    values (include/pastix/api.h); iparm / dparm are indices into the users'
+    arrays, so a shifted member would silently change a parameter."""
+    ours = HEADER.read_text()
+    ref = REF_API.read_text()
+    names = re.findall(r"typedef enum (pastix_\w+_e)", re.sub(r"/\*.*?\*/", "", ours, flags=re.S))
+    assert "pastix_iparm_e" in names and "pastix_dparm_e" in names
+    for name in names:
+        r = _enum_values(ref, name)
+        assert r is not None, name
+        o = _enum_values(ours, name)
+        assert o == {k: v for k, v in r.items() if k in o}, name
+        if name in ("pastix_iparm_e", "pastix_dparm_e", "pastix_error_e"):
+            assert o == r, name

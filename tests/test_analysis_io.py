@@ -77,7 +77,9 @@ def test_order_load_reference_format(lib, tmp_path, monkeypatch):
     perm, peri, rang, tree = px.orderLoad()
     assert perm.tolist() == [2, 0, 4, 1, 3]
     assert peri.tolist() == [1, 3, 0, 4, 2]
-    assert rang is None and tree is None  # supernodes are recomputed from the graph when used
+    # the supernode partition is kept as read (order/order_io.c:80-85), only the tree is absent
+    assert rang.tolist() == [0, 3, 5]
+    assert tree is None
 
 
 def test_load_rejects_a_bad_file(lib, tmp_path, monkeypatch):
@@ -89,5 +91,38 @@ def test_load_rejects_a_bad_file(lib, tmp_path, monkeypatch):
     ip[px.iparm.ordering] = int(px.ordering.Personal)
     pd = px.init(ip, dp)
     S = spmatrix(gen.laplacian7(2, 2, 1), mtxtype.Symmetric)
+    rc = lib.pastix_task_analyze(pd.ptr, S.pointer())
+    assert rc == px.error.FILE
+
+
+def test_load_rejects_a_corrupted_symbol(lib, tmp_path, monkeypatch):
+    """A symbol file whose blok faces an earlier cblk is refused with
+    PASTIX_ERR_FILE before the supernode split walks it."""
+    A = gen.laplacian7(5, 4, 3)
+    monkeypatch.setenv("PASTIX_OUTPUT_DIR", str(tmp_path / "pastix"))
+    monkeypatch.delenv("PASTIX_FILE_ORDER", raising=False)
+    _analyze(A, io=px.io.Save)
+    d = glob.glob(str(tmp_path / "pastix-*"))[0]
+    symb = _ints(os.path.join(d, "symbgen"))
+    cb, bk = symb[1], symb[2]
+    cbt = np.array(symb[5:5 + 3 * cb]).reshape(cb, 3)
+    bkt = np.array(symb[5 + 3 * cb:]).reshape(bk, 3)
+    # first off-diagonal blok of the last cblk that has one: make it face cblk 0
+    for k in range(cb - 1, -1, -1):
+        lb = cbt[k + 1, 2] if k + 1 < cb else bk
+        if lb - cbt[k, 2] > 1:
+            bkt[cbt[k, 2] + 1, 2] = 0
+            break
+    else:
+        raise AssertionError("no off-diagonal blok")
+    vals = symb[:5] + cbt.ravel().tolist() + bkt.ravel().tolist()
+    (tmp_path / "symbname").write_text("\n".join(str(v) for v in vals) + "\n")
+    monkeypatch.setenv("PASTIX_FILE_ORDER", os.path.join(d, "ordergen"))
+    monkeypatch.chdir(tmp_path)
+    ip, dp = px.initParam()
+    ip[px.iparm.io_strategy] = int(px.io.Load)
+    ip[px.iparm.ordering] = int(px.ordering.Personal)
+    pd = px.init(ip, dp)
+    S = spmatrix(A, mtxtype.Symmetric)
     rc = lib.pastix_task_analyze(pd.ptr, S.pointer())
     assert rc == px.error.FILE

@@ -86,3 +86,22 @@ def test_adjoint_vs_cpu_solves(lib, oracle_mod, name, fact):
         gvals[off] -= lam[S.col[off]] * xc[S.row[off]]
     assert np.linalg.norm(bb.grad.cpu().numpy() - lam) <= 1e-10 * np.linalg.norm(lam)
     assert np.linalg.norm(v.grad.cpu().numpy() - gvals) <= 1e-10 * np.linalg.norm(gvals)
+
+
+def test_backward_after_another_forward(lib):
+    """Two forwards with different values on one solver, then the first
+    backward: its gradient must be the one of its own matrix."""
+    A, solver, vals, b, x_obs = _setup("grf512", "POTRF")
+    v1 = vals.clone().requires_grad_(True)
+    loss1, _ = _loss(solver, v1, b, x_obs)
+    loss1.backward()
+    g_ref = v1.grad.clone()
+
+    v1 = vals.clone().requires_grad_(True)
+    loss1, _ = _loss(solver, v1, b, x_obs)
+    v2 = (vals * 1.5).requires_grad_(True)
+    loss2, _ = _loss(solver, v2, b, x_obs)  # replaces the resident factors
+    loss1.backward()
+    assert torch.linalg.norm(v1.grad - g_ref) <= 1e-12 * torch.linalg.norm(g_ref)
+    loss2.backward()
+    assert torch.linalg.norm(v2.grad - g_ref) > 1e-3 * torch.linalg.norm(g_ref)

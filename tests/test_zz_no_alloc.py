@@ -1,5 +1,6 @@
 """pgpu_solve_device_static (the solve that allocates nothing) against
-pgpu_solve_device, through the C ABI, on two calls in a row."""
+pgpu_solve_device, through the C ABI, on two calls in a row, with device
+free memory unchanged across the calls that follow the first."""
 from __future__ import annotations
 
 import ctypes as C
@@ -39,10 +40,21 @@ def test_static_solve_matches(lib, fact, mixed):
     n = A.shape[0]
     g = torch.Generator(device="cuda").manual_seed(7)
     B = torch.rand(n, 3, dtype=torch.float64, device="cuda", generator=g) - 0.5
+    # the static solve runs first on this freshly factorized instance, so the
+    # work areas of pgpu_solve_device do not exist yet; after the first call
+    # (the per-device set-up) device memory must not change
+    X0 = _solve(l.pgpu_solve_device_static, pd, B)
+    Xs = [B.clone().t().contiguous().t() for _ in range(2)]
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for X in Xs:
+        rc = l.pgpu_solve_device_static(pd.ptr, X.shape[1], C.c_void_p(X.data_ptr()), n,
+                                        C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert rc == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
     ref = _solve(l.pgpu_solve_device, pd, B)
-    for _ in range(2):
-        X = _solve(l.pgpu_solve_device_static, pd, B)
-        torch.cuda.synchronize()
+    for X in [X0] + Xs:
         err = torch.linalg.norm(X - ref) / torch.linalg.norm(ref)
         assert err.item() <= TOL[mixed], err.item()
     assert l.pgpu_device_status(pd.ptr) == 0

@@ -71,7 +71,7 @@ def use_blas(enable: bool = True) -> bool:
                 C.CDLL(str(dep), mode=C.RTLD_GLOBAL)
             except OSError:
                 pass
-        if lib.ora_load_blas(p.encode()) == 0:
+        if lib.ora_load_blas(str(p).encode()) == 0:
             return True
     return False
 

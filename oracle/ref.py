@@ -108,6 +108,30 @@ def symmetric_pattern(A) -> sps.csc_matrix:
     return B
 
 
+def node_matrix(A, dof: int, lower: bool):
+    """Scalar matrix A (dof unknowns per node, unknown v*dof+d of node v) as the
+    SpM descriptor of a dof > 1 matrix: node CSC pattern, and per stored node
+    pair (I, J) its dof x dof block A[I*dof:, J*dof:] column-major, as
+    bcsc/bcsc_zinit.c reads it.  lower: keep the node pairs I >= J only."""
+    T = sps.coo_matrix(A)
+    n = A.shape[0] // dof
+    r, c = T.row.astype(np.int64), T.col.astype(np.int64)
+    P = sps.coo_matrix((np.ones(T.nnz), (r // dof, c // dof)), shape=(n, n)).tocsc()
+    P.sum_duplicates()
+    if lower:
+        P = sps.tril(P, format="csc")
+    P.sort_indices()
+    # entry e of P has key col * n + row; keys are sorted because P is sorted CSC
+    cols = np.repeat(np.arange(n, dtype=np.int64), np.diff(P.indptr))
+    keys = cols * n + P.indices.astype(np.int64)
+    sel = (r // dof >= c // dof) if lower else np.ones(T.nnz, dtype=bool)
+    k = (c[sel] // dof) * n + r[sel] // dof
+    e = np.searchsorted(keys, k)
+    vals = np.zeros(P.nnz * dof * dof)
+    vals[e * dof * dof + (c[sel] % dof) * dof + r[sel] % dof] = T.data[sel]
+    return P.indptr.astype(np.int64), P.indices.astype(np.int64), vals
+
+
 class RefPastix:
     """One instance of the reference solver on one matrix.
 
@@ -136,18 +160,22 @@ class RefPastix:
             raise RuntimeError(f"pastixInit failed ({rc})")
         A = sps.csc_matrix(A, dtype=np.float64)
         A.sum_duplicates()
-        if fact == "GETRF":
-            A = symmetric_pattern(A)
-            mtx = 111
-        else:
-            A = sps.tril(A, format="csc")
-            mtx = 112
-        A.sort_indices()
-        self.A = A
+        mtx = 111 if fact == "GETRF" else 112
         self.n = A.shape[0]
-        self._cp, self._ri = _i64(A.indptr), _i64(A.indices)
-        self._va = np.ascontiguousarray(A.data, dtype=np.float64)
-        rc = self.lib.ref_set_matrix(self.h, C.c_int64(self.n), self._cp.ctypes.data_as(I64P),
+        if dof > 1:  # node descriptor with dof x dof blocks
+            cp, ri, va = node_matrix(symmetric_pattern(A) if fact == "GETRF" else A, dof, lower=fact != "GETRF")
+            self._cp, self._ri, self._va = _i64(cp), _i64(ri), np.ascontiguousarray(va)
+            nn = self.n // dof
+        else:
+            if fact == "GETRF":
+                A = symmetric_pattern(A)
+            else:
+                A = sps.tril(A, format="csc")
+            A.sort_indices()
+            self._cp, self._ri = _i64(A.indptr), _i64(A.indices)
+            self._va = np.ascontiguousarray(A.data, dtype=np.float64)
+            nn = self.n
+        rc = self.lib.ref_set_matrix(self.h, C.c_int64(nn), self._cp.ctypes.data_as(I64P),
                                      self._ri.ctypes.data_as(I64P), self._va.ctypes.data_as(DP),
                                      C.c_int(mtx), C.c_int64(dof))
         if rc:

@@ -110,6 +110,29 @@ void order_grid(Order &o, idx_t nx, idx_t ny, idx_t nz) {
     }
 }
 
+// Node graph of a matrix with dof unknowns per node (unknown v*dof+d belongs
+// to node v): two nodes are adjacent when any of their unknowns are.
+void graph_collapse(const Graph &g, idx_t dof, Graph &out) {
+    const idx_t nn = g.n / dof;
+    out.n = nn;
+    out.colptr.assign(nn + 1, 0);
+    out.rowind.clear();
+    std::vector<idx_t> mark(nn, -1), adj;
+    for (idx_t v = 0; v < nn; v++) {
+        adj.clear();
+        for (idx_t d = 0; d < dof; d++) {
+            idx_t i = v * dof + d;
+            for (idx_t e = g.colptr[i]; e < g.colptr[i + 1]; e++) {
+                idx_t w = g.rowind[e] / dof;
+                if (w != v && mark[w] != v) { mark[w] = v; adj.push_back(w); }
+            }
+        }
+        std::sort(adj.begin(), adj.end());
+        out.rowind.insert(out.rowind.end(), adj.begin(), adj.end());
+        out.colptr[v + 1] = (idx_t)out.rowind.size();
+    }
+}
+
 // Expand a node ordering to dof unknowns per node (pastixOrderExpand,
 // order/order.c): unknown v*dof+d of node v keeps node order, dof-major.
 void order_expand_dof(Order &o, idx_t dof) {
@@ -123,6 +146,260 @@ void order_expand_dof(Order &o, idx_t dof) {
     o.peritab.swap(peri);
     for (auto &r : o.rangtab) r *= dof;
     o.n = n * dof;
+}
+
+// ---------------------------------------------------------------------------
+// Supernodes renumbered level by level of the elimination tree
+// (orderApplyLevelOrder, order/order_apply_level_order.c:95-338).  The tree is
+// walked breadth first from the roots; the sons of a supernode are queued in
+// reverse index order, and the final numbering is the reverse of the queue,
+// so that the roots come last and every son precedes its father.  With
+// level2d < 0 (automatic 2D tasks), supernodes of at least width2d columns
+// whose father is a root or a 2D supernode with exactly two sons are "2D"
+// and are queued ahead of all the others, level by level as well.  Columns
+// keep their order inside each supernode.
+// ---------------------------------------------------------------------------
+void order_apply_level_order(Order &o, idx_t level2d, idx_t width2d) {
+    const idx_t cb = o.cblknbr;
+    if (cb <= 1) return;
+    // sons of every node in increasing index order; roots are the sons of -1
+    std::vector<idx_t> nsons(cb + 1, 0), first(cb + 2, 0), sons(cb);
+    for (idx_t k = 0; k < cb; k++) nsons[o.treetab[k] + 1]++;
+    for (idx_t f = 0; f <= cb; f++) first[f + 1] = first[f] + nsons[f];
+    {
+        std::vector<idx_t> pos(first.begin(), first.end() - 1);
+        for (idx_t k = 0; k < cb; k++) sons[pos[o.treetab[k] + 1]++] = k;
+    }
+    auto sons_of = [&](idx_t f) { return std::make_pair(first[f + 1], first[f + 2]); };  // f = -1 for roots
+    std::vector<idx_t> queue(cb), father(o.treetab);  // father becomes the new number of the father
+    if (level2d < 0) {
+        std::vector<char> is2d(cb, 0);
+        idx_t n2d = 0;
+        for (idx_t k = cb - 1; k >= 0; k--) {
+            idx_t f = o.treetab[k], size = o.rangtab[k + 1] - o.rangtab[k];
+            if (size >= width2d && (f == -1 || (is2d[f] && nsons[f + 1] == 2))) { is2d[k] = 1; n2d++; }
+        }
+        idx_t p2 = 0, p1 = n2d;
+        auto roots = sons_of(-1);
+        for (idx_t r = roots.first; r < roots.second; r++) {
+            idx_t k = sons[r];
+            if (is2d[k]) queue[p2++] = k; else queue[p1++] = k;
+        }
+        for (idx_t i = 0; i < cb; i++) {
+            idx_t node = queue[i];
+            auto sr = sons_of(node);
+            idx_t s2 = 0;
+            for (idx_t r = sr.first; r < sr.second; r++) s2 += is2d[sons[r]];
+            idx_t s1 = (sr.second - sr.first) - s2, c2 = 0, c1 = 0;
+            for (idx_t r = sr.first; r < sr.second; r++) {
+                idx_t son = sons[r];
+                if (is2d[son]) queue[p2 + s2 - 1 - c2++] = son;
+                else queue[p1 + s1 - 1 - c1++] = son;
+                father[son] = cb - 1 - i;
+            }
+            p2 += s2;
+            p1 += s1;
+        }
+    } else {
+        auto roots = sons_of(-1);
+        idx_t pos = roots.second - roots.first;
+        std::copy(sons.begin() + roots.first, sons.begin() + roots.second, queue.begin());
+        for (idx_t i = 0; i < cb; i++) {
+            idx_t node = queue[i];
+            auto sr = sons_of(node);
+            idx_t ns = sr.second - sr.first;
+            for (idx_t j = 0; j < ns; j++) {
+                idx_t son = sons[sr.first + j];
+                queue[pos + ns - 1 - j] = son;
+                father[son] = cb - 1 - i;
+            }
+            pos += ns;
+        }
+    }
+    std::vector<idx_t> rang(cb + 1, 0), tree(cb), peri(o.n);
+    for (idx_t i = 0; i < cb; i++) {
+        idx_t node = queue[cb - 1 - i];
+        idx_t size = o.rangtab[node + 1] - o.rangtab[node];
+        rang[i + 1] = rang[i] + size;
+        tree[i] = father[node];
+        std::copy(o.peritab.begin() + o.rangtab[node], o.peritab.begin() + o.rangtab[node + 1], peri.begin() + rang[i]);
+    }
+    o.rangtab.swap(rang);
+    o.treetab.swap(tree);
+    o.peritab.swap(peri);
+    for (idx_t i = 0; i < o.n; i++) o.permtab[o.peritab[i]] = i;
+}
+
+// ---------------------------------------------------------------------------
+// Reordering of the unknowns inside each supernode (pastixSymbolReordering,
+// symbol/symbol_reordering.c:619-660, per supernode :455-610, tour :107-370).
+// Row i of supernode k is described by the sorted list of the supernodes whose
+// off-diagonal bloks cover it; rows with close lists should be adjacent so that
+// the bloks they form are few.  The rows are inserted one by one into a cyclic
+// tour that starts with a ghost row (empty list), at the position that adds the
+// least Hamming distance between neighbours (ties broken by the smaller cut),
+// and the tour is read from the row after the ghost.  split_level separates
+// the lists into contributors of the upper levels of the tree (their distance
+// only gates the candidate positions) and of the lower levels; stop caps every
+// distance.  Each supernode is independent of the others.
+// ---------------------------------------------------------------------------
+namespace {
+struct RowSets {
+    std::vector<idx_t> ptr, val;  // row r: val[ptr[r] .. ptr[r+1])
+    idx_t size(idx_t r) const { return r < 0 ? 0 : ptr[r + 1] - ptr[r]; }
+};
+
+// |A xor B| of two sorted lists, capped at stop; the ghost row (-1) is empty
+idx_t hamming(const RowSets &v, idx_t a, idx_t b, idx_t stop) {
+    if (a == -1) return v.size(b);
+    if (b == -1) return v.size(a);
+    idx_t na = v.size(a), nb = v.size(b);
+    if (na - nb >= stop || nb - na >= stop) return stop;
+    const idx_t *x = v.val.data() + v.ptr[a], *xe = x + na;
+    const idx_t *y = v.val.data() + v.ptr[b], *ye = y + nb;
+    idx_t sum = 0;
+    while (x < xe && y < ye) {
+        if (*x == *y) { x++; y++; }
+        else if (*x < *y) { while (x < xe && *x < *y) { sum++; x++; } }
+        else { while (y < ye && *x > *y) { sum++; y++; } }
+        if (sum >= stop) return stop;
+    }
+    sum += (xe - x) + (ye - y);
+    return sum >= stop ? stop : sum;
+}
+
+// Tour of `size` rows; returns the new order of the local row indices.
+std::vector<idx_t> row_tour(idx_t size, const RowSets &lw, const RowSets &up, idx_t stop) {
+    std::vector<idx_t> tour(size + 1), len(size + 1, 0);
+    tour[0] = -1;
+    tour[1] = 0;
+    len[0] = len[1] = hamming(lw, 0, -1, stop);
+    for (idx_t i = 1; i < size; i++) {
+        idx_t before = hamming(lw, i, tour[0], stop);
+        idx_t after = hamming(lw, i, tour[1], stop);
+        idx_t up_after = hamming(up, i, tour[1], 1);
+        idx_t best = before + after - len[0], bpos = 1, cut = -1;
+        for (idx_t j = 1; j < i; j++) {
+            idx_t up_before = up_after;
+            up_after = hamming(up, i, tour[j + 1], 1);
+            if (up_before < 1 || up_after < 1) {
+                before = (after == -1) ? hamming(lw, i, tour[j], stop) : after;
+                after = hamming(lw, i, tour[j + 1], stop);
+                idx_t l = before + after - len[j];
+                if (l == best) {
+                    if (before < cut) { cut = before; best = l; bpos = j + 1; }
+                    if (after < cut) { cut = after; best = l; bpos = j + 1; }
+                }
+                if (l < best) {
+                    cut = before;
+                    best = l;
+                    bpos = j + 1;
+                    if (after < cut) cut = after;
+                }
+                if (after == 0) {  // an identical row: go right after it
+                    best = l;
+                    bpos = j + 1;
+                    break;
+                }
+            } else {
+                after = -1;
+            }
+        }
+        idx_t to_first = hamming(lw, i, tour[0], stop);
+        idx_t to_last = hamming(lw, i, tour[i], stop);
+        before = hamming(lw, i, tour[bpos - 1], stop);
+        after = hamming(lw, i, tour[bpos], stop);
+        if (to_first + to_last - len[i] < best) bpos = i + 1;
+        if (bpos > 0) len[bpos - 1] = before;
+        if (bpos < i + 1) {  // shift the tail right and insert
+            idx_t k = i, l = after;
+            for (idx_t j = bpos; j < i + 2; j++) {
+                std::swap(tour[j], k);
+                std::swap(len[j], l);
+            }
+        } else {
+            tour[i + 1] = i;
+            len[i + 1] = to_first;
+        }
+    }
+    idx_t ghost = 0;
+    for (idx_t i = 0; i < size; i++)
+        if (tour[i] == -1) ghost = i;
+    std::vector<idx_t> out(size);
+    for (idx_t i = 0; i < size; i++) out[i] = tour[(i + 1 + ghost) % (size + 1)];
+    return out;
+}
+}  // namespace
+
+void symbol_reorder_rows(const Symbol &s, Order &o, idx_t split_level, idx_t stop) {
+    const idx_t cb = s.cblknbr();
+    // depth of every supernode in the ordering's tree (root = 1)
+    std::vector<idx_t> level(cb, 0);
+    idx_t maxdepth = 0;
+    for (idx_t k = cb - 1; k >= 0; k--) {  // fathers have larger numbers
+        idx_t f = o.treetab[k];
+        level[k] = (f < 0) ? 1 : level[f] + 1;
+        maxdepth = std::max(maxdepth, level[k]);
+    }
+    // bloks facing each supernode, in increasing blok number (pastixSymbolBuildRowtab)
+    std::vector<idx_t> bptr(cb + 1, 0), brow;
+    for (idx_t b = 0; b < s.bloknbr(); b++)
+        if (s.bloktab[b].fcblknm != s.bloktab[b].lcblknm) bptr[s.bloktab[b].fcblknm + 1]++;
+    for (idx_t k = 0; k < cb; k++) bptr[k + 1] += bptr[k];
+    brow.resize(bptr[cb]);
+    {
+        std::vector<idx_t> pos(bptr.begin(), bptr.end() - 1);
+        for (idx_t b = 0; b < s.bloknbr(); b++)
+            if (s.bloktab[b].fcblknm != s.bloktab[b].lcblknm) brow[pos[s.bloktab[b].fcblknm]++] = b;
+    }
+    std::vector<idx_t> weight(maxdepth);
+    for (idx_t k = 0; k < cb; k++) {
+        const SymCblk &c = s.cblktab[k];
+        const idx_t size = c.lcolnum - c.fcolnum + 1;
+        // move the split level until neither side dominates (symbol_reordering.c:487-530)
+        std::fill(weight.begin(), weight.end(), 0);
+        for (idx_t e = bptr[k]; e < bptr[k + 1]; e++) {
+            const SymBlok &b = s.bloktab[brow[e]];
+            weight[level[b.lcblknm] - 1] += b.lrownum - b.frownum + 1;
+        }
+        idx_t split = split_level;
+        for (int sign = 0;;) {
+            idx_t upw = 0, lww = 0, i = 0;
+            for (; i < split && i < maxdepth; i++) upw += weight[i];
+            for (; i < maxdepth; i++) lww += weight[i];
+            if (lww < 5 * upw && lww > 10 && upw > 10 && sign <= 0) { split--; sign--; continue; }
+            if (lww > 3 * upw && lww > 10 && upw > 10 && sign >= 0) { split++; sign++; continue; }
+            break;
+        }
+        if (size < 3) continue;
+        RowSets lw, up;
+        lw.ptr.assign(size + 1, 0);
+        up.ptr.assign(size + 1, 0);
+        for (idx_t e = bptr[k]; e < bptr[k + 1]; e++) {
+            const SymBlok &b = s.bloktab[brow[e]];
+            RowSets &v = (level[b.lcblknm] <= split) ? up : lw;
+            for (idx_t r = b.frownum; r <= b.lrownum; r++) v.ptr[r - c.fcolnum + 1]++;
+        }
+        for (idx_t r = 0; r < size; r++) { lw.ptr[r + 1] += lw.ptr[r]; up.ptr[r + 1] += up.ptr[r]; }
+        lw.val.resize(lw.ptr[size]);
+        up.val.resize(up.ptr[size]);
+        {
+            std::vector<idx_t> pl(lw.ptr.begin(), lw.ptr.end() - 1), pu(up.ptr.begin(), up.ptr.end() - 1);
+            for (idx_t e = bptr[k]; e < bptr[k + 1]; e++) {
+                const SymBlok &b = s.bloktab[brow[e]];
+                bool isup = level[b.lcblknm] <= split;
+                for (idx_t r = b.frownum; r <= b.lrownum; r++) {
+                    idx_t lr = r - c.fcolnum;
+                    if (isup) up.val[pu[lr]++] = b.lcblknm; else lw.val[pl[lr]++] = b.lcblknm;
+                }
+            }
+        }
+        std::vector<idx_t> t = row_tour(size, lw, up, stop);
+        std::vector<idx_t> seg(size);
+        for (idx_t i = 0; i < size; i++) seg[i] = o.peritab[c.fcolnum + t[i]];
+        std::copy(seg.begin(), seg.end(), o.peritab.begin() + c.fcolnum);
+    }
+    for (idx_t i = 0; i < o.n; i++) o.permtab[o.peritab[i]] = i;
 }
 
 // ---------------------------------------------------------------------------

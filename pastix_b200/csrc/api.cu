@@ -258,6 +258,9 @@ struct pastix_data_s {
     pgpu::Graph graph;
     pgpu::Order order;
     bool user_order = false;
+    idx_t dof = 1;              // unknowns per node of a node ordering
+    pgpu::Graph node_graph;     // dof > 1: the node graph
+    pgpu::Order node_order;     // dof > 1: the ordering of the nodes
     pgpu::Symbol symbol;
     pgpu::Solver solver;
     // value maps (host, structure only)
@@ -828,6 +831,7 @@ extern "C" int pastix_subtask_order(pastix_data_t *pd, const spmatrix_t *spm, pa
     }
     pgpu::Order &o = pd->order;
     o = pgpu::Order{};
+    idx_t dof = 1;  // > 1: the ordering numbers nodes of dof unknowns each
     const bool personal = pd->iparm[IPARM_ORDERING] == PastixOrderPersonal;
     if (personal && (pd->iparm[IPARM_IO_STRATEGY] & PastixIOLoad)) {
         // the ordering file replaces the personal ordering (order/order_compute_personal.c:71-77)
@@ -835,7 +839,7 @@ extern "C" int pastix_subtask_order(pastix_data_t *pd, const spmatrix_t *spm, pa
         if (rc) return rc;
         if (o.n != n) {
             if (n % o.n != 0) { perr("loaded ordering size mismatch"); return PASTIX_ERR_BADPARAMETER; }
-            pgpu::order_expand_dof(o, n / o.n);  // node ordering of a dof > 1 matrix
+            dof = n / o.n;
         }
         pd->user_order = true;
     } else if (personal && myorder && myorder->permtab) {
@@ -856,7 +860,7 @@ extern "C" int pastix_subtask_order(pastix_data_t *pd, const spmatrix_t *spm, pa
             for (idx_t k = 0; k <= o.cblknbr; k++) o.rangtab[k] = myorder->rangtab[k] - ob;
             for (idx_t k = 0; k < o.cblknbr; k++) o.treetab[k] = myorder->treetab[k] < 0 ? -1 : myorder->treetab[k] - ob;
         }
-        if (vn != n) pgpu::order_expand_dof(o, n / vn);  // node ordering of a dof>1 matrix
+        dof = n / vn;
         pd->user_order = true;
     } else {
         // identity start; nested dissection of the graph is applied below
@@ -866,20 +870,45 @@ extern "C" int pastix_subtask_order(pastix_data_t *pd, const spmatrix_t *spm, pa
         pgpu::order_nd_graph(o, pd->graph);
         pd->user_order = false;
     }
+    // A node ordering of a matrix with dof unknowns per node is analysed on the
+    // node graph, as the reference analyses spm->dof > 1 matrices, and expanded
+    // to unknowns afterwards.
+    pd->dof = dof;
+    pd->node_graph = pgpu::Graph{};
+    if (dof > 1) pgpu::graph_collapse(pd->graph, dof, pd->node_graph);
+    const pgpu::Graph &g = dof > 1 ? pd->node_graph : pd->graph;
     if (o.rangtab.empty() || o.treetab.empty()) {  // order/pastix_subtask_order.c:360-364
         o.rangtab.clear();
         o.treetab.clear();
         o.cblknbr = 0;
-        pgpu::order_find_supernodes(o, pd->graph);
+        pgpu::order_find_supernodes(o, g);
     }
+    // supernodes renumbered by tree level (order/pastix_subtask_order.c:399-401)
+    pgpu::order_apply_level_order(o, pd->iparm[IPARM_TASKS2D_LEVEL], pd->iparm[IPARM_TASKS2D_WIDTH]);
     std::string err = pgpu::order_check(o);
     if (!err.empty()) { perr("ordering check failed: %s", err.c_str()); return PASTIX_ERR_BADPARAMETER; }
     if (pd->iparm[IPARM_IO_STRATEGY] & PastixIOSave) {  // order/pastix_subtask_order.c:485
         rc = order_save_file(pd, o);
         if (rc) return rc;
     }
+    pd->node_order = pgpu::Order{};
+    if (dof > 1) {
+        pd->node_order = o;
+        pgpu::order_expand_dof(o, dof);
+    }
     pd->steps = STEP_INIT | STEP_ORDERING;
     return PASTIX_SUCCESS;
+}
+
+static int symbol_save_file(pastix_data_t *pd) {
+    const char *dir = output_dir(pd);
+    if (!dir) return PASTIX_ERR_FILE;
+    const std::string path = std::string(dir) + "/symbgen";
+    FILE *f = fopen(path.c_str(), "w");
+    if (!f) { perr("cannot write %s", path.c_str()); return PASTIX_ERR_FILE; }
+    int rc = symbol_write(f, pd->symbol);
+    if (fclose(f) != 0 && rc == PASTIX_SUCCESS) rc = PASTIX_ERR_FILE;
+    return rc;
 }
 
 extern "C" int pastix_subtask_symbfact(pastix_data_t *pd) {
@@ -909,13 +938,7 @@ extern "C" int pastix_subtask_symbfact(pastix_data_t *pd) {
         pgpu::symbol_fax(pd->symbol, pd->graph, pd->order);
     }
     if (pd->iparm[IPARM_IO_STRATEGY] & PastixIOSave) {  // symbol/pastix_subtask_symbfact.c:275-285
-        const char *dir = output_dir(pd);
-        if (!dir) return PASTIX_ERR_FILE;
-        const std::string path = std::string(dir) + "/symbgen";
-        FILE *f = fopen(path.c_str(), "w");
-        if (!f) { perr("cannot write %s", path.c_str()); return PASTIX_ERR_FILE; }
-        int rc = symbol_write(f, pd->symbol);
-        if (fclose(f) != 0 && rc == PASTIX_SUCCESS) rc = PASTIX_ERR_FILE;
+        int rc = symbol_save_file(pd);
         if (rc) return rc;
     }
     pd->dparm[DPARM_SYMBFACT_TIME] = now_s() - t0;
@@ -923,9 +946,36 @@ extern "C" int pastix_subtask_symbfact(pastix_data_t *pd) {
     return PASTIX_SUCCESS;
 }
 
+// pastix_subtask_reordering (symbol/pastix_subtask_reordering.c:60): the rows
+// of every supernode reordered to group the bloks that face it, then the block
+// symbolic factorization again with the new ordering.
 extern "C" int pastix_subtask_reordering(pastix_data_t *pd) {
     if (!pd || !(pd->steps & STEP_SYMBFACT)) return PASTIX_ERR_BADPARAMETER;
-    pd->dparm[DPARM_REORDER_TIME] = 0.0;
+    double t0 = now_s();
+    // a loaded analysis (PastixIOLoad) was saved after its reordering
+    if (!(pd->iparm[IPARM_IO_STRATEGY] & PastixIOLoad) && (idx_t)pd->order.treetab.size() == pd->symbol.cblknbr() &&
+        pd->graph.n == pd->order.n && (pd->dof == 1 || pd->node_order.n * pd->dof == pd->order.n)) {
+        const idx_t split = pd->iparm[IPARM_REORDERING_SPLIT], stop = pd->iparm[IPARM_REORDERING_STOP];
+        if (pd->dof > 1) {  // rows of nodes, on the node structure
+            pgpu::Symbol nsym;
+            pgpu::symbol_fax(nsym, pd->node_graph, pd->node_order);
+            pgpu::symbol_reorder_rows(nsym, pd->node_order, split, stop);
+            pd->order = pd->node_order;
+            pgpu::order_expand_dof(pd->order, pd->dof);
+        } else {
+            pgpu::symbol_reorder_rows(pd->symbol, pd->order, split, stop);
+        }
+        if (pd->iparm[IPARM_IO_STRATEGY] & PastixIOSave) {
+            int rc = order_save_file(pd, pd->dof > 1 ? pd->node_order : pd->order);
+            if (rc) return rc;
+        }
+        pgpu::symbol_fax(pd->symbol, pd->graph, pd->order);
+        if (pd->iparm[IPARM_IO_STRATEGY] & PastixIOSave) {  // the symbolic step runs again and saves
+            int rc = symbol_save_file(pd);
+            if (rc) return rc;
+        }
+    }
+    pd->dparm[DPARM_REORDER_TIME] = now_s() - t0;
     return PASTIX_SUCCESS;
 }
 

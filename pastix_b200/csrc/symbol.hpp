@@ -93,7 +93,10 @@ struct Solver {
 // ---- analysis steps ----
 void order_grid(Order &o, idx_t nx, idx_t ny, idx_t nz);
 void order_expand_dof(Order &o, idx_t dof);
+void graph_collapse(const Graph &g, idx_t dof, Graph &out);
 void order_find_supernodes(Order &o, const Graph &g);
+void order_apply_level_order(Order &o, idx_t level2d, idx_t width2d);
+void symbol_reorder_rows(const Symbol &s, Order &o, idx_t split_level, idx_t stop);
 void order_nd_graph(Order &o, const Graph &g, idx_t leaf = 64);
 std::string order_check(const Order &o);
 void symbol_fax(Symbol &s, const Graph &g, const Order &o);

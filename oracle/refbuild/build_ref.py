@@ -159,7 +159,11 @@ def include_flags(src: Path) -> list[str]:
     return [f"-I{d}" for d in dirs]
 
 
-CFLAGS = ["-O2", "-g0", "-fPIC", "-std=gnu11", "-w", "-Drestrict=", "-pthread", "-fno-strict-aliasing"]
+# -DNDEBUG as in an optimized build: one debug assertion of the reference
+# (blend/solver_matrix_gen_utils.c:514-515) compares the rows of a symbol blok,
+# counted in nodes, with those of its solver blok, counted in unknowns, and so
+# fails for dof > 1 matrices whose supernodes are wide enough for 2D tasks.
+CFLAGS = ["-O2", "-g0", "-fPIC", "-std=gnu11", "-w", "-Drestrict=", "-pthread", "-fno-strict-aliasing", "-DNDEBUG"]
 
 
 def _obj_name(path: Path, prec: str, src: Path) -> Path:
@@ -225,6 +229,13 @@ def build(src: Path | None = None, jobs: int | None = None) -> Path:
     if blas is None:
         raise FileNotFoundError("no OpenBLAS with CBLAS/LAPACKE names found")
     OUT.mkdir(parents=True, exist_ok=True)
+    stamp = OUT / "cflags.txt"
+    if not stamp.exists() or stamp.read_text() != " ".join(CFLAGS):
+        import shutil
+        shutil.rmtree(OBJ, ignore_errors=True)  # objects of other flags
+        if LIB.exists():
+            LIB.unlink()
+        stamp.write_text(" ".join(CFLAGS))
     units = generate(src)
     for own in ("shim/spm_min.c", "shim/missing.c", "ref_driver.c"):
         units.append((HERE / own, ""))

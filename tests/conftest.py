@@ -64,3 +64,30 @@ def backward_error(A, x, b) -> float:
     import scipy.sparse.linalg as spla
     r = b - A @ x
     return float(np.linalg.norm(r) / (spla.norm(A) * np.linalg.norm(x) + np.linalg.norm(b)))
+
+
+@pytest.fixture(scope="session")
+def ref_mod():
+    """The reference PaStiX compiled from its sources (oracle/_ref).  Built here
+    when the source tree is on this machine; the tests that need it are skipped
+    when it is neither built nor buildable."""
+    from oracle import ref
+    if not ref.available():
+        from oracle.refbuild import build_ref
+        src = build_ref.ref_root()
+        if not (src / "sopalin" / "pastix_task_sopalin.c").exists():
+            pytest.skip("oracle/_ref is not built and the reference source tree is absent")
+        ref.build(src)
+    ref.load()
+    return ref
+
+
+def fixture_matrix(name):
+    """A reference test matrix from tests/golden (CSC, 0-based) and its HB type."""
+    import scipy.sparse as sps
+    z = np.load(ROOT / "tests" / "golden" / f"{name}.npz")
+    n = int(z["n"])
+    A = sps.csc_matrix((z["values"], z["rowind"], z["colptr"]), shape=(n, n))
+    if str(z["mxtype"])[1] == "S":  # symmetric: the file stores one triangle
+        A = (A + sps.tril(A, -1).T).tocsc()
+    return A, str(z["mxtype"])

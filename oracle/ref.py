@@ -248,6 +248,21 @@ class RefPastix:
             raise RuntimeError("ref_get_coef failed")
         return out
 
+    def compare_panels(self, P: np.ndarray, info: dict, side: int = 0, mask_upper: bool = False) -> float:
+        """Relative Frobenius distance between the reference's factors and
+        factors P in the product's panel layout (``info``: pgpu_solver_info of
+        the same structure), computed without a second copy of the factors."""
+        P = np.ascontiguousarray(P)
+        arrs = [_i64(info[k]) for k in ("cb_coef", "cb_stride", "bk_rowoff")]
+        out = np.zeros(2)
+        rc = self.lib.ref_compare_panels(self.h, C.c_int(side), P.ctypes.data_as(C.c_void_p),
+                                         C.c_int(int(P.dtype == np.float32)),
+                                         *(a.ctypes.data_as(I64P) for a in arrs), C.c_int(int(mask_upper)),
+                                         out.ctypes.data_as(DP))
+        if rc:
+            raise RuntimeError("ref_compare_panels failed")
+        return float(np.sqrt(out[0] / out[1]))
+
     def solve(self, B: np.ndarray) -> np.ndarray:
         X = np.asfortranarray(np.array(B, dtype=np.float64, copy=True))
         if X.ndim == 1:

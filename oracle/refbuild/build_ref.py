@@ -164,6 +164,8 @@ def include_flags(src: Path) -> list[str]:
 # counted in nodes, with those of its solver blok, counted in unknowns, and so
 # fails for dof > 1 matrices whose supernodes are wide enough for 2D tasks.
 CFLAGS = ["-O2", "-g0", "-fPIC", "-std=gnu11", "-w", "-Drestrict=", "-pthread", "-fno-strict-aliasing", "-DNDEBUG"]
+# the comparison helper of ref_driver.c runs its loop with OpenMP
+DRIVER_FLAGS = ["-fopenmp"]
 
 
 def _obj_name(path: Path, prec: str, src: Path) -> Path:
@@ -184,6 +186,8 @@ def compile_unit(path: Path, prec: str, src: Path) -> tuple[Path, str | None]:
         return obj, None
     obj.parent.mkdir(parents=True, exist_ok=True)
     flags = list(CFLAGS)
+    if path.name == "ref_driver.c":
+        flags += DRIVER_FLAGS
     if prec:
         flags.append(f"-DPRECISION_{prec}")
     cmd = ["gcc", *flags, *include_flags(src), "-c", str(path), "-o", str(obj)]
@@ -199,7 +203,7 @@ def _undefined(log: str) -> list[str]:
 
 def link(objs: list[Path], blas: Path) -> None:
     base = ["gcc", "-shared", "-o", str(LIB), *map(str, objs), str(blas), f"-Wl,-rpath,{blas.parent}",
-            "-lm", "-lpthread", "-Wl,--no-undefined"]
+            "-lm", "-lpthread", "-fopenmp", "-Wl,--no-undefined"]
     r = subprocess.run(base, capture_output=True, text=True)
     if r.returncode == 0:
         (OUT / "stubbed.txt").write_text("")

@@ -264,3 +264,51 @@ int ref_refine( ref_handle_t *h, pastix_int_t nrhs, double *b, pastix_int_t ldb,
 {
     return pastix_task_refine( h->pd, h->spm.nexp, nrhs, b, ldb, x, ldx );
 }
+
+/*
+ * Distance between the reference's factors and factors stored in the product's
+ * panel layout (cblk k: one column-major panel of stride x width at
+ * cb_coef[k], blok b starting at row bk_rowoff[b]) for the same structure,
+ * without a second copy of the factors: out[0] = sum (ref - P)^2,
+ * out[1] = sum ref^2.  mask_upper skips the strict upper triangle of the
+ * diagonal blocks (unused by LL^T).  P holds doubles, or floats if single.
+ */
+int ref_compare_panels( ref_handle_t *h, int side, const void *P, int single, const pastix_int_t *cb_coef,
+                        const pastix_int_t *cb_stride, const pastix_int_t *bk_rowoff, int mask_upper, double *out )
+{
+    const SolverMatrix *s = h->pd ? h->pd->solvmatr : NULL;
+    double              d2 = 0.0, r2 = 0.0;
+    if ( s == NULL ) {
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    const int rsingle = ( s->flttype == PastixFloat );
+    #pragma omp parallel for reduction(+:d2,r2) schedule(dynamic, 16)
+    for ( pastix_int_t k = 0; k < s->cblknbr; k++ ) {
+        const SolverCblk *c    = s->cblktab + k;
+        const void       *src  = side ? c->ucoeftab : c->lcoeftab;
+        const int         is2d = ( c->cblktype & CBLK_LAYOUT_2D ) != 0;
+        pastix_int_t      nc   = c->lcolnum - c->fcolnum + 1;
+        if ( src == NULL ) {
+            continue;
+        }
+        for ( const SolverBlok *b = c->fblokptr; b < c[1].fblokptr; b++ ) {
+            pastix_int_t nr   = b->lrownum - b->frownum + 1;
+            pastix_int_t ld   = is2d ? nr : c->stride;
+            pastix_int_t bi   = b - s->bloktab;
+            int          diag = ( b == c->fblokptr );
+            for ( pastix_int_t j = 0; j < nc; j++ ) {
+                for ( pastix_int_t i = ( diag && mask_upper ) ? j : 0; i < nr; i++ ) {
+                    pastix_int_t e  = b->coefind + j * ld + i;
+                    pastix_int_t q  = cb_coef[k] + bk_rowoff[bi] + i + j * cb_stride[k];
+                    double       rv = rsingle ? (double)( (const float *)src )[e] : ( (const double *)src )[e];
+                    double       pv = single ? (double)( (const float *)P )[q] : ( (const double *)P )[q];
+                    d2 += ( rv - pv ) * ( rv - pv );
+                    r2 += rv * rv;
+                }
+            }
+        }
+    }
+    out[0] = d2;
+    out[1] = r2;
+    return PASTIX_SUCCESS;
+}

@@ -760,6 +760,25 @@ void symbol_split(Symbol &s, idx_t bmin, idx_t bmax) {
     s = std::move(ns);
 }
 
+// Symbol of nodes -> symbol of unknowns, dof per node (the expansion
+// blend/solver_matrix_gen.c applies when it builds the solver of a dof > 1
+// matrix): every column or row range [f, l] becomes [f*dof, l*dof + dof-1].
+void symbol_expand(const Symbol &node, idx_t dof, Symbol &out) {
+    out.nodenbr = node.nodenbr * dof;
+    out.cblktab = node.cblktab;
+    for (auto &c : out.cblktab) {
+        c.fcolnum *= dof;
+        c.lcolnum = c.lcolnum * dof + dof - 1;
+    }
+    out.cblktab.back().fcolnum = out.nodenbr;
+    out.cblktab.back().lcolnum = out.nodenbr - 1;
+    out.bloktab = node.bloktab;
+    for (auto &b : out.bloktab) {
+        b.frownum *= dof;
+        b.lrownum = b.lrownum * dof + dof - 1;
+    }
+}
+
 std::string symbol_check(const Symbol &s) {
     std::ostringstream err;
     idx_t cbn = s.cblknbr();

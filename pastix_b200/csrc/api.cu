@@ -1283,7 +1283,21 @@ extern "C" int pastix_subtask_blend(pastix_data_t *pd) {
     if (bmin > bmax || bmin < 1) { perr("IPARM_MIN_BLOCKSIZE > IPARM_MAX_BLOCKSIZE"); return PASTIX_ERR_BADPARAMETER; }
     // the wide-cblk kernels keep a (32 x width) strip per operand in shared memory
     if (bmax > 384) { perr("IPARM_MAX_BLOCKSIZE above 384 is not supported by the GPU kernels"); return PASTIX_ERR_BADPARAMETER; }
-    pgpu::symbol_split(pd->symbol, bmin, bmax);
+    // The reference splits the supernodes of a dof > 1 matrix on its node
+    // symbol, widths counted in nodes (blend/splitsymbol.c:78-102 on the symbol
+    // before the expansion of blend/solver_matrix_gen.c).  That is done here
+    // whenever the expanded widths fit the kernels (IPARM_MAX_BLOCKSIZE * dof
+    // <= 384); otherwise the split counts unknowns, so that no cblk is wider
+    // than IPARM_MAX_BLOCKSIZE unknowns.
+    if (pd->dof > 1 && bmax * pd->dof <= 384 && pd->node_order.n * pd->dof == pd->order.n &&
+        !(pd->iparm[IPARM_IO_STRATEGY] & PastixIOLoad)) {
+        pgpu::Symbol nsym;
+        pgpu::symbol_fax(nsym, pd->node_graph, pd->node_order);
+        pgpu::symbol_split(nsym, bmin, bmax);
+        pgpu::symbol_expand(nsym, pd->dof, pd->symbol);
+    } else {
+        pgpu::symbol_split(pd->symbol, bmin, bmax);
+    }
     std::string err = pgpu::symbol_check(pd->symbol);
     if (!err.empty()) { perr("symbol check failed: %s", err.c_str()); return PASTIX_ERR_INTERNAL; }
     pd->factotype = (int)pd->iparm[IPARM_FACTORIZATION];

@@ -101,6 +101,7 @@ void order_nd_graph(Order &o, const Graph &g, idx_t leaf = 64);
 std::string order_check(const Order &o);
 void symbol_fax(Symbol &s, const Graph &g, const Order &o);
 void symbol_split(Symbol &s, idx_t blcolmin, idx_t blcolmax);
+void symbol_expand(const Symbol &node, idx_t dof, Symbol &out);
 std::string symbol_check(const Symbol &s);
 double symbol_flops(const Symbol &s, int factotype);
 void solver_build(Solver &sv, const Symbol &s, int factotype);

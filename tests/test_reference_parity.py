@@ -56,6 +56,23 @@ def test_analysis_identical_to_reference(lib, ref_mod, name):
 TOL = {"el48": 5e-12}
 
 
+def test_analysis_identical_dof3_split(lib, ref_mod):
+    """dof = 3: the reference splits the supernodes of the node symbol, widths
+    in nodes.  With IPARM_MAX_BLOCKSIZE * dof within the GPU kernels' limit
+    the product does the same, and both give one structure."""
+    K, _ = gen.elastic27_dof3(16, 16, 16)
+    grid = (16, 16, 16)
+    r = ref_mod.RefPastix(K, "SYTRF", dof=3, min_bs=53, max_bs=106)
+    r.analyze(grid=grid)
+    s = r.structure()
+    pd, S, info = analyse(K, grid, "SYTRF", min_bs=53, max_bs=106)
+    assert s["cblknbr"] > 16 ** 3 // 106  # wide supernodes were split
+    assert np.array_equal(_expanded_perm(s, 3), np.asarray(info["permtab"]))
+    for k in STRUCT_KEYS:
+        assert np.array_equal(np.asarray(s[k]), np.asarray(info[k])), k
+    assert s["thflops"] == info["thflops"]
+
+
 def _compare_factors(ref_mod, oracle_mod, r, A, fact, magn=0.0, tol=1e-13):
     s = r.structure()
     npiv_ref = r.numfact()
@@ -119,3 +136,22 @@ def test_orsirr_lu_sign_keeping_pivots(lib, ref_mod, oracle_mod, magn, expected)
     r = ref_mod.RefPastix(A, "GETRF", nthreads=2, magn_ctrl=magn)
     r.analyze(perm=_product_perm(A, "GETRF"))
     assert _compare_factors(ref_mod, oracle_mod, r, A, "GETRF", magn) == expected
+
+
+def test_panel_comparison_helper(lib, ref_mod, oracle_mod):
+    """ref_compare_panels (used by the GPU parity tests on full-size factors)
+    against a plain comparison: the oracle's factors moved to the product's
+    panel layout are at rounding distance, a planted error is seen."""
+    A, grid, fact = gen.workload("lap20")
+    r = ref_mod.RefPastix(A, fact, nthreads=2)
+    r.analyze(grid=grid)
+    r.numfact()
+    pd, S, info = analyse(A, grid, fact)
+    sym = oracle_mod.Symbol(info)
+    Ap = oracle_mod.permuted_full(A, np.asarray(info["permtab"]))
+    L, _, _ = oracle_mod.factor(sym, Ap, fact, oracle_mod.criterion(Ap))
+    P = oracle_mod.to_panels(sym, L)
+    assert r.compare_panels(P, info, mask_upper=True) < 1e-14
+    k = int(info["cblknbr"]) - 1  # last cblk: its diagonal entry
+    P[int(info["cb_coef"][k])] *= 1.0 + 1e-6
+    assert r.compare_panels(P, info, mask_upper=True) > 1e-9

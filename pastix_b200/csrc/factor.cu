@@ -1605,7 +1605,9 @@ __global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__
 // ---------------------------------------------------------------------------
 constexpr int DC = 8;                      // CTAs per cluster
 constexpr int DC_MIN_NC = 96;              // narrower blocks stay on one CTA
-constexpr long long DC_MAX_SMEM = 180 * 1024;  // dynamic shared memory next to the static 46 KB
+// dynamic shared memory next to the static ~37 KB
+__host__ __device__ constexpr long long dc_max_smem(int) { return 180 * 1024LL; }
+constexpr int DC_SLOTS = (DG_MAXNC / 32 + DC - 1) / DC;  // panels one CTA can own (nc <= DG_MAXNC)
 
 __host__ __device__ inline int dc_lo(int p, int fact) { return fact == FACT_GETRF ? 0 : 32 * p; }
 // Shared memory (doubles) of the panels CTA `rank` owns for a block of width nc.
@@ -1615,8 +1617,30 @@ __host__ __device__ inline long long dc_panel_doubles(int nc, int fact, int rank
     for (int p = rank; p < np; p += DC) n += (long long)(nc - dc_lo(p, fact)) * DG_LD;
     return n;
 }
+// GETRF: the inverted (L_pp)^T of each panel a CTA factors, read by the other
+// CTAs, one slot per panel it owns, ahead of the panels
+__host__ __device__ inline long long dc_zs1_doubles(int fact) {
+    return fact == FACT_GETRF ? (long long)DC_SLOTS * 32 * DG_LD : 0;
+}
 __host__ __device__ inline long long diag_cluster_smem_bytes(int nc, int fact) {
-    return 8 * dc_panel_doubles(nc, fact, 0);  // CTA 0 holds the most
+    return 8 * (dc_zs1_doubles(fact) + dc_panel_doubles(nc, fact, 0));  // CTA 0 holds the most
+}
+
+// Cluster-scope flag of one CTA, read from another CTA of the cluster.
+__device__ __forceinline__ uint32_t dsmem_map(const void *local, int rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+                 : "=r"(r)
+                 : "r"((uint32_t)__cvta_generic_to_shared(local)), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ int dsmem_ld_acquire(uint32_t addr) {
+    int v;
+    asm volatile("ld.acquire.cluster.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+    return v;
+}
+__device__ __forceinline__ void dsmem_st_release(uint32_t addr, int v) {
+    asm volatile("st.release.cluster.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
 
 template <typename T, int FACT>
@@ -1624,11 +1648,14 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
     k_diag_cluster(DevStruct s, const int *__restrict__ list, T *L, T *U, T *dinv, FactParams fp) {
     namespace cg = cooperative_groups;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *Wl = reinterpret_cast<double *>(smem_raw);  // this CTA's panels, one after the other
-    __shared__ double Zs[2][32 * DG_LD];                 // inverted top blocks of the last panel factored here
+    // GETRF: inverted (L_pp)^T of each panel factored here (read by the other CTAs
+    // for U_pq), one slot per panel; then this CTA's panels, one after the other
+    double *Zs1 = reinterpret_cast<double *>(smem_raw);
+    double *Wl = Zs1 + dc_zs1_doubles(FACT);
+    __shared__ double Zs0[32 * DG_LD];                   // inverted top block of the panel being factored here
     __shared__ __align__(16) double Sx[8][8 * DG_LD];  // also the published steps of the top block's factorization
-    __shared__ double Tb[32 * DG_LD];                    // the top block being factored
-    __shared__ int npiv, prog;
+    __shared__ double Tb[32 * DG_LD];                    // the top block being factored / an update's B block
+    __shared__ int npiv, prog, fdone;                    // fdone: 1 + last panel factored by this CTA
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
     const int k = list[blockIdx.x / DC];
@@ -1638,7 +1665,10 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
     T *A = L + s.cb_coef[k];
     T *gZ = dinv + s.cb_dinv[k];
-    if (tid == 0) npiv = 0;
+    if (tid == 0) {
+        npiv = 0;
+        fdone = 0;
+    }
     // panel p of CTA p % DC: its offset inside that CTA's shared memory
     auto poff = [&](int p) {
         long long off = 0;
@@ -1665,107 +1695,145 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
             },
             [&](int r, int c, double v) { W[r * DG_LD + c] = v; });
     }
-    __syncthreads();
-    for (int p = 0; p < np; p++) {
+    cluster.sync();  // panels loaded and flags cleared in every CTA before any flag is read
+
+    // Factor panel p (this CTA owns it; every update from panels < p applied):
+    // top block, its inverse(s), the rows below; then announce it.
+    auto factor_panel = [&](int p) {
         const int nb = min(32, nc - 32 * p);
         const int lop = dc_lo(p, FACT);
-        if (p % DC == rank) {  // factor panel p
-            double *W = Wl + poff(p);
-            double *Wt = W + (32 * p - lop) * DG_LD;  // top block
-            for (int e = tid; e < nb * DG_LD; e += blockDim.x) Tb[e] = Wt[e];  // the panel has nb rows left at its top
-            if (tid == 0) prog = 0;
-            __syncthreads();
-            if (warp == 0) {
-                const int n = dg_factor32<FACT>(Tb, nb, __ldg(fp.criterion), &Sx[0][0], &prog);
-                if (lane == 0 && n) npiv += n;
-            } else if (warp == 1) {
-                dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 0, &prog, Zs[0], gZ + (size_t)p * 1024, fp.status);
-            } else if (FACT == FACT_GETRF && warp == 2) {
-                dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 1, &prog, Zs[1], gZ + (size_t)(np + p) * 1024, fp.status);
-            }
-            __syncthreads();
-            for (int e = tid; e < nb * DG_LD; e += blockDim.x) Wt[e] = Tb[e];
-            __syncthreads();
-            const int r0 = 32 * p + 32;  // rows below the top block
-            const int nrf = (nc - r0 + 7) / 8;
-            for (int i = warp; i < nrf; i += 8) {
-                const int rb = r0 + 8 * i;
-                dg_solve8(
-                    [&](int row, int col) { return (rb + row < nc) ? W[(rb + row - lop) * DG_LD + col] : 0.0; },
-                    [&](int a, int b) { return (a <= b && b < nb) ? dg_t<FACT>(Tb, a, b, 0) : 0.0; }, Zs[0],
-                    Sx[warp],
-                    [&](int row, int col, double v) {
-                        if (rb + row < nc) W[(rb + row - lop) * DG_LD + col] = v;
-                    });
+        double *W = Wl + poff(p);
+        double *Wt = W + (32 * p - lop) * DG_LD;  // top block
+        double *Z1 = (FACT == FACT_GETRF) ? Zs1 + (p / DC) * 32 * DG_LD : Zs1;
+        for (int e = tid; e < nb * DG_LD; e += blockDim.x) Tb[e] = Wt[e];  // the panel has nb rows left at its top
+        if (tid == 0) prog = 0;
+        __syncthreads();
+        if (warp == 0) {
+            const int n = dg_factor32<FACT>(Tb, nb, __ldg(fp.criterion), &Sx[0][0], &prog);
+            if (lane == 0 && n) npiv += n;
+        } else if (warp == 1) {
+            dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 0, &prog, Zs0, gZ + (size_t)p * 1024, fp.status);
+        } else if (FACT == FACT_GETRF && warp == 2) {
+            dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 1, &prog, Z1, gZ + (size_t)(np + p) * 1024, fp.status);
+        }
+        __syncthreads();
+        for (int e = tid; e < nb * DG_LD; e += blockDim.x) Wt[e] = Tb[e];
+        __syncthreads();
+        const int r0 = 32 * p + 32;  // rows below the top block
+        const int nrf = (nc - r0 + 7) / 8;
+        for (int i = warp; i < nrf; i += 8) {
+            const int rb = r0 + 8 * i;
+            dg_solve8(
+                [&](int row, int col) { return (rb + row < nc) ? W[(rb + row - lop) * DG_LD + col] : 0.0; },
+                [&](int a, int b) { return (a <= b && b < nb) ? dg_t<FACT>(Tb, a, b, 0) : 0.0; }, Zs0, Sx[warp],
+                [&](int row, int col, double v) {
+                    if (rb + row < nc) W[(rb + row - lop) * DG_LD + col] = v;
+                });
+        }
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("fence.acq_rel.cluster;" ::: "memory");
+            dsmem_st_release(dsmem_map(&fdone, rank), p + 1);
+        }
+    };
+    // Wait until panel p is factored (bounded; on expiry the status word records
+    // PGPU_STATUS_TIMEOUT and the CTA carries on, so that the kernel ends).
+    auto wait_panel = [&](int p) {
+        if (p % DC != rank && tid == 0) {
+            const uint32_t fa = dsmem_map(&fdone, p % DC);
+            int spins = 0;
+            while (dsmem_ld_acquire(fa) < p + 1) {
+                if (++spins > DG_SPIN) {
+                    atomicExch(fp.status, PGPU_STATUS_TIMEOUT);
+                    break;
+                }
+                __nanosleep(20);
             }
         }
-        cluster.sync();  // panel p (and its inverted blocks) visible to the cluster
-        if (p + 1 == np) break;
+        __syncthreads();
+    };
+    // Update of this CTA's panel q by the factored panel p (read remotely).
+    auto update_panel = [&](int p, int q) {
+        const int nb = min(32, nc - 32 * p);
+        const int lop = dc_lo(p, FACT);
         const double *Wp = panel(p);
         const double *Wpt = Wp + (32 * p - lop) * DG_LD;
-        const double *Zr = cluster.map_shared_rank(&Zs[0][0], p % DC);
-        for (int q = p + 1 + ((rank - (p + 1)) % DC + DC) % DC; q < np; q += DC) {
-            const int nbq = min(32, nc - 32 * q);
-            const int loq = dc_lo(q, FACT);
-            double *Wq = Wl + poff(q);
-            if (FACT == FACT_GETRF) {  // U_pq = L_pp^{-1} A_pq, as (U_pq)^T L_pp^T = (A_pq)^T, 8 columns per warp
-                double *Ab = Wq + (32 * p - loq) * DG_LD;  // rows 32 p .. 32 p + 31 of panel q
-                if (warp < 4) {
-                    const int c0 = 8 * warp;
-                    dg_solve8(
-                        [&](int row, int col) { return (c0 + row < nbq) ? Ab[col * DG_LD + c0 + row] : 0.0; },
-                        [&](int a, int b) { return (a <= b && b < nb) ? dg_t<FACT>(Wpt, a, b, 1) : 0.0; },
-                        Zr + 32 * DG_LD, Sx[warp],
-                        [&](int row, int col, double v) {
-                            if (c0 + row < nbq) Ab[col * DG_LD + c0 + row] = v;
-                        });
-                }
-                __syncthreads();
-            }
-            // B block of this update (32 x 32: k by the columns of panel q) staged locally
-            for (int e = tid; e < 1024; e += blockDim.x) {
-                const int kk = e >> 5, cc = e & 31;
-                double b = 0.0;
-                if (cc < nbq && kk < nb) {
-                    if (FACT == FACT_GETRF) b = Wq[(32 * p + kk - loq) * DG_LD + cc];
-                    else {
-                        b = Wp[(32 * q + cc - lop) * DG_LD + kk];
-                        if (FACT == FACT_SYTRF) b *= Wpt[kk * DG_LD + kk];
-                    }
-                }
-                Tb[kk * DG_LD + cc] = b;
-            }
-            __syncthreads();
-            // trailing rows of panel q: rows from 32 p + 32 (GETRF) or 32 q (lower part) to nc;
-            // the 8 remote A values of a row fragment are requested together
-            const int rs = (FACT == FACT_GETRF) ? 32 * p + 32 : 32 * q;
-            const int nrf = (nc - rs + 7) / 8;
-            for (int i = warp; i < nrf; i += 8) {
-                const int rb = rs + 8 * i;
-                const bool rowok = rb + g < nc;
-                double av[8];
-#pragma unroll
-                for (int ks = 0; ks < 8; ks++) av[ks] = rowok ? -Wp[(rb + g - lop) * DG_LD + 4 * ks + t4] : 0.0;
-                double c[4][2];
-#pragma unroll
-                for (int cf = 0; cf < 4; cf++)
-#pragma unroll
-                    for (int e = 0; e < 2; e++)
-                        c[cf][e] = rowok ? Wq[(rb + g - loq) * DG_LD + 8 * cf + 2 * t4 + e] : 0.0;
-#pragma unroll
-                for (int ks = 0; ks < 8; ks++)
-#pragma unroll
-                    for (int cf = 0; cf < 4; cf++)
-                        dmma884(c[cf][0], c[cf][1], av[ks], Tb[(4 * ks + t4) * DG_LD + 8 * cf + g]);
-#pragma unroll
-                for (int cf = 0; cf < 4; cf++)
-#pragma unroll
-                    for (int e = 0; e < 2; e++)
-                        if (rowok) Wq[(rb + g - loq) * DG_LD + 8 * cf + 2 * t4 + e] = c[cf][e];
+        const int nbq = min(32, nc - 32 * q);
+        const int loq = dc_lo(q, FACT);
+        double *Wq = Wl + poff(q);
+        if (FACT == FACT_GETRF) {  // U_pq = L_pp^{-1} A_pq, as (U_pq)^T L_pp^T = (A_pq)^T, 8 columns per warp
+            const double *Zr = cluster.map_shared_rank(Zs1 + (p / DC) * 32 * DG_LD, p % DC);
+            double *Ab = Wq + (32 * p - loq) * DG_LD;  // rows 32 p .. 32 p + 31 of panel q
+            if (warp < 4) {
+                const int c0 = 8 * warp;
+                dg_solve8(
+                    [&](int row, int col) { return (c0 + row < nbq) ? Ab[col * DG_LD + c0 + row] : 0.0; },
+                    [&](int a, int b) { return (a <= b && b < nb) ? dg_t<FACT>(Wpt, a, b, 1) : 0.0; }, Zr,
+                    Sx[warp], [&](int row, int col, double v) {
+                        if (c0 + row < nbq) Ab[col * DG_LD + c0 + row] = v;
+                    });
             }
             __syncthreads();
         }
+        // B block of this update (32 x 32: k by the columns of panel q) staged locally
+        for (int e = tid; e < 1024; e += blockDim.x) {
+            const int kk = e >> 5, cc = e & 31;
+            double b = 0.0;
+            if (cc < nbq && kk < nb) {
+                if (FACT == FACT_GETRF) b = Wq[(32 * p + kk - loq) * DG_LD + cc];
+                else {
+                    b = Wp[(32 * q + cc - lop) * DG_LD + kk];
+                    if (FACT == FACT_SYTRF) b *= Wpt[kk * DG_LD + kk];
+                }
+            }
+            Tb[kk * DG_LD + cc] = b;
+        }
+        __syncthreads();
+        // trailing rows of panel q: rows from 32 p + 32 (GETRF) or 32 q (lower part) to nc;
+        // the 8 remote A values of a row fragment are requested together
+        const int rs = (FACT == FACT_GETRF) ? 32 * p + 32 : 32 * q;
+        const int nrf = (nc - rs + 7) / 8;
+        for (int i = warp; i < nrf; i += 8) {
+            const int rb = rs + 8 * i;
+            const bool rowok = rb + g < nc;
+            double av[8];
+#pragma unroll
+            for (int ks = 0; ks < 8; ks++) av[ks] = rowok ? -Wp[(rb + g - lop) * DG_LD + 4 * ks + t4] : 0.0;
+            double c[4][2];
+#pragma unroll
+            for (int cf = 0; cf < 4; cf++)
+#pragma unroll
+                for (int e = 0; e < 2; e++) c[cf][e] = rowok ? Wq[(rb + g - loq) * DG_LD + 8 * cf + 2 * t4 + e] : 0.0;
+#pragma unroll
+            for (int ks = 0; ks < 8; ks++)
+#pragma unroll
+                for (int cf = 0; cf < 4; cf++) dmma884(c[cf][0], c[cf][1], av[ks], Tb[(4 * ks + t4) * DG_LD + 8 * cf + g]);
+#pragma unroll
+            for (int cf = 0; cf < 4; cf++)
+#pragma unroll
+                for (int e = 0; e < 2; e++)
+                    if (rowok) Wq[(rb + g - loq) * DG_LD + 8 * cf + 2 * t4 + e] = c[cf][e];
+        }
+        __syncthreads();
+    };
+
+    // Right looking with lookahead: once panel p is factored, the owner of panel
+    // p + 1 applies p's update to that panel alone and factors it at once, and
+    // only then updates its other panels; every other CTA updates its panels.
+    // The critical path per panel is one panel update and one panel
+    // factorization; no cluster-wide barrier separates the steps.
+    if (rank == 0) factor_panel(0);
+    for (int p = 0; p + 1 < np; p++) {
+        wait_panel(p);
+        int q0 = p + 1 + ((rank - (p + 1)) % DC + DC) % DC;  // this CTA's first panel after p
+        if (q0 == p + 1) {
+            update_panel(p, p + 1);
+            factor_panel(p + 1);
+            q0 += DC;
+        }
+        for (int q = q0; q < np; q += DC) update_panel(p, q);
     }
+    wait_panel(np - 1);  // every panel is final before the write-out and the tail below
     // this CTA's panels are final: write them out
     for (int p = rank; p < np; p += DC) {
         const int lop = dc_lo(p, FACT), nb = min(32, nc - 32 * p);
@@ -2420,7 +2488,7 @@ void launch_diag_large(const DevStruct &s, const int *list, int count, int maxnc
             nsm = 1;
     }
     const long long csm = diag_cluster_smem_bytes(maxnc, FACT);
-    if (maxnc <= DG_MAXNC && maxnc >= DC_MIN_NC && (long long)count * DC <= nsm && csm <= DC_MAX_SMEM)
+    if (maxnc <= DG_MAXNC && maxnc >= DC_MIN_NC && (long long)count * DC <= nsm && csm <= dc_max_smem(FACT))
         k_diag_cluster<T, FACT><<<count * DC, 256, (size_t)csm, st>>>(s, list, L, U, dinv, fp);
     else if (maxnc <= DG_MAXNC)
         k_diag_dmma<T, FACT><<<count, 256, (size_t)diag_dmma_smem_bytes(maxnc), st>>>(s, list, L, U, dinv, fp);

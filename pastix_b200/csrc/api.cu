@@ -50,7 +50,7 @@ template <typename T, int F>
 void launch_update_big(const DevStruct &, const UpdTile *, int, T *, T *, cudaStream_t);
 template <int F>
 void launch_update_tc(const DevStruct &, const UpdTile *, int, float *, float *, const unsigned char *,
-                      const unsigned char *, const int64_t *, int *, cudaStream_t);
+                      const unsigned char *, const int64_t *, int *, int *, cudaStream_t);
 void launch_split(const DevStruct &, const SplitSlab *, int, const float *, const float *, const int64_t *,
                   unsigned char *, int, cudaStream_t);
 long long split_image_bytes(int nc, int st);
@@ -62,7 +62,7 @@ void launch_trinv(const DevStruct &, const int *, int, int, const float *, const
 void launch_split_dense(const DenseSlab *, int, const float *, unsigned char *, cudaStream_t);
 template <int F>
 void launch_trsm_tc(const DevStruct &, const UpdTile *, int, float *, float *, const unsigned char *,
-                    const unsigned char *, const int64_t *, const unsigned char *, const int64_t *, int *,
+                    const unsigned char *, const int64_t *, const unsigned char *, const int64_t *, int *, int *,
                     cudaStream_t);
 template <typename T, int F>
 cudaError_t set_smem_attrs(size_t, size_t, size_t);
@@ -210,6 +210,7 @@ struct Device {
     int fltsize = 0;
     // work
     DBuf<int> counters;      // [0] nbpivots, [1] status
+    DBuf<int> queues;        // tile work-queue heads of the tcgen05 launches, 3 per level, zeroed per factorization
     DBuf<double> crit;       // static pivoting threshold of the current factorization
     DBuf<double> part, scal; // reduction partials, scalars
     DBuf<double> w1, w2;     // permuted double work vectors
@@ -1430,6 +1431,7 @@ static int device_setup(pastix_data_t *pd) {
     CUDA_TRY(d.vals.alloc(std::max<idx_t>(1, pd->nnz)));
     CUDA_TRY(d.csr_val.alloc(std::max<idx_t>(1, pd->csr_nnz)));
     CUDA_TRY(d.counters.alloc(4));
+    CUDA_TRY(d.queues.alloc(std::max<size_t>(1, 3 * pd->levels.size())));
     CUDA_TRY(d.crit.alloc(1));
     CUDA_TRY(cudaMemsetAsync(d.counters.p, 0, 4 * sizeof(int), st));
     CUDA_TRY(d.part.alloc(pgpu::reduce_partials()));
@@ -1475,6 +1477,8 @@ static int run_factor(pastix_data_t *pd, double criterion) {
     // (the profiled pass keeps one stream so that each class's events time it alone)
     const bool two = sizeof(T) == 4 && !pd->prof_on;
     const cudaStream_t sd = two ? d.side : st;
+    if constexpr (sizeof(T) == 4)
+        CUDA_TRY(cudaMemsetAsync(d.queues.p, 0, 3 * pd->levels.size() * sizeof(int), st));
     if (two) {
         CUDA_TRY(cudaEventRecord(d.ev_chain[0], st));
         CUDA_TRY(cudaStreamWaitEvent(d.side, d.ev_chain[0], 0));
@@ -1508,7 +1512,7 @@ static int run_factor(pastix_data_t *pd, double criterion) {
                 pgpu::launch_split(d.ds, sl, cnt, L, L, d.sp_off.p, d.img0.p, 0, st);
                 if (F == pgpu::FACT_GETRF) pgpu::launch_split(d.ds, sl, cnt, U, L, d.sp_off.p, d.img1.p, 0, st);
                 pgpu::launch_trsm_tc<F>(d.ds, d.trsm_tc_tiles.p + lv.tt0, lv.tt1 - lv.tt0, L, U, d.img0.p, d.img1.p,
-                                        d.sp_off.p, d.timg.p, d.ti_img.p, d.counters.p + 1, st);
+                                        d.sp_off.p, d.timg.p, d.ti_img.p, d.queues.p + 3 * l, d.counters.p + 1, st);
             });
             launch_cls(pd, PC_TRSM, lv.tr32_1 - lv.tr32_0, [&] {
                 pgpu::launch_trsm<T, F>(d.ds, d.trsm_tiles32.p + lv.tr32_0, lv.tr32_1 - lv.tr32_0, lv.trsm_maxnc,
@@ -1534,7 +1538,7 @@ static int run_factor(pastix_data_t *pd, double criterion) {
             });
             launch_cls(pd, PC_UPDATE_BIG, lv.updtn - lv.updt0, [&] {
                 pgpu::launch_update_tc<F>(d.ds, d.upd_tc_tiles.p + lv.updt0, lv.updtn - lv.updt0, L, U, d.img0.p,
-                                          d.img1.p, d.sp_off.p, d.counters.p + 1, st);
+                                          d.img1.p, d.sp_off.p, d.queues.p + 3 * l + 1, d.counters.p + 1, st);
             });
             // far targets on the side stream, once this level's panels and images are final
             if (two) {
@@ -1551,7 +1555,8 @@ static int run_factor(pastix_data_t *pd, double criterion) {
                 pd, PC_UPDATE_BIG, lv.updt1 - lv.updtn,
                 [&] {
                     pgpu::launch_update_tc<F>(d.ds, d.upd_tc_tiles.p + lv.updtn, lv.updt1 - lv.updtn, L, U,
-                                              d.img0.p, d.img1.p, d.sp_off.p, d.counters.p + 1, sd);
+                                              d.img0.p, d.img1.p, d.sp_off.p, d.queues.p + 3 * l + 2,
+                                              d.counters.p + 1, sd);
                 },
                 sd);
             if (two) CUDA_TRY(cudaEventRecord(d.ev_rest[l], d.side));

@@ -1654,8 +1654,9 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
     double *Wl = Zs1 + dc_zs1_doubles(FACT);
     __shared__ double Zs0[32 * DG_LD];                   // inverted top block of the panel being factored here
     __shared__ __align__(16) double Sx[8][8 * DG_LD];  // also the published steps of the top block's factorization
-    __shared__ double Tb[32 * DG_LD];                    // the top block being factored / an update's B block
-    __shared__ int npiv, prog, fdone;                    // fdone: 1 + last panel factored by this CTA
+    __shared__ double Tb[32 * DG_LD];                    // the top block being factored
+    __shared__ double Bs[32 * DG_LD];                    // an update's B block
+    __shared__ int npiv, prog, fpart, fdone;             // announcements of this CTA's panels (below)
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
     const int k = list[blockIdx.x / DC];
@@ -1667,6 +1668,7 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
     T *gZ = dinv + s.cb_dinv[k];
     if (tid == 0) {
         npiv = 0;
+        fpart = 0;
         fdone = 0;
     }
     // panel p of CTA p % DC: its offset inside that CTA's shared memory
@@ -1697,13 +1699,42 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
     }
     cluster.sync();  // panels loaded and flags cleared in every CTA before any flag is read
 
-    // Factor panel p (this CTA owns it; every update from panels < p applied):
-    // top block, its inverse(s), the rows below; then announce it.
-    auto factor_panel = [&](int p) {
+    // Each panel is announced in two stages through this CTA's flags: fpart = p + 1
+    // once its factored top block and the rows that form the top block of panel
+    // p + 1 are final, fdone = p + 1 once all its rows are.  The owner of panel
+    // p + 1 starts on its top block at fpart, so the rest of panel p's TRSM and
+    // every other update run beside the critical chain
+    //   rows of p for p + 1's top -> p + 1's top updated -> factored -> ...
+    auto publish = [&](int *flag, int p) {
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("fence.acq_rel.cluster;" ::: "memory");
+            dsmem_st_release(dsmem_map(flag, rank), p + 1);
+        }
+    };
+    // Wait until the owner of panel p has raised `flag` to p + 1 (bounded; on
+    // expiry the status word records PGPU_STATUS_TIMEOUT and the CTA carries on,
+    // so that the kernel ends).
+    auto wait_flag = [&](int *flag, int p) {
+        if (p % DC != rank && tid == 0) {
+            const uint32_t fa = dsmem_map(flag, p % DC);
+            int spins = 0;
+            while (dsmem_ld_acquire(fa) < p + 1) {
+                if (++spins > DG_SPIN) {
+                    atomicExch(fp.status, PGPU_STATUS_TIMEOUT);
+                    break;
+                }
+                __nanosleep(20);
+            }
+        }
+        __syncthreads();
+    };
+    // Top block of this CTA's panel p (every update from panels < p applied to
+    // it): factored by warp 0 with static pivoting, inverted beside it.
+    auto factor_top = [&](int p) {
         const int nb = min(32, nc - 32 * p);
         const int lop = dc_lo(p, FACT);
-        double *W = Wl + poff(p);
-        double *Wt = W + (32 * p - lop) * DG_LD;  // top block
+        double *Wt = Wl + poff(p) + (32 * p - lop) * DG_LD;  // top block
         double *Z1 = (FACT == FACT_GETRF) ? Zs1 + (p / DC) * 32 * DG_LD : Zs1;
         for (int e = tid; e < nb * DG_LD; e += blockDim.x) Tb[e] = Wt[e];  // the panel has nb rows left at its top
         if (tid == 0) prog = 0;
@@ -1719,41 +1750,29 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         __syncthreads();
         for (int e = tid; e < nb * DG_LD; e += blockDim.x) Wt[e] = Tb[e];
         __syncthreads();
-        const int r0 = 32 * p + 32;  // rows below the top block
-        const int nrf = (nc - r0 + 7) / 8;
+    };
+    // Rows [ra, rb) (below the top block) of this CTA's panel p against its
+    // factored top block (still in Tb, inverse in Zs0): X T = A.
+    auto trsm_rows = [&](int p, int ra, int rb) {
+        const int nb = min(32, nc - 32 * p);
+        const int lop = dc_lo(p, FACT);
+        double *W = Wl + poff(p);
+        rb = min(rb, nc);
+        const int nrf = (rb - ra + 7) / 8;
         for (int i = warp; i < nrf; i += 8) {
-            const int rb = r0 + 8 * i;
+            const int r8 = ra + 8 * i;
             dg_solve8(
-                [&](int row, int col) { return (rb + row < nc) ? W[(rb + row - lop) * DG_LD + col] : 0.0; },
+                [&](int row, int col) { return (r8 + row < rb) ? W[(r8 + row - lop) * DG_LD + col] : 0.0; },
                 [&](int a, int b) { return (a <= b && b < nb) ? dg_t<FACT>(Tb, a, b, 0) : 0.0; }, Zs0, Sx[warp],
                 [&](int row, int col, double v) {
-                    if (rb + row < nc) W[(rb + row - lop) * DG_LD + col] = v;
+                    if (r8 + row < rb) W[(r8 + row - lop) * DG_LD + col] = v;
                 });
         }
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("fence.acq_rel.cluster;" ::: "memory");
-            dsmem_st_release(dsmem_map(&fdone, rank), p + 1);
-        }
     };
-    // Wait until panel p is factored (bounded; on expiry the status word records
-    // PGPU_STATUS_TIMEOUT and the CTA carries on, so that the kernel ends).
-    auto wait_panel = [&](int p) {
-        if (p % DC != rank && tid == 0) {
-            const uint32_t fa = dsmem_map(&fdone, p % DC);
-            int spins = 0;
-            while (dsmem_ld_acquire(fa) < p + 1) {
-                if (++spins > DG_SPIN) {
-                    atomicExch(fp.status, PGPU_STATUS_TIMEOUT);
-                    break;
-                }
-                __nanosleep(20);
-            }
-        }
-        __syncthreads();
-    };
-    // Update of this CTA's panel q by the factored panel p (read remotely).
-    auto update_panel = [&](int p, int q) {
+    // Rows [ra, rb) of this CTA's panel q updated by the factored panel p (read
+    // remotely).  GETRF: the call that starts at the first row also forms the
+    // U block U_pq = L_pp^{-1} A_pq that every row's update reads.
+    auto update_rows = [&](int p, int q, int ra, int rb) {
         const int nb = min(32, nc - 32 * p);
         const int lop = dc_lo(p, FACT);
         const double *Wp = panel(p);
@@ -1761,7 +1780,8 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         const int nbq = min(32, nc - 32 * q);
         const int loq = dc_lo(q, FACT);
         double *Wq = Wl + poff(q);
-        if (FACT == FACT_GETRF) {  // U_pq = L_pp^{-1} A_pq, as (U_pq)^T L_pp^T = (A_pq)^T, 8 columns per warp
+        const int rs = (FACT == FACT_GETRF) ? 32 * p + 32 : 32 * q;
+        if (FACT == FACT_GETRF && ra <= rs) {  // (U_pq)^T L_pp^T = (A_pq)^T, 8 columns per warp
             const double *Zr = cluster.map_shared_rank(Zs1 + (p / DC) * 32 * DG_LD, p % DC);
             double *Ab = Wq + (32 * p - loq) * DG_LD;  // rows 32 p .. 32 p + 31 of panel q
             if (warp < 4) {
@@ -1775,9 +1795,15 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
             }
             __syncthreads();
         }
-        // B block of this update (32 x 32: k by the columns of panel q) staged locally
-        for (int e = tid; e < 1024; e += blockDim.x) {
-            const int kk = e >> 5, cc = e & 31;
+        ra = max(ra, rs);
+        rb = min(rb, nc);
+        if (ra >= rb) return;
+        // B block of this update (32 x 32: k by the columns of panel q) staged
+        // locally, every remote load of a thread issued before its stores
+        double bv[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int e = tid + 256 * u, kk = e >> 5, cc = e & 31;
             double b = 0.0;
             if (cc < nbq && kk < nb) {
                 if (FACT == FACT_GETRF) b = Wq[(32 * p + kk - loq) * DG_LD + cc];
@@ -1786,54 +1812,89 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
                     if (FACT == FACT_SYTRF) b *= Wpt[kk * DG_LD + kk];
                 }
             }
-            Tb[kk * DG_LD + cc] = b;
+            bv[u] = b;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int e = tid + 256 * u;
+            Bs[(e >> 5) * DG_LD + (e & 31)] = bv[u];
         }
         __syncthreads();
-        // trailing rows of panel q: rows from 32 p + 32 (GETRF) or 32 q (lower part) to nc;
-        // the 8 remote A values of a row fragment are requested together
-        const int rs = (FACT == FACT_GETRF) ? 32 * p + 32 : 32 * q;
-        const int nrf = (nc - rs + 7) / 8;
-        for (int i = warp; i < nrf; i += 8) {
-            const int rb = rs + 8 * i;
-            const bool rowok = rb + g < nc;
-            double av[8];
+        // two 8-row fragments per warp at a time: their 16 remote A values are
+        // requested together and their DMMA chains interleave
+        const int nrf = (rb - ra + 7) / 8;
+        for (int i = warp; i < nrf; i += 16) {
+            double av[2][8], c[2][4][2];
+            bool rowok[2];
 #pragma unroll
-            for (int ks = 0; ks < 8; ks++) av[ks] = rowok ? -Wp[(rb + g - lop) * DG_LD + 4 * ks + t4] : 0.0;
-            double c[4][2];
+            for (int f = 0; f < 2; f++) {
+                const int r = ra + 8 * (i + 8 * f) + g;
+                rowok[f] = (i + 8 * f < nrf) && r < rb;
 #pragma unroll
-            for (int cf = 0; cf < 4; cf++)
+                for (int ks = 0; ks < 8; ks++) av[f][ks] = rowok[f] ? -Wp[(r - lop) * DG_LD + 4 * ks + t4] : 0.0;
 #pragma unroll
-                for (int e = 0; e < 2; e++) c[cf][e] = rowok ? Wq[(rb + g - loq) * DG_LD + 8 * cf + 2 * t4 + e] : 0.0;
+                for (int cf = 0; cf < 4; cf++)
+#pragma unroll
+                    for (int e = 0; e < 2; e++)
+                        c[f][cf][e] = rowok[f] ? Wq[(r - loq) * DG_LD + 8 * cf + 2 * t4 + e] : 0.0;
+            }
 #pragma unroll
             for (int ks = 0; ks < 8; ks++)
 #pragma unroll
-                for (int cf = 0; cf < 4; cf++) dmma884(c[cf][0], c[cf][1], av[ks], Tb[(4 * ks + t4) * DG_LD + 8 * cf + g]);
+                for (int cf = 0; cf < 4; cf++) {
+                    const double bb = Bs[(4 * ks + t4) * DG_LD + 8 * cf + g];
 #pragma unroll
-            for (int cf = 0; cf < 4; cf++)
+                    for (int f = 0; f < 2; f++) dmma884(c[f][cf][0], c[f][cf][1], av[f][ks], bb);
+                }
 #pragma unroll
-                for (int e = 0; e < 2; e++)
-                    if (rowok) Wq[(rb + g - loq) * DG_LD + 8 * cf + 2 * t4 + e] = c[cf][e];
+            for (int f = 0; f < 2; f++) {
+                const int r = ra + 8 * (i + 8 * f) + g;
+#pragma unroll
+                for (int cf = 0; cf < 4; cf++)
+#pragma unroll
+                    for (int e = 0; e < 2; e++)
+                        if (rowok[f]) Wq[(r - loq) * DG_LD + 8 * cf + 2 * t4 + e] = c[f][cf][e];
+            }
         }
         __syncthreads();
     };
+    // Rows of panel p after its top block: first those that form the top block
+    // of panel p + 1, announced at once, then the others.
+    auto finish_panel = [&](int p) {
+        const int r0 = 32 * p + 32;
+        trsm_rows(p, r0, r0 + 32);
+        publish(&fpart, p);
+        trsm_rows(p, r0 + 32, nc);
+        publish(&fdone, p);
+    };
 
-    // Right looking with lookahead: once panel p is factored, the owner of panel
-    // p + 1 applies p's update to that panel alone and factors it at once, and
-    // only then updates its other panels; every other CTA updates its panels.
-    // The critical path per panel is one panel update and one panel
-    // factorization; no cluster-wide barrier separates the steps.
-    if (rank == 0) factor_panel(0);
-    for (int p = 0; p + 1 < np; p++) {
-        wait_panel(p);
-        int q0 = p + 1 + ((rank - (p + 1)) % DC + DC) % DC;  // this CTA's first panel after p
-        if (q0 == p + 1) {
-            update_panel(p, p + 1);
-            factor_panel(p + 1);
-            q0 += DC;
-        }
-        for (int q = q0; q < np; q += DC) update_panel(p, q);
+    if (rank == 0) {
+        factor_top(0);
+        finish_panel(0);
     }
-    wait_panel(np - 1);  // every panel is final before the write-out and the tail below
+    for (int p = 0; p + 1 < np; p++) {
+        const int q1 = p + 1;
+        int q0 = q1 + ((rank - q1) % DC + DC) % DC;  // this CTA's first panel after p
+        if (q0 == q1) {
+            // the critical chain: p + 1's top block as soon as the rows it needs are final
+            wait_flag(&fpart, p);
+            update_rows(p, q1, 0, 32 * q1 + 32);
+            factor_top(q1);
+            wait_flag(&fdone, p);
+            update_rows(p, q1, 32 * q1 + 32, 32 * q1 + 64);  // the rows of p + 2's top block
+            const int r0 = 32 * q1 + 32;
+            trsm_rows(q1, r0, r0 + 32);
+            publish(&fpart, q1);
+            update_rows(p, q1, 32 * q1 + 64, nc);
+            trsm_rows(q1, r0 + 32, nc);
+            publish(&fdone, q1);
+            q0 += DC;
+        } else {
+            wait_flag(&fdone, p);
+        }
+        for (int q = q0; q < np; q += DC) update_rows(p, q, 0, nc);
+    }
+    wait_flag(&fdone, np - 1);  // every panel is final before the write-out and the tail below
     // this CTA's panels are final: write them out
     for (int p = rank; p < np; p += DC) {
         const int lop = dc_lo(p, FACT), nb = min(32, nc - 32 * p);
@@ -2208,13 +2269,22 @@ __device__ __forceinline__ int epi_bar_or(int pred) {
     return r;
 }
 
+constexpr int TQ = 4;  // tile-index ring between the producer and the other roles
+
+// The persistent tile engine.  Tiles come from a device work queue: the
+// producer claims the next tile index with an atomic on *queue (zeroed before
+// the launch) and hands it to the MMA issuer and the epilogue warps through a
+// ring of TQ slots guarded by mbarriers; an index past `count` ends every
+// role.  CTAs that draw cheap tiles simply draw more, so uneven tile costs
+// (source widths, masked rows) do not leave SMs idle at the end of a launch.
 template <typename Setup, typename RowInfo, typename ColInfo, typename Epi>
-__device__ __forceinline__ void tc_persistent(int count, int *status, Setup setup, RowInfo rowinfo, ColInfo colinfo,
-                                              Epi epi) {
+__device__ __forceinline__ void tc_persistent(int count, int *queue, int *status, Setup setup, RowInfo rowinfo,
+                                              ColInfo colinfo, Epi epi) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full[TP_STAGES], empty[TP_STAGES], tfull[2], tempty[2];
+    __shared__ __align__(8) uint64_t full[TP_STAGES], empty[TP_STAGES], tfull[2], tempty[2], tq_full[TQ], tq_empty[TQ];
     __shared__ uint32_t tmem_sh;
     __shared__ int ctab[2][TC_BN];
+    __shared__ int tq[TQ];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (warp == 5) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
@@ -2230,6 +2300,10 @@ __device__ __forceinline__ void tc_persistent(int count, int *status, Setup setu
             mbar_init(&tfull[i], 1);
             mbar_init(&tempty[i], 4 * 32);
         }
+        for (int i = 0; i < TQ; i++) {
+            mbar_init(&tq_full[i], 1);
+            mbar_init(&tq_empty[i], 1 + 4 * 32);  // the MMA issuer and the 128 epilogue threads
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -2238,9 +2312,19 @@ __device__ __forceinline__ void tc_persistent(int count, int *status, Setup setu
     const uint32_t tmem = tmem_sh;
     int late = 0;
     if (warp == 4) {
-        if (lane == 0) {  // producer
+        if (lane == 0) {  // producer: claims tiles, loads their operands
             uint32_t g = 0;
-            for (int t = blockIdx.x; t < count && !late; t += gridDim.x) {
+            for (int j = 0; !late; j++) {
+                const int slot = j % TQ;
+                if (j >= TQ && !mbar_wait(&tq_empty[slot], ((j / TQ) - 1) & 1)) {
+                    late = 1;
+                    break;
+                }
+                int t = atomicAdd(queue, 1);
+                if (t >= count) t = -1;
+                tq[slot] = t;
+                mbar_arrive(&tq_full[slot]);
+                if (t < 0) break;
                 TcOperands op;
                 setup(t, op);
                 const uint32_t bbytes = (uint32_t)(op.nmma / 8) * TC_GROUP;
@@ -2266,8 +2350,15 @@ __device__ __forceinline__ void tc_persistent(int count, int *status, Setup setu
         if (lane == 0) {  // MMA issuer
             const uint32_t sbase = smem_u32(smem_raw);
             uint32_t g = 0;
-            int i = 0;
-            for (int t = blockIdx.x; t < count && !late; t += gridDim.x, i++) {
+            for (int i = 0; !late; i++) {
+                const int slot = i % TQ;
+                if (!mbar_wait(&tq_full[slot], (i / TQ) & 1)) {
+                    late = 1;
+                    break;
+                }
+                const int t = tq[slot];
+                mbar_arrive(&tq_empty[slot]);
+                if (t < 0) break;
                 TcOperands op;
                 setup(t, op);
                 const int b = i & 1;
@@ -2303,8 +2394,16 @@ __device__ __forceinline__ void tc_persistent(int count, int *status, Setup setu
             }
         }
     } else {  // epilogue warps 0-3: tile row = tid, tensor-memory lanes 32 warp .. 32 warp + 31
-        int i = 0;
-        for (int t = blockIdx.x; t < count; t += gridDim.x, i++) {
+        for (int i = 0;; i++) {
+            const int slot = i % TQ;
+            const int qfail = epi_bar_or(!mbar_wait(&tq_full[slot], (i / TQ) & 1));
+            if (qfail) {
+                late = 1;
+                break;
+            }
+            const int t = tq[slot];
+            mbar_arrive(&tq_empty[slot]);
+            if (t < 0) break;
             TcOperands op;
             setup(t, op);
             const int b = i & 1;
@@ -2338,7 +2437,8 @@ template <int FACT>
 __global__ void __launch_bounds__(TP_THREADS, 2) k_update_tcp(DevStruct s, const UpdTile *__restrict__ tiles,
                                                                int count, float *L, float *U,
                                                                const unsigned char *img0, const unsigned char *img1,
-                                                               const int64_t *__restrict__ sp_off, int *status) {
+                                                               const int64_t *__restrict__ sp_off, int *queue,
+                                                               int *status) {
     if (*(volatile int *)status != 0) return;
     auto setup = [&](int t, TcOperands &op) {
         const UpdTile tl = tiles[t];
@@ -2394,7 +2494,7 @@ __global__ void __launch_bounds__(TP_THREADS, 2) k_update_tcp(DevStruct s, const
             if (cc >= 0) atomicAdd(Cp + (size_t)cc * stf, -v[j]);  // reduction without return
         }
     };
-    tc_persistent(count, status, setup, rowinfo, colinfo, epi);
+    tc_persistent(count, queue, status, setup, rowinfo, colinfo, epi);
 }
 
 template <int FACT>
@@ -2403,7 +2503,8 @@ __global__ void __launch_bounds__(TP_THREADS, 2) k_trsm_tcp(DevStruct s, const U
                                                              const unsigned char *img1,
                                                              const int64_t *__restrict__ sp_off,
                                                              const unsigned char *timg,
-                                                             const int64_t *__restrict__ ti_img, int *status) {
+                                                             const int64_t *__restrict__ ti_img, int *queue,
+                                                             int *status) {
     if (*(volatile int *)status != 0) return;
     auto setup = [&](int t, TcOperands &op) {
         const UpdTile tl = tiles[t];
@@ -2446,7 +2547,7 @@ __global__ void __launch_bounds__(TP_THREADS, 2) k_trsm_tcp(DevStruct s, const U
             if (c >= 0) P[(size_t)c * st] = v[j];
         }
     };
-    tc_persistent(count, status, setup, rowinfo, colinfo, epi);
+    tc_persistent(count, queue, status, setup, rowinfo, colinfo, epi);
 }
 
 // ---------------------------------------------------------------------------
@@ -2526,11 +2627,11 @@ void launch_update_big(const DevStruct &s, const UpdTile *tiles, int count, T *L
 // FP32 updates of 128 x 128 tiles on tcgen05 from the split BF16 images
 template <int FACT>
 void launch_update_tc(const DevStruct &s, const UpdTile *tiles, int count, float *L, float *U,
-                      const unsigned char *img0, const unsigned char *img1, const int64_t *sp_off, int *status,
-                      cudaStream_t st) {
+                      const unsigned char *img0, const unsigned char *img1, const int64_t *sp_off, int *queue,
+                      int *status, cudaStream_t st) {
     if (count <= 0) return;
     const int grid = std::min(count, 2 * sm_count());
-    k_update_tcp<FACT><<<grid, TP_THREADS, TP_SMEM, st>>>(s, tiles, count, L, U, img0, img1, sp_off, status);
+    k_update_tcp<FACT><<<grid, TP_THREADS, TP_SMEM, st>>>(s, tiles, count, L, U, img0, img1, sp_off, queue, status);
 }
 
 template <int FACT>
@@ -2550,11 +2651,11 @@ void launch_split_dense(const DenseSlab *slabs, int count, const float *src, uns
 template <int FACT>
 void launch_trsm_tc(const DevStruct &s, const UpdTile *tiles, int count, float *L, float *U,
                     const unsigned char *img0, const unsigned char *img1, const int64_t *sp_off,
-                    const unsigned char *timg, const int64_t *ti_img, int *status, cudaStream_t st) {
+                    const unsigned char *timg, const int64_t *ti_img, int *queue, int *status, cudaStream_t st) {
     if (count <= 0) return;
     const int grid = std::min(count, 2 * sm_count());
     k_trsm_tcp<FACT><<<grid, TP_THREADS, TP_SMEM, st>>>(s, tiles, count, L, U, img0, img1, sp_off, timg, ti_img,
-                                                         status);
+                                                         queue, status);
 }
 
 void launch_split(const DevStruct &s, const SplitSlab *slabs, int count, const float *P, const float *D,
@@ -2623,26 +2724,26 @@ template void launch_trinv<FACT_POTRF>(const DevStruct &, const int *, int, int,
                                       const float *, const int64_t *, float *, cudaStream_t);
 template void launch_trsm_tc<FACT_POTRF>(const DevStruct &, const UpdTile *, int, float *, float *, const unsigned char *,
                                         const unsigned char *, const int64_t *, const unsigned char *,
-                                        const int64_t *, int *, cudaStream_t);
+                                        const int64_t *, int *, int *, cudaStream_t);
 template void launch_update_tc<FACT_POTRF>(const DevStruct &, const UpdTile *, int, float *, float *,
                                            const unsigned char *, const unsigned char *, const int64_t *, int *,
-                                           cudaStream_t);
+                                           int *, cudaStream_t);
 template void launch_trinv<FACT_SYTRF>(const DevStruct &, const int *, int, int, const float *, const float *,
                                       const float *, const int64_t *, float *, cudaStream_t);
 template void launch_trsm_tc<FACT_SYTRF>(const DevStruct &, const UpdTile *, int, float *, float *, const unsigned char *,
                                         const unsigned char *, const int64_t *, const unsigned char *,
-                                        const int64_t *, int *, cudaStream_t);
+                                        const int64_t *, int *, int *, cudaStream_t);
 template void launch_update_tc<FACT_SYTRF>(const DevStruct &, const UpdTile *, int, float *, float *,
                                            const unsigned char *, const unsigned char *, const int64_t *, int *,
-                                           cudaStream_t);
+                                           int *, cudaStream_t);
 template void launch_trinv<FACT_GETRF>(const DevStruct &, const int *, int, int, const float *, const float *,
                                       const float *, const int64_t *, float *, cudaStream_t);
 template void launch_trsm_tc<FACT_GETRF>(const DevStruct &, const UpdTile *, int, float *, float *, const unsigned char *,
                                         const unsigned char *, const int64_t *, const unsigned char *,
-                                        const int64_t *, int *, cudaStream_t);
+                                        const int64_t *, int *, int *, cudaStream_t);
 template void launch_update_tc<FACT_GETRF>(const DevStruct &, const UpdTile *, int, float *, float *,
                                            const unsigned char *, const unsigned char *, const int64_t *, int *,
-                                           cudaStream_t);
+                                           int *, cudaStream_t);
 template void launch_fill_coef<double>(int64_t, const double *, const int64_t *, const int64_t *, double *,
                                        double *, cudaStream_t);
 template void launch_fill_coef<float>(int64_t, const double *, const int64_t *, const int64_t *, float *,

@@ -1780,6 +1780,7 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         const int nbq = min(32, nc - 32 * q);
         const int loq = dc_lo(q, FACT);
         double *Wq = Wl + poff(q);
+        if (q >= np) return;  // (uniform) no such panel
         const int rs = (FACT == FACT_GETRF) ? 32 * p + 32 : 32 * q;
         if (FACT == FACT_GETRF && ra <= rs) {  // (U_pq)^T L_pp^T = (A_pq)^T, 8 columns per warp
             const double *Zr = cluster.map_shared_rank(Zs1 + (p / DC) * 32 * DG_LD, p % DC);

@@ -3,8 +3,9 @@
 Bars: static-pivot counts equal; FP64 factors within 1e-12 relative Frobenius
 of the oracle's (both stored in the same panel layout); solutions to backward
 error <= 1e-14.  The shifted indefinite elastic matrix factored by LDL^T
-without pivoting has element growth max|L| ~ 1.4e3 and the oracle's own factor
-differs from an extended-precision LDL^T by 3e-13, so its bar is 5e-12.
+without pivoting has element growth max|L| ~ 1.4e3: two CPU codes (the
+reference and the oracle's restatement) already differ by up to 4e-12 on it,
+so its bar is 1e-11.
 """
 from __future__ import annotations
 
@@ -24,7 +25,7 @@ CASES = [
     ("cd64", "GETRF", True),
     ("el48", "SYTRF", True),
 ]
-TOL = {"el48": 5e-12}
+TOL = {"el48": 1e-11}
 
 
 def _mask_compare(fact, info):

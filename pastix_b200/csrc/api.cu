@@ -85,6 +85,9 @@ template <typename T>
 void launch_diag_scale(const DevStruct &, int, const T *, T *, int, int, cudaStream_t);
 int solve_rows_per_tile();
 // vec.cu
+void spmv_partition(int n, const int *rowptr, std::vector<int> &part);
+void launch_spmv_stream(int nblocks, const int *part, const int *rowptr, const int *col, const double *val,
+                        double alpha, const double *x, double beta, double *y, cudaStream_t st);
 void launch_spmv(int, int64_t, const int *, const int *, const double *, double, const double *, double, double *,
                  cudaStream_t);
 int reduce_partials();
@@ -205,6 +208,8 @@ struct Device {
     DBuf<double> vals, csr_val;
     DBuf<int64_t> lmap, umap, csr_src, perm;
     DBuf<int> csr_rowptr, csr_col, e_row, e_col;
+    DBuf<int> spmv_part;     // row blocks of the streamed SpMV
+    int spmv_nblocks = 0;
     // factor
     DBuf<unsigned char> Lc, Uc, dinv;  // panels; inverted 32x32 diagonal sub-blocks of wide cblks
     int fltsize = 0;
@@ -1423,6 +1428,12 @@ static int device_setup(pastix_data_t *pd) {
     else d.umap.reset();
     CUDA_TRY(d.csr_src.upload(pd->csr_src, st));
     CUDA_TRY(d.csr_rowptr.upload(pd->csr_rowptr, st));
+    {
+        std::vector<int> part;
+        pgpu::spmv_partition((int)pd->n, pd->csr_rowptr.data(), part);
+        d.spmv_nblocks = (int)part.size() - 1;
+        CUDA_TRY(d.spmv_part.upload(part, st));
+    }
     CUDA_TRY(d.csr_col.upload(pd->csr_col, st));
     CUDA_TRY(d.e_row.upload(pd->e_row, st));
     CUDA_TRY(d.e_col.upload(pd->e_col, st));
@@ -2137,8 +2148,8 @@ struct Refiner {
     }
     void spmv(double alpha, const double *x, double beta, double *y) {
         launch_cls(pd, PC_SPMV, 1, [&] {
-            pgpu::launch_spmv((int)n, pd->csr_nnz, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha, x, beta, y,
-                              d.stream);
+            pgpu::launch_spmv_stream(d.spmv_nblocks, d.spmv_part.p, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha,
+                                     x, beta, y, d.stream);
         });
     }
     void copy(const double *a, double *b) { cudaMemcpyAsync(b, a, n * 8, cudaMemcpyDeviceToDevice, d.stream); }
@@ -2712,7 +2723,8 @@ extern "C" int pgpu_spmv_device(pastix_data_t *pd, double alpha, const double *x
     cudaStream_t st = (cudaStream_t)stream;     // the caller's stream; NULL = legacy default stream
     pgpu::launch_permute<double, double>((int)pd->n, 1, d.perm.p, 1, x, pd->n, d.w1.p, pd->n, st);
     pgpu::launch_permute<double, double>((int)pd->n, 1, d.perm.p, 1, y, pd->n, d.w2.p, pd->n, st);
-    pgpu::launch_spmv((int)pd->n, pd->csr_nnz, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha, d.w1.p, beta, d.w2.p, st);
+    pgpu::launch_spmv_stream(d.spmv_nblocks, d.spmv_part.p, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha, d.w1.p,
+                             beta, d.w2.p, st);
     pgpu::launch_permute<double, double>((int)pd->n, 1, d.perm.p, 0, d.w2.p, pd->n, y, pd->n, st);
     CUDA_TRY(cudaGetLastError());
     return PASTIX_SUCCESS;

@@ -2315,14 +2315,18 @@ __device__ __forceinline__ void tc_persistent(int count, int *queue, int *status
     if (warp == 4) {
         if (lane == 0) {  // producer: claims tiles, loads their operands
             uint32_t g = 0;
+            // the claim of the next tile is issued one tile ahead, so that its
+            // round trip to L2 overlaps this tile's copies
+            int next = atomicAdd(queue, 1);
             for (int j = 0; !late; j++) {
                 const int slot = j % TQ;
                 if (j >= TQ && !mbar_wait(&tq_empty[slot], ((j / TQ) - 1) & 1)) {
                     late = 1;
                     break;
                 }
-                int t = atomicAdd(queue, 1);
+                int t = next;
                 if (t >= count) t = -1;
+                else next = atomicAdd(queue, 1);
                 tq[slot] = t;
                 mbar_arrive(&tq_full[slot]);
                 if (t < 0) break;

@@ -16,6 +16,7 @@
 #include <cstdint>
 
 #include <algorithm>
+#include <vector>
 
 namespace pgpu {
 
@@ -34,6 +35,46 @@ __global__ void k_spmv(int n, const int *__restrict__ rowptr, const int *__restr
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, G);
     if (lane == 0 && gid < n) y[gid] = alpha * acc + (beta == 0.0 ? 0.0 : beta * y[gid]);
+}
+
+// SpMV by row blocks of at most SPMV_ROWS rows and SPMV_CAP stored entries
+// (partition `part`, built once on the host by spmv_partition): the block's
+// products val[p] * x[col[p]] are formed with fully coalesced loads of val and
+// col into shared memory, then each thread sums one row of them.  A row longer
+// than SPMV_CAP gets a block of its own, reduced by the whole block.
+constexpr int SPMV_ROWS = 256, SPMV_CAP = 2304;
+__global__ void __launch_bounds__(256) k_spmv_stream(const int *__restrict__ part, const int *__restrict__ rowptr,
+                                                     const int *__restrict__ col, const double *__restrict__ val,
+                                                     double alpha, const double *__restrict__ x, double beta,
+                                                     double *__restrict__ y) {
+    __shared__ double prod[SPMV_CAP];
+    __shared__ double red[8];
+    const int r0 = part[blockIdx.x], r1 = part[blockIdx.x + 1];
+    const int p0 = rowptr[r0], p1 = rowptr[r1];
+    const int tid = threadIdx.x;
+    if (p1 - p0 <= SPMV_CAP) {
+#pragma unroll 3
+        for (int p = p0 + tid; p < p1; p += 256) prod[p - p0] = val[p] * x[col[p]];
+        __syncthreads();
+        const int r = r0 + tid;
+        if (r < r1) {
+            const int b = rowptr[r] - p0, e = rowptr[r + 1] - p0;
+            double acc = 0.0;
+            for (int q = b; q < e; q++) acc += prod[q];
+            y[r] = alpha * acc + (beta == 0.0 ? 0.0 : beta * y[r]);
+        }
+    } else {  // one long row
+        double acc = 0.0;
+        for (int p = p0 + tid; p < p1; p += 256) acc += val[p] * x[col[p]];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if ((tid & 31) == 0) red[tid >> 5] = acc;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < 8; w++) t += red[w];
+            y[r0] = alpha * t + (beta == 0.0 ? 0.0 : beta * y[r0]);
+        }
+    }
 }
 
 constexpr int RED_THREADS = 256;
@@ -269,6 +310,23 @@ void launch_xpby_cols(int64_t n, int nb, const double *Z, const double *beta, do
 void launch_gemv_cols(int64_t n, int nb, int m, const double *W, int64_t sW, const double *y, double *X, int64_t ldx,
                       cudaStream_t st) {
     if (nb > 0 && m > 0) k_gemv_cols<<<cols_grid(n, nb), 256, 0, st>>>(n, nb, m, W, sW, y, X, ldx);
+}
+
+// Row blocks of k_spmv_stream: consecutive rows, at most SPMV_ROWS of them and
+// SPMV_CAP entries, a longer row alone.  part[0] = 0, part[nblocks] = n.
+void spmv_partition(int n, const int *rowptr, std::vector<int> &part) {
+    part.assign(1, 0);
+    int r = 0;
+    while (r < n) {
+        int e = r + 1;
+        while (e < n && e - r < SPMV_ROWS && rowptr[e + 1] - rowptr[r] <= SPMV_CAP) e++;
+        part.push_back(e);
+        r = e;
+    }
+}
+void launch_spmv_stream(int nblocks, const int *part, const int *rowptr, const int *col, const double *val,
+                        double alpha, const double *x, double beta, double *y, cudaStream_t st) {
+    if (nblocks > 0) k_spmv_stream<<<nblocks, 256, 0, st>>>(part, rowptr, col, val, alpha, x, beta, y);
 }
 
 void launch_spmv(int n, int64_t nnz, const int *rowptr, const int *col, const double *val, double alpha,

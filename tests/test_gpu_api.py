@@ -13,6 +13,7 @@ from conftest import analyse, backward_error
 from pastix_b200 import _lib, gen
 from pastix_b200 import pastix as px
 from pastix_b200._lib import PDBL, PINT
+from pastix_b200.spm import mtxtype, spmatrix
 
 pytestmark = pytest.mark.gpu
 
@@ -100,6 +101,33 @@ def test_device_spmv(lib):
     px.spmv_device(pd, 2.0, xd, -0.5, yd)
     torch.cuda.synchronize()
     ref = 2.0 * (S.full() @ x) - 0.5 * y
+    assert np.linalg.norm(yd.cpu().numpy() - ref) <= 1e-13 * np.linalg.norm(ref)
+
+
+def test_device_spmv_long_row(lib):
+    """A row longer than the streamed SpMV's per-block capacity (an arrow
+    matrix: one node coupled to every other) goes through the one-row blocks."""
+    import scipy.sparse as sps
+    n = 6000
+    A = sps.lil_matrix((n, n))
+    A.setdiag(4.0 * n)
+    A[0, 1:] = 1.0
+    A[1:, 0] = 1.0
+    A = sps.csc_matrix(A)
+    ip, dp = px.initParam()
+    ip[px.iparm.factorization] = px.factotype.POTRF
+    pd = px.init(ip, dp)
+    S = spmatrix(A, mtxtype.Symmetric)
+    px.task_analyze(pd, S)
+    px.task_numfact(pd, S)
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(n)
+    y = rng.standard_normal(n)
+    xd = torch.tensor(x, device="cuda")
+    yd = torch.tensor(y, device="cuda")
+    px.spmv_device(pd, 1.5, xd, 0.25, yd)
+    torch.cuda.synchronize()
+    ref = 1.5 * (A @ x) + 0.25 * y
     assert np.linalg.norm(yd.cpu().numpy() - ref) <= 1e-13 * np.linalg.norm(ref)
 
 

@@ -141,3 +141,48 @@ def test_fp32_factors_match_reference_fp32(lib, ref_mod, name, fact):
     pd, S, info = analyse(A, grid, fact, mixed=True)
     px.task_numfact(pd, S)
     _check_factors(r, pd, fact, 2e-6)
+
+
+@pytest.mark.parametrize("name,fact,refine,magn,mixed", [
+    ("orsirr", "GETRF", 0, 0.0, False),    # GMRES (example/CTestLists.txt:121)
+    ("orsirr", "GETRF", 3, 0.0, False),    # BiCGStab
+    ("small", "SYTRF", 1, 1e-14, False),   # CG with magnitude control 1e-14 (:117, :147)
+    ("orsirr", "GETRF", 0, 0.0, True),     # FP32 factors + FP64 GMRES (IPARM_MIXED)
+])
+def test_refinement_matches_reference(lib, ref_mod, name, fact, refine, magn, mixed):
+    """pastix_task_solve + pastix_task_refine on the reference's own analysis:
+    both reach the reference's stopping test ||b - Ax|| / ||b|| <= 1e-12
+    (refinement/z_refine_gmres.c:164-172) and take the same number of Krylov
+    iterations, within one (the factors agree to rounding, so the residual
+    histories agree until the last digits)."""
+    A, _ = fixture_matrix(name)
+    r = ref_mod.RefPastix(A, fact, nthreads=NTHREADS, magn_ctrl=magn, mixed=mixed)
+    r.iparm[ref_mod.IPARM_REFINEMENT] = refine
+    r.dparm[ref_mod.DPARM_EPSILON_REFINEMENT] = 1e-12
+    r.analyze(perm=_product_perm(A, fact))
+    r.numfact()
+    n = A.shape[0]
+    rng = np.random.default_rng(9)
+    b = A @ rng.uniform(-1, 1, n)
+    xr = r.refine(b, r.solve(b))[:, 0]
+    it_ref = int(r.iparm[ref_mod.IPARM_NBITER])
+
+    s = r.structure()
+    ip, dp = px.initParam()
+    ip[px.iparm.factorization] = FACT_ID[fact]
+    ip[px.iparm.refinement] = refine
+    ip[px.iparm.mixed] = 1 if mixed else 0
+    dp[px.dparm.epsilon_magn_ctrl] = magn
+    dp[px.dparm.epsilon_refinement] = 1e-12
+    pd = px.init(ip, dp)
+    S = spmatrix(A, mtxtype.General if fact == "GETRF" else mtxtype.Symmetric)
+    px.set_symbol(pd, S, s["permtab"], s["cb_fcol"], s["cb_lcol"], s["cb_fblok"], s["bk_frow"], s["bk_lrow"],
+                  s["bk_fcblk"])
+    px.task_numfact(pd, S)
+    x = b.copy()
+    px.task_solve(pd, S, x)
+    px.task_refine(pd, S, b, x)
+    it_gpu = int(pd.iparm[px.iparm.nbiter])
+    for xx in (xr, x):
+        assert np.linalg.norm(b - A @ xx) <= 1e-12 * np.linalg.norm(b)
+    assert abs(it_gpu - it_ref) <= 1, (it_gpu, it_ref)

@@ -2723,8 +2723,10 @@ extern "C" int pgpu_spmv_device(pastix_data_t *pd, double alpha, const double *x
     cudaStream_t st = (cudaStream_t)stream;     // the caller's stream; NULL = legacy default stream
     pgpu::launch_permute<double, double>((int)pd->n, 1, d.perm.p, 1, x, pd->n, d.w1.p, pd->n, st);
     pgpu::launch_permute<double, double>((int)pd->n, 1, d.perm.p, 1, y, pd->n, d.w2.p, pd->n, st);
-    pgpu::launch_spmv_stream(d.spmv_nblocks, d.spmv_part.p, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha, d.w1.p,
-                             beta, d.w2.p, st);
+    launch_cls(pd, PC_SPMV, 1, [&] {
+        pgpu::launch_spmv_stream(d.spmv_nblocks, d.spmv_part.p, d.csr_rowptr.p, d.csr_col.p, d.csr_val.p, alpha,
+                                 d.w1.p, beta, d.w2.p, st);
+    }, st ? st : cudaStreamLegacy);
     pgpu::launch_permute<double, double>((int)pd->n, 1, d.perm.p, 0, d.w2.p, pd->n, y, pd->n, st);
     CUDA_TRY(cudaGetLastError());
     return PASTIX_SUCCESS;

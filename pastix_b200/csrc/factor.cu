@@ -2111,21 +2111,40 @@ struct TcOperands {
 // of T^{-1}) in FP32, ready to be split into the BF16 operand image.
 // ---------------------------------------------------------------------------
 // Dynamic shared memory of k_trinv for blocks of up to maxnzb 32-column blocks:
-// the block column of T^{-1} (FP64) and one block row of T (FP32).
+// the block column of T^{-1} (FP64) and two buffers, each with one block row
+// of T and one inverted diagonal block Z_i (FP32).
+constexpr int TI_ZLD = 36;  // row stride of Z_i (floats): conflict-free fragment loads
 __host__ __device__ inline int ti_ts_ld(int maxnzb) { return 32 * maxnzb + 4; }
 __host__ __device__ inline long long trinv_smem_bytes(int maxnzb) {
-    return 32LL * maxnzb * DG_LD * 8 + 32LL * ti_ts_ld(maxnzb) * 4;
+    return 32LL * maxnzb * DG_LD * 8 + 2 * 32LL * (ti_ts_ld(maxnzb) + TI_ZLD) * 4;
 }
 
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem, bool valid) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    int sz = valid ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz));
+}
+
+// T^{-1} of the diagonal block of a cblk, one 32-column block column j per
+// CTA, by the backward recurrence Y_j = Z_j, Y_i = -Z_i (T_{i, i+1..j}
+// Y_{i+1..j}) over the inverted 32 x 32 diagonal blocks Z_i.  The copies of
+// block row i - 1 of T and of Z_{i-1} (cp.async, two buffers) are in flight
+// while block row i is computed: the recurrence is latency-bound and the
+// loads, not the DMMA, would otherwise set its pace.  Off the diagonal T is a
+// plain copy of the factor (T(a, b) = L(b, a); the LU's U(a, b) on the L
+// side), scaled by d_a for LDL^T -- a factor of the row, applied to the
+// accumulated row of T Y.
 template <typename T, int FACT>
 __global__ void __launch_bounds__(256, 1) k_trinv(DevStruct s, const int *__restrict__ list, const T *L, const T *U,
                                                    const T *__restrict__ dinv, const int64_t *__restrict__ ti_off,
                                                    float *tinv, int maxnzb) {
+    static_assert(sizeof(T) == 4, "k_trinv stages FP32 factors");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *Yb = reinterpret_cast<double *>(smem_raw);       // rows 0 .. 32 j + 31 of the block column, ld DG_LD
-    float *Ts = reinterpret_cast<float *>(Yb + 32 * maxnzb * DG_LD);  // block row i of T, ld ti_ts_ld
     const int tld = ti_ts_ld(maxnzb);
-    __shared__ double Zs[32 * DG_LD], Ss[32 * DG_LD];
+    float *Ts = reinterpret_cast<float *>(Yb + 32 * maxnzb * DG_LD);  // 2 x block row i of T, ld tld
+    float *Zf = Ts + 2 * 32 * tld;                                     // 2 x Z_i, ld TI_ZLD
+    __shared__ double Ss[32 * DG_LD];
     const int k = list[blockIdx.x];
     const int j = blockIdx.y;
     const int side = blockIdx.z;
@@ -2133,42 +2152,71 @@ __global__ void __launch_bounds__(256, 1) k_trinv(DevStruct s, const int *__rest
     const int st = s.cb_stride[k];
     const int nzb = (nc + 31) / 32;
     if (j >= nzb || ti_off[k] < 0) return;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
     const T *D = L + s.cb_coef[k];
     const T *gZ = dinv + s.cb_dinv[k] + (size_t)(side ? nzb : 0) * 1024;
     float *out = tinv + ti_off[k] + (size_t)side * nc * nc;
     const int orf = warp >> 1, ocf = 2 * (warp & 1);  // this warp's two 8 x 8 fragments of a 32 x 32 block
+    const bool trans = (FACT == FACT_GETRF && side == 0);  // T = U, stored by columns in the L panel
+    // issue the copies of block row i of T (columns 32 (i + 1) .. 32 j + 31) and Z_i into buffer b
+    auto stage = [&](int i, int b) {
+        const int k0 = 32 * (i + 1), K = 32 * (j - i);
+        float *ts = Ts + b * 32 * tld;
+        if (trans) {
+            for (int e = tid; e < 32 * K; e += 256) {
+                const int r = e & 31, c = e >> 5, col = k0 + c;
+                const bool v = col < nc;
+                cp_async4(ts + r * tld + c, v ? D + 32 * i + r + (size_t)col * st : D, v);
+            }
+        } else {
+            for (int e = tid; e < 32 * K; e += 256) {
+                const int r = e / K, c = e - r * K, col = k0 + c;
+                const bool v = col < nc;
+                cp_async4(ts + r * tld + c, v ? D + col + (size_t)(32 * i + r) * st : D, v);
+            }
+        }
+        float *zs = Zf + b * 32 * TI_ZLD;
+        for (int e = tid; e < 1024; e += 256) cp_async4(zs + (e >> 5) * TI_ZLD + (e & 31), gZ + (size_t)i * 1024 + e, true);
+        cp_async_commit();
+    };
+    if (j > 0) stage(j - 1, 0);
     // Y_j = Z_j
     for (int e = tid; e < 1024; e += blockDim.x) Yb[(32 * j + (e >> 5)) * DG_LD + (e & 31)] = (double)gZ[(size_t)j * 1024 + e];
-    for (int i = j - 1; i >= 0; i--) {
-        // stage block row i of T (columns 32 (i + 1) .. 32 j + 31) and Z_i in one pass
-        const int k0 = 32 * (i + 1), K = 32 * (j - i);
-        for (int e = tid; e < 32 * K; e += blockDim.x) {
-            const int r = e / K, c = e - r * K;
-            const int b = k0 + c;
-            Ts[r * tld + c] = (b < nc) ? (float)trsm_tval<T, FACT>(D, st, 32 * i + r, b, side) : 0.f;
+    for (int i = j - 1, b = 0; i >= 0; i--, b ^= 1) {
+        if (i > 0) {
+            stage(i - 1, b ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
-        for (int e = tid; e < 1024; e += blockDim.x) Zs[(e >> 5) * DG_LD + (e & 31)] = (double)gZ[(size_t)i * 1024 + e];
         __syncthreads();
+        const float *ts = Ts + b * 32 * tld;
+        const float *zs = Zf + b * 32 * TI_ZLD;
+        const int k0 = 32 * (i + 1), K = 32 * (j - i);
         // S = T_{i, i+1..j} Y_{i+1..j}
         double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
         for (int ks = 0; ks < K / 4; ks++) {
-            const double a = (double)Ts[(8 * orf + g) * tld + 4 * ks + t4];
+            const double a = (double)ts[(8 * orf + g) * tld + 4 * ks + t4];
 #pragma unroll
             for (int c = 0; c < 2; c++)
                 dmma884(acc[c][0], acc[c][1], a, Yb[(k0 + 4 * ks + t4) * DG_LD + 8 * (ocf + c) + g]);
         }
+        double scale = 1.0;
+        if (FACT == FACT_SYTRF) {
+            const int a = 32 * i + 8 * orf + g;
+            scale = (double)D[a + (size_t)a * st];
+        }
 #pragma unroll
         for (int c = 0; c < 2; c++) {
-            Ss[(8 * orf + g) * DG_LD + 8 * (ocf + c) + 2 * t4] = acc[c][0];
-            Ss[(8 * orf + g) * DG_LD + 8 * (ocf + c) + 2 * t4 + 1] = acc[c][1];
+            Ss[(8 * orf + g) * DG_LD + 8 * (ocf + c) + 2 * t4] = scale * acc[c][0];
+            Ss[(8 * orf + g) * DG_LD + 8 * (ocf + c) + 2 * t4 + 1] = scale * acc[c][1];
         }
         __syncthreads();
         // Y_i = -Z_i S
         double y[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
         for (int ks = 0; ks < 8; ks++) {
-            const double a = -Zs[(8 * orf + g) * DG_LD + 4 * ks + t4];
+            const double a = -(double)zs[(8 * orf + g) * TI_ZLD + 4 * ks + t4];
 #pragma unroll
             for (int c = 0; c < 2; c++) dmma884(y[c][0], y[c][1], a, Ss[(4 * ks + t4) * DG_LD + 8 * (ocf + c) + g]);
         }

@@ -56,6 +56,7 @@ void launch_split(const DevStruct &, const SplitSlab *, int, const float *, cons
 long long split_image_bytes(int nc, int st);
 long long panel_small_bytes(long long panel_elems, int tsize, int maxst);
 int trinv_max_blocks();
+size_t diag_cluster_scratch_doubles();
 template <int F>
 void launch_trinv(const DevStruct &, const int *, int, int, const float *, const float *, const float *,
                   const int64_t *, float *, cudaStream_t);
@@ -216,6 +217,7 @@ struct Device {
     // work
     DBuf<int> counters;      // [0] nbpivots, [1] status
     DBuf<int> queues;        // tile work-queue heads of the tcgen05 launches, 3 per level, zeroed per factorization
+    DBuf<double> dcscr;      // finished panels of the cluster diagonal kernel (read by the cluster's other CTAs)
     DBuf<double> crit;       // static pivoting threshold of the current factorization
     DBuf<double> part, scal; // reduction partials, scalars
     DBuf<double> w1, w2;     // permuted double work vectors
@@ -1443,6 +1445,7 @@ static int device_setup(pastix_data_t *pd) {
     CUDA_TRY(d.csr_val.alloc(std::max<idx_t>(1, pd->csr_nnz)));
     CUDA_TRY(d.counters.alloc(4));
     CUDA_TRY(d.queues.alloc(std::max<size_t>(1, 3 * pd->levels.size())));
+    CUDA_TRY(d.dcscr.alloc(pgpu::diag_cluster_scratch_doubles()));
     CUDA_TRY(d.crit.alloc(1));
     CUDA_TRY(cudaMemsetAsync(d.counters.p, 0, 4 * sizeof(int), st));
     CUDA_TRY(d.part.alloc(pgpu::reduce_partials()));
@@ -1482,7 +1485,7 @@ static int run_factor(pastix_data_t *pd, double criterion) {
     T *U = reinterpret_cast<T *>(d.Uc.p);
     T *Dinv = reinterpret_cast<T *>(d.dinv.p);
     (void)criterion;  // copied to d.crit by the caller
-    pgpu::FactParams fp{d.crit.p, d.counters.p, d.counters.p + 1};
+    pgpu::FactParams fp{d.crit.p, d.counters.p, d.counters.p + 1, d.dcscr.p};
     // FP32: the updates of level l whose targets sit two or more levels up run on a
     // second stream and overlap level l + 1 (all FP32 update writes are reductions)
     // (the profiled pass keeps one stream so that each class's events time it alone)

@@ -80,6 +80,7 @@ struct FactParams {
                                 // a captured launch sequence stays valid when the values change
     int *nbpivots;              // device counter
     int *status;                // device status word (0 = fine)
+    double *dscr;               // k_diag_cluster: the finished panels of each cblk of a launch, DC_SCR_DOUBLES per cblk
 };
 
 // Element-wise transfer by a whole CTA with UNR independent loads in flight per

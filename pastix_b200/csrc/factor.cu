@@ -1189,11 +1189,12 @@ __device__ __forceinline__ int dg_factor32_impl(double *W, int nbr, double crit,
 // and updates the rest of its row; the row then moves 8 places left, so the
 // loop over the blocks runs rolled with static register indices.  `Blk`: 320
 // doubles, 16-byte aligned.  Block b is announced by an arrival at named
-// barrier 1 + b (64 threads: this warp and the inverse warp, which waits there)
+// barrier 1 + b (bar_n threads: this warp, the inverse warp and the warps that
+// solve the rows below the block in step (dg_follow_rows), which wait there)
 // instead of through *prog.
 template <int FACT>
 __device__ __noinline__ int dg_factor32_sym(double *W, int nb, double crit, double *Pub, volatile int *prog,
-                                            double *Blk) {
+                                            double *Blk, int bar_n, double *gX, int ldx) {
     const int lane = threadIdx.x & 31;
     double *D8 = Blk, *Xr = Blk + 64;
     double r[32];
@@ -1253,7 +1254,10 @@ __device__ __noinline__ int dg_factor32_sym(double *W, int nb, double crit, doub
         for (int c = 0; c < 8; c++) pv[c] = (FACT == FACT_SYTRF && lane != jb + c) ? x[c] * dd[c] : x[c];
 #pragma unroll
         for (int c = 0; c < 8; c++) {  // rows jb + c <= 31 of Pub exist even beyond nb (never read there)
-            if (lane < nb && jb + c < nb) W[lane * DG_LD + jb + c] = x[c];
+            if (lane < nb && jb + c < nb) {
+                W[lane * DG_LD + jb + c] = x[c];
+                if (gX) gX[lane + (size_t)(jb + c) * ldx] = x[c];
+            }
             Pub[(jb + c) * DG_BLD + lane] = pv[c];
             if (lane == c) Pub[(jb + c) * DG_BLD + 32] = iv[c];
         }
@@ -1261,7 +1265,7 @@ __device__ __noinline__ int dg_factor32_sym(double *W, int nb, double crit, doub
         for (int c = 0; c < 8; c += 2) *reinterpret_cast<double2 *>(Xr + lane * 8 + c) = make_double2(pv[c], pv[c + 1]);
         __syncwarp();
         // block published: release the inverse warp(s) waiting at named barrier 1 + jb / 8
-        asm volatile("bar.arrive %0, 64;" ::"r"(1 + jb / 8) : "memory");
+        asm volatile("bar.arrive %0, %1;" ::"r"(1 + jb / 8), "r"(bar_n) : "memory");
         // rank-8 update of the rest of the row (lower part: columns jb + j <= lane), by
         // groups of 8 columns that exist; no branch inside a group, so its columns overlap
 #pragma unroll
@@ -1291,9 +1295,70 @@ __device__ __noinline__ int dg_factor32_sym(double *W, int nb, double crit, doub
     return np;
 }
 
+// One warp beside dg_factor32_sym: rows lane < nrows of W (row major, ld
+// DG_LD: rows below the top block being factored, every earlier update
+// applied) solved against the block's factor as it is published -- the
+// off-diagonal TRSM of kernels/core_ztrsmsp.c by substitution, in step with the
+// factorization instead of after it.  After named barrier 1 + jb / 8 (bar_n
+// threads), with P(c, j) = Pub[jb + c][jb + j] (POTRF L(jb + j, jb + c), SYTRF
+// D(jb + c) L(jb + j, jb + c)) and Pub[jb + c][32] = 1 / d:
+//   x_c = (w_c - sum_{k<c} x_k P(k, c)) / d_c      (L(i, jb + c), written in place
+//                                                   and to gX, column-major, ld ldx)
+//   w_j -= sum_c x_c P(c, j)                        (the row's later columns)
 template <int FACT>
-__device__ __forceinline__ int dg_factor32(double *W, int nb, double crit, double *Pub, volatile int *prog) {
-    if (FACT != FACT_GETRF) return dg_factor32_sym<FACT>(W, nb, crit, Pub, prog, Pub + 32 * DG_BLD);
+__device__ __noinline__ void dg_follow_rows(double *W, int nrows, int nb, const double *Pub, int bar_n, double *gX,
+                                            int ldx) {
+    const int lane = threadIdx.x & 31;
+    const bool own = lane < nrows;
+    double r[32];
+#pragma unroll
+    for (int j = 0; j < 32; j++) r[j] = (own && j < nb) ? W[lane * DG_LD + j] : 0.0;
+#pragma unroll 1
+    for (int jb = 0; jb < nb; jb += 8) {
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + jb / 8), "r"(bar_n) : "memory");
+        const double *P = Pub + jb * DG_BLD + jb;
+        double x[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            double sc = r[c];
+#pragma unroll
+            for (int k = 0; k < c; k++) sc -= x[k] * P[k * DG_BLD + c];
+            x[c] = sc * Pub[(jb + c) * DG_BLD + 32];
+        }
+#pragma unroll
+        for (int c = 0; c < 8; c++)
+            if (own && jb + c < nb) {
+                W[lane * DG_LD + jb + c] = x[c];
+                gX[lane + (size_t)(jb + c) * ldx] = x[c];
+            }
+        // rank-8 update of the later columns, by groups of 8 that exist
+#pragma unroll
+        for (int g = 8; g < 32; g += 8) {
+            if (jb + g < 32) {
+#pragma unroll
+                for (int j = g; j < g + 8; j++) {
+                    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                    for (int c = 0; c < 8; c += 2) {
+                        s0 += x[c] * P[c * DG_BLD + j];
+                        s1 += x[c + 1] * P[(c + 1) * DG_BLD + j];
+                    }
+                    r[j] -= s0 + s1;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 24; j++) r[j] = r[j + 8];
+#pragma unroll
+        for (int j = 24; j < 32; j++) r[j] = 0.0;
+    }
+}
+
+template <int FACT>
+__device__ __forceinline__ int dg_factor32(double *W, int nb, double crit, double *Pub, volatile int *prog,
+                                           int bar_n = 64, double *gX = nullptr, int ldx = 0) {
+    if (FACT != FACT_GETRF)
+        return dg_factor32_sym<FACT>(W, nb, crit, Pub, prog, Pub + 32 * DG_BLD, bar_n, gX, ldx);
     return (nb == 32) ? dg_factor32_impl<FACT, true>(W, 32, crit, Pub, prog)
                       : dg_factor32_impl<FACT, false>(W, nb, crit, Pub, prog);
 }
@@ -1305,11 +1370,12 @@ __device__ __forceinline__ int dg_factor32(double *W, int nb, double crit, doubl
 // forms column j of M^{-1} by forward substitution, row i as soon as the
 // factorization has published step i (M(i, k) = Pub[k][i], side 1 Pub[i][k]),
 // so the inverse ends one step after the factorization.  POTRF / SYTRF wait at
-// the named barrier of each 8-row block; GETRF polls *prog, and a wait that
-// runs past its bound records PGPU_STATUS_TIMEOUT in `status` and stops waiting.
+// the named barrier of each 8-row block (bar_n threads); GETRF polls *prog, and a
+// wait that runs past its bound records PGPU_STATUS_TIMEOUT in `status` and
+// stops waiting.
 template <typename T, int FACT>
 __device__ __forceinline__ void dg_inverse_pipe(const double *Pub, int nb, int side, const volatile int *prog,
-                                                double *Z, T *gZ, int *status) {
+                                                double *Z, T *gZ, int *status, int bar_n = 64) {
     const int lane = threadIdx.x & 31;
     const bool lower_l = FACT == FACT_GETRF && side == 1;
     double y[32];
@@ -1318,7 +1384,7 @@ __device__ __forceinline__ void dg_inverse_pipe(const double *Pub, int nb, int s
     for (int i = 0; i < 32; i++) {
         if (i < nb) {
             if (FACT != FACT_GETRF) {  // POTRF / SYTRF: block i / 8 announced at a named barrier
-                if ((i & 7) == 0) asm volatile("bar.sync %0, 64;" ::"r"(1 + i / 8) : "memory");
+                if ((i & 7) == 0) asm volatile("bar.sync %0, %1;" ::"r"(1 + i / 8), "r"(bar_n) : "memory");
             } else {
                 for (int spins = 0; ok && *prog <= i;)
                     if (++spins > DG_SPIN) ok = false;
@@ -1608,6 +1674,13 @@ constexpr int DC_MIN_NC = 96;              // narrower blocks stay on one CTA
 // dynamic shared memory next to the static ~37 KB
 __host__ __device__ constexpr long long dc_max_smem(int) { return 180 * 1024LL; }
 constexpr int DC_SLOTS = (DG_MAXNC / 32 + DC - 1) / DC;  // panels one CTA can own (nc <= DG_MAXNC)
+// POTRF / SYTRF: every finished panel is also written (FP64, column-major nc x nc,
+// from its top row down) to a per-cblk area of global memory, from which the
+// other CTAs read it for their updates: eight CTAs reading one CTA's shared
+// memory at once through the cluster are bound by that one SM, while L2 serves
+// them in parallel.
+constexpr size_t DC_SCR_DOUBLES = (size_t)DG_MAXNC * DG_MAXNC;
+constexpr int DC_MAX_CLUSTERS = 160 / DC;  // cblks of one launch: count * DC <= SM count
 
 __host__ __device__ inline int dc_lo(int p, int fact) { return fact == FACT_GETRF ? 0 : 32 * p; }
 // Shared memory (doubles) of the panels CTA `rank` owns for a block of width nc.
@@ -1666,6 +1739,7 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
     T *A = L + s.cb_coef[k];
     T *gZ = dinv + s.cb_dinv[k];
+    double *X = fp.dscr + (size_t)(blockIdx.x / DC) * DC_SCR_DOUBLES;  // this cblk's finished panels (POTRF / SYTRF)
     if (tid == 0) {
         npiv = 0;
         fpart = 0;
@@ -1699,11 +1773,11 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
     }
     cluster.sync();  // panels loaded and flags cleared in every CTA before any flag is read
 
-    // Each panel is announced in two stages through this CTA's flags: fpart = p + 1
-    // once its factored top block and the rows that form the top block of panel
-    // p + 1 are final, fdone = p + 1 once all its rows are.  The owner of panel
-    // p + 1 starts on its top block at fpart, so the rest of panel p's TRSM and
-    // every other update run beside the critical chain
+    // Panels are announced through this CTA's flags: fdone = p + 1 once all rows
+    // of panel p are final.  GETRF announces in two stages: fpart = p + 1 once
+    // its factored top block and the rows that form the top block of panel p + 1
+    // are final; the owner of panel p + 1 starts on its top block at fpart, so
+    // the rest of panel p's TRSM and every other update run beside the chain
     //   rows of p for p + 1's top -> p + 1's top updated -> factored -> ...
     auto publish = [&](int *flag, int p) {
         __syncthreads();
@@ -1757,15 +1831,19 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         const int nb = min(32, nc - 32 * p);
         const int lop = dc_lo(p, FACT);
         double *W = Wl + poff(p);
+        const double *Wt = W + (32 * p - lop) * DG_LD;  // the factored top block
         rb = min(rb, nc);
         const int nrf = (rb - ra + 7) / 8;
         for (int i = warp; i < nrf; i += 8) {
             const int r8 = ra + 8 * i;
             dg_solve8(
                 [&](int row, int col) { return (r8 + row < rb) ? W[(r8 + row - lop) * DG_LD + col] : 0.0; },
-                [&](int a, int b) { return (a <= b && b < nb) ? dg_t<FACT>(Tb, a, b, 0) : 0.0; }, Zs0, Sx[warp],
+                [&](int a, int b) { return (a <= b && b < nb) ? dg_t<FACT>(Wt, a, b, 0) : 0.0; }, Zs0, Sx[warp],
                 [&](int row, int col, double v) {
-                    if (r8 + row < rb) W[(r8 + row - lop) * DG_LD + col] = v;
+                    if (r8 + row < rb) {
+                        W[(r8 + row - lop) * DG_LD + col] = v;
+                        if (FACT != FACT_GETRF && col < nb) X[(r8 + row) + (size_t)(32 * p + col) * nc] = v;
+                    }
                 });
         }
     };
@@ -1809,8 +1887,9 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
             if (cc < nbq && kk < nb) {
                 if (FACT == FACT_GETRF) b = Wq[(32 * p + kk - loq) * DG_LD + cc];
                 else {
-                    b = Wp[(32 * q + cc - lop) * DG_LD + kk];
-                    if (FACT == FACT_SYTRF) b *= Wpt[kk * DG_LD + kk];
+                    const double *Xp = X + (size_t)(32 * p + kk) * nc;  // column 32 p + kk
+                    b = __ldcg(Xp + 32 * q + cc);
+                    if (FACT == FACT_SYTRF) b *= __ldcg(Xp + 32 * p + kk);
                 }
             }
             bv[u] = b;
@@ -1832,7 +1911,10 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
                 const int r = ra + 8 * (i + 8 * f) + g;
                 rowok[f] = (i + 8 * f < nrf) && r < rb;
 #pragma unroll
-                for (int ks = 0; ks < 8; ks++) av[f][ks] = rowok[f] ? -Wp[(r - lop) * DG_LD + 4 * ks + t4] : 0.0;
+                for (int ks = 0; ks < 8; ks++) {
+                    if (FACT == FACT_GETRF) av[f][ks] = rowok[f] ? -Wp[(r - lop) * DG_LD + 4 * ks + t4] : 0.0;
+                    else av[f][ks] = rowok[f] ? -__ldcg(X + r + (size_t)(32 * p + 4 * ks + t4) * nc) : 0.0;
+                }
 #pragma unroll
                 for (int cf = 0; cf < 4; cf++)
 #pragma unroll
@@ -1869,31 +1951,88 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         publish(&fdone, p);
     };
 
-    if (rank == 0) {
-        factor_top(0);
-        finish_panel(0);
-    }
-    for (int p = 0; p + 1 < np; p++) {
-        const int q1 = p + 1;
-        int q0 = q1 + ((rank - q1) % DC + DC) % DC;  // this CTA's first panel after p
-        if (q0 == q1) {
-            // the critical chain: p + 1's top block as soon as the rows it needs are final
-            wait_flag(&fpart, p);
-            update_rows(p, q1, 0, 32 * q1 + 32);
-            factor_top(q1);
-            wait_flag(&fdone, p);
-            update_rows(p, q1, 32 * q1 + 32, 32 * q1 + 64);  // the rows of p + 2's top block
-            const int r0 = 32 * q1 + 32;
-            trsm_rows(q1, r0, r0 + 32);
-            publish(&fpart, q1);
-            update_rows(p, q1, 32 * q1 + 64, nc);
-            trsm_rows(q1, r0 + 32, nc);
-            publish(&fdone, q1);
-            q0 += DC;
-        } else {
-            wait_flag(&fdone, p);
+    // POTRF / SYTRF: panel q whole, every earlier update applied.  Warp 0 factors
+    // its top block in place, warp 1 inverts it one step behind, and up to six
+    // more warps solve the rows below it in step with the factorization
+    // (dg_follow_rows, 32 rows each), so the panel is final one block step after
+    // its top block and is announced then (fdone = q + 1), while the inverse
+    // (kept for the later TRSM kernels and the solve) is still being written.
+    // Rows beyond the followers' 192 (blocks wider than 224 columns, first
+    // panels) take the TRSM by the inverse before the announcement.
+    constexpr int DC_FOLLOW = 6;
+    auto factor_panel = [&](int q) {
+        const int nb = min(32, nc - 32 * q);
+        double *W = Wl + poff(q);  // lo = 32 q: the top block is the panel's first nb rows
+        const int nr = nc - 32 * q - nb;
+        const int F = min(DC_FOLLOW, (nr + 31) / 32);
+        const int bar_n = 64 + 32 * F;
+        const bool rest = nr > 32 * DC_FOLLOW;
+        __syncthreads();
+        double *Xq = X + 32 * q + (size_t)(32 * q) * nc;  // the panel's mirror from its top row
+        if (warp == 0) {
+            const int n = dg_factor32<FACT>(W, nb, __ldg(fp.criterion), &Sx[0][0], &prog, bar_n, Xq, nc);
+            if (lane == 0 && n) npiv += n;
+        } else if (warp == 1) {
+            dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 0, &prog, Zs0, gZ + (size_t)q * 1024, fp.status, bar_n);
+        } else if (warp - 2 < F) {
+            const int f = warp - 2;
+            dg_follow_rows<FACT>(W + (nb + 32 * f) * DG_LD, min(32, nr - 32 * f), nb, &Sx[0][0], bar_n,
+                                 Xq + nb + 32 * f, nc);
         }
-        for (int q = q0; q < np; q += DC) update_rows(p, q, 0, nc);
+        if (!rest && warp != 1 && warp < 2 + F) {
+            asm volatile("bar.sync 5, %0;" ::"r"(32 * (1 + F)) : "memory");
+            if (tid == 0) {
+                asm volatile("fence.acq_rel.cluster;" ::: "memory");
+                dsmem_st_release(dsmem_map(&fdone, rank), q + 1);
+            }
+        }
+        __syncthreads();
+        if (rest) {
+            trsm_rows(q, 32 * q + nb + 32 * DC_FOLLOW, nc);
+            publish(&fdone, q);
+        }
+    };
+
+    if (FACT != FACT_GETRF) {
+        if (rank == 0) factor_panel(0);
+        for (int p = 0; p + 1 < np; p++) {
+            const int q1 = p + 1;
+            int q0 = q1 + ((rank - q1) % DC + DC) % DC;  // this CTA's first panel after p
+            wait_flag(&fdone, p);
+            if (q0 == q1) {  // the critical chain: panel p + 1 as soon as panel p is final
+                update_rows(p, q1, 0, nc);
+                factor_panel(q1);
+                q0 += DC;
+            }
+            for (int q = q0; q < np; q += DC) update_rows(p, q, 0, nc);
+        }
+    } else {
+        if (rank == 0) {
+            factor_top(0);
+            finish_panel(0);
+        }
+        for (int p = 0; p + 1 < np; p++) {
+            const int q1 = p + 1;
+            int q0 = q1 + ((rank - q1) % DC + DC) % DC;  // this CTA's first panel after p
+            if (q0 == q1) {
+                // the critical chain: p + 1's top block as soon as the rows it needs are final
+                wait_flag(&fpart, p);
+                update_rows(p, q1, 0, 32 * q1 + 32);
+                factor_top(q1);
+                wait_flag(&fdone, p);
+                update_rows(p, q1, 32 * q1 + 32, 32 * q1 + 64);  // the rows of p + 2's top block
+                const int r0 = 32 * q1 + 32;
+                trsm_rows(q1, r0, r0 + 32);
+                publish(&fpart, q1);
+                update_rows(p, q1, 32 * q1 + 64, nc);
+                trsm_rows(q1, r0 + 32, nc);
+                publish(&fdone, q1);
+                q0 += DC;
+            } else {
+                wait_flag(&fdone, p);
+            }
+            for (int q = q0; q < np; q += DC) update_rows(p, q, 0, nc);
+        }
     }
     wait_flag(&fdone, np - 1);  // every panel is final before the write-out and the tail below
     // this CTA's panels are final: write them out
@@ -2642,7 +2781,8 @@ void launch_diag_large(const DevStruct &s, const int *list, int count, int maxnc
             nsm = 1;
     }
     const long long csm = diag_cluster_smem_bytes(maxnc, FACT);
-    if (maxnc <= DG_MAXNC && maxnc >= DC_MIN_NC && (long long)count * DC <= nsm && csm <= dc_max_smem(FACT))
+    if (maxnc <= DG_MAXNC && maxnc >= DC_MIN_NC && (long long)count * DC <= nsm && count <= DC_MAX_CLUSTERS &&
+        csm <= dc_max_smem(FACT))
         k_diag_cluster<T, FACT><<<count * DC, 256, (size_t)csm, st>>>(s, list, L, U, dinv, fp);
     else if (maxnc <= DG_MAXNC)
         k_diag_dmma<T, FACT><<<count, 256, (size_t)diag_dmma_smem_bytes(maxnc), st>>>(s, list, L, U, dinv, fp);
@@ -2722,6 +2862,7 @@ long long panel_small_bytes(long long panel_elems, int tsize, int maxst) {
     return panel_small_smem_bytes(panel_elems, tsize, maxst);
 }
 int trinv_max_blocks() { return DG_MAXNC / 32; }
+size_t diag_cluster_scratch_doubles() { return DC_MAX_CLUSTERS * DC_SCR_DOUBLES; }
 
 // Opt every kernel with dynamic shared memory into the largest size the
 // device allows next to its static shared memory.

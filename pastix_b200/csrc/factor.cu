@@ -1354,6 +1354,44 @@ __device__ __noinline__ void dg_follow_rows(double *W, int nrows, int nb, const 
     }
 }
 
+// One warp: rows r < nrows of Wr (row major, ld DG_LD, 32 columns) lose the
+// update of one finished panel, C -= A B: A(r, k) = Xa[r + k ldx] (the panel's
+// rows, global memory), B (32 x 32, ld DG_LD, zero outside the blocks) staged
+// in shared memory.  All 32 A loads of a lane are issued at once; DMMA 8 x 8 x 4.
+__device__ __noinline__ void dg_rows_update(double *Wr, int nrows, const double *Xa, int ldx, const double *Bs) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
+    double av[4][8], c[4][4][2];
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        const int r = 8 * f + g;
+        const bool ok = r < nrows;
+#pragma unroll
+        for (int ks = 0; ks < 8; ks++) av[f][ks] = ok ? -__ldcg(Xa + r + (size_t)(4 * ks + t4) * ldx) : 0.0;
+#pragma unroll
+        for (int cf = 0; cf < 4; cf++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) c[f][cf][e] = ok ? Wr[r * DG_LD + 8 * cf + 2 * t4 + e] : 0.0;
+    }
+#pragma unroll
+    for (int ks = 0; ks < 8; ks++)
+#pragma unroll
+        for (int cf = 0; cf < 4; cf++) {
+            const double bb = Bs[(4 * ks + t4) * DG_LD + 8 * cf + g];
+#pragma unroll
+            for (int f = 0; f < 4; f++) dmma884(c[f][cf][0], c[f][cf][1], av[f][ks], bb);
+        }
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        const int r = 8 * f + g;
+        if (r < nrows)
+#pragma unroll
+            for (int cf = 0; cf < 4; cf++)
+#pragma unroll
+                for (int e = 0; e < 2; e++) Wr[r * DG_LD + 8 * cf + 2 * t4 + e] = c[f][cf][e];
+    }
+    __syncwarp();
+}
+
 template <int FACT>
 __device__ __forceinline__ int dg_factor32(double *W, int nb, double crit, double *Pub, volatile int *prog,
                                            int bar_n = 64, double *gX = nullptr, int ldx = 0) {
@@ -1760,7 +1798,7 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         const int lo = dc_lo(p, FACT), rows = nc - lo, nb = min(32, nc - 32 * p);
         double *W = Wl + poff(p);
         const T *Ut = U + s.cb_coef[k];
-        dg_copy<4>(
+        dg_copy<12>(
             rows, 32,
             [&](int r, int c) {
                 if (c >= nb) return 0.0;
@@ -1951,16 +1989,27 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         publish(&fdone, p);
     };
 
-    // POTRF / SYTRF: panel q whole, every earlier update applied.  Warp 0 factors
-    // its top block in place, warp 1 inverts it one step behind, and up to six
-    // more warps solve the rows below it in step with the factorization
-    // (dg_follow_rows, 32 rows each), so the panel is final one block step after
-    // its top block and is announced then (fdone = q + 1), while the inverse
-    // (kept for the later TRSM kernels and the solve) is still being written.
-    // Rows beyond the followers' 192 (blocks wider than 224 columns, first
-    // panels) take the TRSM by the inverse before the announcement.
+    // POTRF / SYTRF: panel q, every update but that of panel pu (-1: none)
+    // applied, and that one applied to its top block (B block of the update
+    // still staged in Bs).  Warp 0 factors the top block in place, warp 1
+    // inverts it one step behind, and up to six more warps each take 32 rows
+    // below it: they apply panel pu's update to their rows (dg_rows_update)
+    // while the factorization starts, then solve the rows in step with it
+    // (dg_follow_rows), so the panel is final one block step after its top
+    // block and is announced then (fdone = q + 1), while the inverse (kept for
+    // the later TRSM kernels and the solve) is still being written.  Rows beyond
+    // the followers' 192 (blocks wider than 224 columns, first panels) take the
+    // update and the TRSM by the inverse before the announcement.
+    // panel p (final) from shared memory to the factor in global memory
+    auto write_panel = [&](int p) {
+        const int lop = dc_lo(p, FACT), nb = min(32, nc - 32 * p);
+        const double *W = Wl + poff(p);
+        dg_copy<8>(
+            nc - lop, nb, [&](int r, int c) { return W[r * DG_LD + c]; },
+            [&](int r, int c, double v) { A[(lop + r) + (size_t)(32 * p + c) * st] = (T)v; });
+    };
     constexpr int DC_FOLLOW = 6;
-    auto factor_panel = [&](int q) {
+    auto factor_panel = [&](int q, int pu) {
         const int nb = min(32, nc - 32 * q);
         double *W = Wl + poff(q);  // lo = 32 q: the top block is the panel's first nb rows
         const int nr = nc - 32 * q - nb;
@@ -1976,8 +2025,10 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
             dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 0, &prog, Zs0, gZ + (size_t)q * 1024, fp.status, bar_n);
         } else if (warp - 2 < F) {
             const int f = warp - 2;
-            dg_follow_rows<FACT>(W + (nb + 32 * f) * DG_LD, min(32, nr - 32 * f), nb, &Sx[0][0], bar_n,
-                                 Xq + nb + 32 * f, nc);
+            double *Wf = W + (nb + 32 * f) * DG_LD;
+            const int nrows = min(32, nr - 32 * f);
+            if (pu >= 0) dg_rows_update(Wf, nrows, X + 32 * q + nb + 32 * f + (size_t)(32 * pu) * nc, nc, Bs);
+            dg_follow_rows<FACT>(Wf, nrows, nb, &Sx[0][0], bar_n, Xq + nb + 32 * f, nc);
         }
         if (!rest && warp != 1 && warp < 2 + F) {
             asm volatile("bar.sync 5, %0;" ::"r"(32 * (1 + F)) : "memory");
@@ -1988,24 +2039,37 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         }
         __syncthreads();
         if (rest) {
+            if (pu >= 0) update_rows(pu, q, 32 * q + nb + 32 * DC_FOLLOW, nc);
             trsm_rows(q, 32 * q + nb + 32 * DC_FOLLOW, nc);
             publish(&fdone, q);
         }
     };
 
     if (FACT != FACT_GETRF) {
-        if (rank == 0) factor_panel(0);
+        // a panel goes out to the factor as soon as it is final and the CTA's
+        // updates of the step are issued: the CTA waits for the next panels anyway
+        int wq = -1;  // the panel this CTA finished last, not yet written
+        if (rank == 0) {
+            factor_panel(0, -1);
+            wq = 0;
+        }
         for (int p = 0; p + 1 < np; p++) {
             const int q1 = p + 1;
             int q0 = q1 + ((rank - q1) % DC + DC) % DC;  // this CTA's first panel after p
             wait_flag(&fdone, p);
             if (q0 == q1) {  // the critical chain: panel p + 1 as soon as panel p is final
-                update_rows(p, q1, 0, nc);
-                factor_panel(q1);
+                update_rows(p, q1, 0, 32 * q1 + 32);  // its top block; the rows below in factor_panel
+                factor_panel(q1, p);
                 q0 += DC;
+                wq = q1;
             }
             for (int q = q0; q < np; q += DC) update_rows(p, q, 0, nc);
+            if (wq >= 0) {
+                write_panel(wq);
+                wq = -1;
+            }
         }
+        if (wq >= 0) write_panel(wq);
     } else {
         if (rank == 0) {
             factor_top(0);
@@ -2035,14 +2099,9 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         }
     }
     wait_flag(&fdone, np - 1);  // every panel is final before the write-out and the tail below
-    // this CTA's panels are final: write them out
-    for (int p = rank; p < np; p += DC) {
-        const int lop = dc_lo(p, FACT), nb = min(32, nc - 32 * p);
-        const double *W = Wl + poff(p);
-        dg_copy<4>(
-            nc - lop, nb, [&](int r, int c) { return W[r * DG_LD + c]; },
-            [&](int r, int c, double v) { A[(lop + r) + (size_t)(32 * p + c) * st] = (T)v; });
-    }
+    // GETRF: this CTA's panels are final: write them out
+    if (FACT == FACT_GETRF)
+        for (int p = rank; p < np; p += DC) write_panel(p);
     __threadfence();
     cluster.sync();  // all panels written; no CTA leaves while its shared memory may still be read
     if (rank == 0) {

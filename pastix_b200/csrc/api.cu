@@ -335,7 +335,7 @@ static inline void launch_cls(pastix_data_t *pd, int cls, long long count, Fn &&
 // helpers
 // ---------------------------------------------------------------------------
 enum : int { WS_SOLVE = 0, WS_ORDER, WS_GMV, WS_GMW, WS_GMG, WS_VEC, WS_BP, WS_XP, WS_RB, WS_RX, WS_BGV, WS_BGS,
-             WS_SPSV };
+             WS_SPSV, WS_GMH };
 
 // Persistent device work area `slot` of at least `count` doubles (grown, never shrunk).
 static double *work(Device &d, int slot, size_t count) {
@@ -2176,8 +2176,8 @@ static int refine_gmres(Refiner &R, double *x, const double *b, double eps, int 
     const int64_t n = R.n;
     const int im1 = im + 1;
     struct { double *p; } V{work(R.d, WS_GMV, (size_t)n * im1)}, W{work(R.d, WS_GMW, (size_t)n * im)},
-        gdev{work(R.d, WS_GMG, im1)};
-    if (!V.p || !W.p || !gdev.p) return PASTIX_ERR_OUTOFMEMORY;
+        gdev{work(R.d, WS_GMG, im1)}, hdev{work(R.d, WS_GMH, im1)};
+    if (!V.p || !W.p || !gdev.p || !hdev.p) return PASTIX_ERR_OUTOFMEMORY;
     std::vector<double> H((size_t)im * im1, 0.0), gcos(im), gsin(im), G(im1);
     double normb = R.norm(b);
     if (normb == 0.) normb = 1;
@@ -2205,13 +2205,19 @@ static int refine_gmres(Refiner &R, double *x, const double *b, double eps, int 
             if (R.spsv(Wi)) return PASTIX_ERR_INTERNAL;
             double *Vn = Vi + n;
             R.spmv(1.0, Wi, 0., Vn);
+            // modified Gram-Schmidt with the coefficients kept on the device (the
+            // same operations in the same order as host scalars would take), read
+            // back once per Arnoldi step
             for (int j = 0; j <= i; j++) {
-                Hi[j] = R.dot(Vn, V.p + (size_t)j * n);
-                R.axpy(-Hi[j], V.p + (size_t)j * n, Vn);
+                pgpu::launch_dot(n, Vn, V.p + (size_t)j * n, R.d.part.p, 0, hdev.p + j, R.d.stream);
+                pgpu::launch_axpy_cols(n, 1, hdev.p + j, V.p + (size_t)j * n, n, Vn, n, R.d.stream);
             }
-            double nrm = R.norm(Vn);
-            Hi[i + 1] = nrm;
-            if (nrm > 1e-50) R.scal(1.0 / nrm, Vn);
+            pgpu::launch_dot(n, Vn, Vn, R.d.part.p, 1, hdev.p + i + 1, R.d.stream);
+            pgpu::launch_scal_cols(n, 1, hdev.p + i + 1, 1, Vn, n, R.d.stream);  // when the norm is > 1e-50
+            if (cudaMemcpyAsync(Hi, hdev.p, (size_t)(i + 2) * sizeof(double), cudaMemcpyDeviceToHost, R.d.stream) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(R.d.stream) != cudaSuccess)
+                return PASTIX_ERR_INTERNAL;
             for (int j = 0; j < i; j++) {
                 double t = Hi[j];
                 Hi[j] = gcos[j] * t + gsin[j] * Hi[j + 1];

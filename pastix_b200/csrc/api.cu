@@ -520,6 +520,12 @@ extern "C" void pastixFinalize(pastix_data_t **pd) {
         cudaStreamSynchronize(p->dev.stream);
     }
     cudaStream_t st = p->dev.stream;
+    if (p->dev.ready) {
+        if (p->dev.side) cudaStreamSynchronize(p->dev.side);
+        for (auto *v : {&p->dev.ev_chain, &p->dev.ev_rest})
+            for (cudaEvent_t e : *v) cudaEventDestroy(e);
+        if (p->dev.side) cudaStreamDestroy(p->dev.side);
+    }
     delete p;  // DBuf destructors free device memory
     if (st) cudaStreamDestroy(st);
     *pd = nullptr;

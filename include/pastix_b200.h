@@ -312,6 +312,11 @@ int pgpu_spmv_device(pastix_data_t *pastix_data, double alpha, const double *x, 
                      double *y, void *stream);
 /* Last device status word (0 = fine); non-zero after a bounded wait expired. */
 int pgpu_device_status(const pastix_data_t *pastix_data);
+/* Self-test of the kernels' bounded waits on the current device: one wait on
+ * a cluster flag that nothing raises and one on an mbarrier that nothing
+ * completes; both must give up.  timed_out[0..1] receive how many did (1, 1
+ * expected).  Takes a few seconds.  No counterpart in the reference. */
+int pgpu_wait_selftest(int *timed_out);
 
 /* The library's CUDA stream (cudaStream_t) after the analysis; every entry
  * point above orders its work on it.  NULL before pastix_task_analyze. */

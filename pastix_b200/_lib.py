@@ -32,7 +32,7 @@ EXPORTS = [
     "pgpu_numfact_device", "pgpu_sampled_outer", "pgpu_spmv_device", "pgpu_device_status",
     "pgpu_stream", "pgpu_solve_refine_device", "pgpu_profile", "pgpu_profile_get", "pgpu_set_symbol",
     "pgpu_solve_device_static", "pgpu_graphs", "pgpu_set_tuning", "pgpu_get_tuning", "pgpu_autotune",
-    "pgpu_refine_block",
+    "pgpu_refine_block", "pgpu_wait_selftest",
 ]
 
 # kernel classes of pgpu_profile_get, in order
@@ -124,6 +124,7 @@ def load() -> C.CDLL:
         "pgpu_sampled_outer": (C.c_int, [P, C.c_double, VP, VP, VP, VP]),
         "pgpu_spmv_device": (C.c_int, [P, C.c_double, VP, C.c_double, VP, VP]),
         "pgpu_device_status": (C.c_int, [P]),
+        "pgpu_wait_selftest": (C.c_int, [C.POINTER(C.c_int)]),
         "pgpu_stream": (C.c_void_p, [P]),
         "pgpu_solve_refine_device": (C.c_int, [P, pastix_int_t, VP, pastix_int_t, VP, pastix_int_t]),
         "pgpu_profile": (C.c_int, [P, C.c_int]),

@@ -57,6 +57,7 @@ long long split_image_bytes(int nc, int st);
 long long panel_small_bytes(long long panel_elems, int tsize, int maxst);
 int trinv_max_blocks();
 size_t diag_cluster_scratch_doubles();
+cudaError_t wait_selftest(int *timed_out_host);
 template <int F>
 void launch_trinv(const DevStruct &, const int *, int, int, const float *, const float *, const float *,
                   const int64_t *, float *, cudaStream_t);
@@ -1798,6 +1799,13 @@ extern "C" int pgpu_get_coeftab(const pastix_data_t *pd, void *L, void *U) {
     if (U && d.Uc.p) CUDA_TRY(cudaMemcpyAsync(U, d.Uc.p, bytes, cudaMemcpyDeviceToHost, d.stream));
     CUDA_TRY(cudaStreamSynchronize(d.stream));
     return PASTIX_SUCCESS;
+}
+
+extern "C" int pgpu_wait_selftest(int *timed_out) {
+    if (!timed_out) return PASTIX_ERR_BADPARAMETER;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PASTIX_ERR_INTERNAL;
+    return pgpu::wait_selftest(timed_out) == cudaSuccess ? PASTIX_SUCCESS : PASTIX_ERR_INTERNAL;
 }
 
 extern "C" int pgpu_device_status(const pastix_data_t *pd) {

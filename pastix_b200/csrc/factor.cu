@@ -1753,6 +1753,15 @@ __device__ __forceinline__ int dsmem_ld_acquire(uint32_t addr) {
 __device__ __forceinline__ void dsmem_st_release(uint32_t addr, int v) {
     asm volatile("st.release.cluster.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
+// Wait until the cluster-shared flag at `addr` reaches `target`, with back-off;
+// false once DG_SPIN polls have gone by without it.
+__device__ __forceinline__ bool dc_wait(uint32_t addr, int target) {
+    for (int spins = 0; dsmem_ld_acquire(addr) < target;) {
+        if (++spins > DG_SPIN) return false;
+        __nanosleep(20);
+    }
+    return true;
+}
 
 template <typename T, int FACT>
 __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
@@ -1828,17 +1837,8 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
     // expiry the status word records PGPU_STATUS_TIMEOUT and the CTA carries on,
     // so that the kernel ends).
     auto wait_flag = [&](int *flag, int p) {
-        if (p % DC != rank && tid == 0) {
-            const uint32_t fa = dsmem_map(flag, p % DC);
-            int spins = 0;
-            while (dsmem_ld_acquire(fa) < p + 1) {
-                if (++spins > DG_SPIN) {
-                    atomicExch(fp.status, PGPU_STATUS_TIMEOUT);
-                    break;
-                }
-                __nanosleep(20);
-            }
-        }
+        if (p % DC != rank && tid == 0 && !dc_wait(dsmem_map(flag, p % DC), p + 1))
+            atomicExch(fp.status, PGPU_STATUS_TIMEOUT);
         __syncthreads();
     };
     // Top block of this CTA's panel p (every update from panels < p applied to
@@ -2921,6 +2921,42 @@ long long panel_small_bytes(long long panel_elems, int tsize, int maxst) {
     return panel_small_smem_bytes(panel_elems, tsize, maxst);
 }
 int trinv_max_blocks() { return DG_MAXNC / 32; }
+
+// Self-test of the bounded waits, on a two-CTA cluster: CTA 1 waits, as
+// k_diag_cluster does, on a flag of CTA 0 that nothing raises, while CTA 0
+// waits, as the tcgen05 engine does, on an mbarrier phase that nothing
+// completes.  Both waits give up; timed_out[r] counts CTA r's, and the kernel
+// ends with the context usable.
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(32) k_wait_selftest(int *timed_out) {
+    namespace cg = cooperative_groups;
+    __shared__ int flag;
+    __shared__ __align__(8) uint64_t bar;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    if (threadIdx.x == 0) {
+        flag = 0;
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    cluster.sync();
+    if (threadIdx.x == 0) {
+        const bool ok = (rank == 1) ? dc_wait(dsmem_map(&flag, 0), 1) : mbar_wait(&bar, 0);
+        if (!ok) atomicAdd(timed_out + rank, 1);
+    }
+    cluster.sync();  // CTA 0's shared memory outlives CTA 1's reads
+}
+cudaError_t wait_selftest(int *timed_out_host) {
+    int *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, 2 * sizeof(int));
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemset(d, 0, 2 * sizeof(int))) == cudaSuccess) {
+        k_wait_selftest<<<2, 32>>>(d);
+        if ((e = cudaGetLastError()) == cudaSuccess && (e = cudaDeviceSynchronize()) == cudaSuccess)
+            e = cudaMemcpy(timed_out_host, d, 2 * sizeof(int), cudaMemcpyDeviceToHost);
+    }
+    cudaFree(d);
+    return e;
+}
 size_t diag_cluster_scratch_doubles() { return DC_MAX_CLUSTERS * DC_SCR_DOUBLES; }
 
 // Opt every kernel with dynamic shared memory into the largest size the

@@ -58,6 +58,7 @@ long long panel_small_bytes(long long panel_elems, int tsize, int maxst);
 int trinv_max_blocks();
 size_t diag_cluster_scratch_doubles();
 cudaError_t wait_selftest(int *timed_out_host);
+void set_pdl(bool on);
 template <int F>
 void launch_trinv(const DevStruct &, const int *, int, int, const float *, const float *, const float *,
                   const int64_t *, float *, cudaStream_t);
@@ -1498,6 +1499,12 @@ static int run_factor(pastix_data_t *pd, double criterion) {
     // (the profiled pass keeps one stream so that each class's events time it alone)
     const bool two = sizeof(T) == 4 && !pd->prof_on;
     const cudaStream_t sd = two ? d.side : st;
+    // FP32 (launched kernel by kernel, not as a graph): each launch of the level
+    // chain overlaps the end of the kernel ahead of it (programmatic dependent launch)
+    struct PdlScope {
+        explicit PdlScope(bool on) { pgpu::set_pdl(on); }
+        ~PdlScope() { pgpu::set_pdl(false); }
+    } pdl_scope(two);
     if constexpr (sizeof(T) == 4)
         CUDA_TRY(cudaMemsetAsync(d.queues.p, 0, 3 * pd->levels.size() * sizeof(int), st));
     if (two) {

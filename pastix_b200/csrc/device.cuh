@@ -75,6 +75,13 @@ struct DevStruct {
 };
 
 // Per-call scalars for the factorization kernels.
+// Programmatic dependent launch: a kernel launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization may be scheduled before the
+// kernel ahead of it in the stream has ended; it waits here, before its first
+// memory access, until that kernel has ended and its writes are visible.
+// Without such a launch it returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 struct FactParams {
     const double *criterion;    // static pivoting threshold (eps * ||A||_F), in device memory so that
                                 // a captured launch sequence stays valid when the values change

@@ -80,6 +80,7 @@ __host__ __device__ inline long long panel_small_smem_bytes(long long panel_elem
 template <typename T, int FACT>
 __global__ void __launch_bounds__(256) k_panel_small(DevStruct s, const int *__restrict__ list, T *L, T *U,
                                                       FactParams fp) {
+    pdl_wait();  // the kernel ahead in the stream has ended (programmatic dependent launch)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *P = reinterpret_cast<T *>(smem_raw);
     const int k = list[blockIdx.x];
@@ -257,6 +258,7 @@ __device__ __forceinline__ void warp_upper_inverse(const T *Wb, int nb, int side
 template <typename T, int FACT>
 __global__ void __launch_bounds__(256) k_diag_large(DevStruct s, const int *__restrict__ list, T *L, T *U, T *dinv,
                                                      FactParams fp) {
+    pdl_wait();  // the kernel ahead in the stream has ended (programmatic dependent launch)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int k = list[blockIdx.x];
     const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
@@ -475,6 +477,7 @@ constexpr int TRSM_MAXT = 10;  // column chunks of 32 per GEMM pass
 template <typename T, int FACT>
 __global__ void __launch_bounds__(256) k_trsm(DevStruct s, const RowTile *__restrict__ tiles, T *L, T *U,
                                                const T *__restrict__ dinv) {
+    pdl_wait();  // the kernel ahead in the stream has ended (programmatic dependent launch)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const RowTile tl = tiles[blockIdx.x];
     const int side = blockIdx.y;
@@ -617,6 +620,7 @@ struct UpdCfg {
 template <typename T, int FACT, int BM, int BN, int BK, int TM, int TN>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN))
     k_update(DevStruct s, const UpdTile *__restrict__ tiles, T *L, T *U) {
+    pdl_wait();  // the kernel ahead in the stream has ended (programmatic dependent launch)
     constexpr int NT = (BM / TM) * (BN / TN);
     constexpr int TX = BM / TM;  // threads along rows
     __shared__ T As[BK][BM + 1];
@@ -1530,6 +1534,7 @@ __device__ __forceinline__ void dg_solve8(AF a_at, TF t_at, const double *Z, dou
 template <typename T, int FACT>
 __global__ void __launch_bounds__(256, 1) k_diag_dmma(DevStruct s, const int *__restrict__ list, T *L, T *U, T *dinv,
                                                        FactParams fp) {
+    pdl_wait();  // the kernel ahead in the stream has ended (programmatic dependent launch)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *W = reinterpret_cast<double *>(smem_raw);  // (nc - jb) x 32 panel, row major, ld DG_LD
     __shared__ double Z0[32 * DG_LD], Z1[32 * DG_LD];
@@ -1766,6 +1771,7 @@ __device__ __forceinline__ bool dc_wait(uint32_t addr, int target) {
 template <typename T, int FACT>
 __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
     k_diag_cluster(DevStruct s, const int *__restrict__ list, T *L, T *U, T *dinv, FactParams fp) {
+    pdl_wait();  // the kernel ahead in the stream has ended (programmatic dependent launch)
     namespace cg = cooperative_groups;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // GETRF: inverted (L_pp)^T of each panel factored here (read by the other CTAs
@@ -2246,6 +2252,7 @@ constexpr int SPLIT_CTAS = 8;
 __global__ void __launch_bounds__(256) k_split(DevStruct s, const SplitSlab *__restrict__ slabs, const float *P,
                                                const float *Dp, const int64_t *__restrict__ sp_off,
                                                unsigned char *img, int scale) {
+    pdl_wait();  // the kernel ahead in the stream has ended (programmatic dependent launch)
     const SplitSlab sl = slabs[blockIdx.x];
     const int k = sl.cblk;
     const int nc = s.cb_lcol[k] - s.cb_fcol[k] + 1;
@@ -2336,6 +2343,7 @@ template <typename T, int FACT>
 __global__ void __launch_bounds__(256, 1) k_trinv(DevStruct s, const int *__restrict__ list, const T *L, const T *U,
                                                    const T *__restrict__ dinv, const int64_t *__restrict__ ti_off,
                                                    float *tinv, int maxnzb) {
+    pdl_wait();  // the kernel ahead in the stream has ended (programmatic dependent launch)
     static_assert(sizeof(T) == 4, "k_trinv stages FP32 factors");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *Yb = reinterpret_cast<double *>(smem_raw);       // rows 0 .. 32 j + 31 of the block column, ld DG_LD
@@ -2437,6 +2445,7 @@ __global__ void __launch_bounds__(256, 1) k_trinv(DevStruct s, const int *__rest
 // Split slabs of dense column-major FP32 matrices into their BF16 images.
 __global__ void __launch_bounds__(256) k_split_dense(const DenseSlab *__restrict__ slabs, const float *src,
                                                      unsigned char *img) {
+    pdl_wait();  // the kernel ahead in the stream has ended (programmatic dependent launch)
     const DenseSlab sl = slabs[blockIdx.x];
     const int nkb = split_nkb(sl.cols), ng = split_ng(sl.rows);
     const float *A = src + sl.src;
@@ -2690,6 +2699,7 @@ __global__ void __launch_bounds__(TP_THREADS, 2) k_update_tcp(DevStruct s, const
                                                                const unsigned char *img0, const unsigned char *img1,
                                                                const int64_t *__restrict__ sp_off, int *queue,
                                                                int *status) {
+    pdl_wait();  // the kernel ahead in the stream has ended (programmatic dependent launch)
     if (*(volatile int *)status != 0) return;
     auto setup = [&](int t, TcOperands &op) {
         const UpdTile tl = tiles[t];
@@ -2756,6 +2766,7 @@ __global__ void __launch_bounds__(TP_THREADS, 2) k_trsm_tcp(DevStruct s, const U
                                                              const unsigned char *timg,
                                                              const int64_t *__restrict__ ti_img, int *queue,
                                                              int *status) {
+    pdl_wait();  // the kernel ahead in the stream has ended (programmatic dependent launch)
     if (*(volatile int *)status != 0) return;
     auto setup = [&](int t, TcOperands &op) {
         const UpdTile tl = tiles[t];
@@ -2821,11 +2832,35 @@ void launch_fill_coef(int64_t nnz, const double *vals, const int64_t *lmap, cons
     k_fill_coef<T><<<blocks, 256, 0, st>>>(nnz, vals, lmap, umap, L, U);
 }
 
+// Launches of the FP32 factorization's level chain may overlap the launch of
+// each kernel with the end of the one ahead of it in its stream (every kernel
+// below waits in pdl_wait first); switched on per host thread by set_pdl.
+static thread_local bool t_pdl = false;
+void set_pdl(bool on) { t_pdl = on; }
+template <typename... KArgs, typename... Args>
+static void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args) {
+    if (!t_pdl) {
+        kernel<<<grid, block, smem, st>>>(args...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 template <typename T, int FACT>
 void launch_panel_small(const DevStruct &s, const int *list, int count, size_t smem, T *L, T *U,
                         const FactParams &fp, cudaStream_t st) {
     if (count <= 0) return;
-    k_panel_small<T, FACT><<<count, 128, smem, st>>>(s, list, L, U, fp);
+    launch_k(k_panel_small<T, FACT>, count, 128, smem, st, s, list, L, U, fp);
 }
 
 template <typename T, int FACT>
@@ -2842,11 +2877,11 @@ void launch_diag_large(const DevStruct &s, const int *list, int count, int maxnc
     const long long csm = diag_cluster_smem_bytes(maxnc, FACT);
     if (maxnc <= DG_MAXNC && maxnc >= DC_MIN_NC && (long long)count * DC <= nsm && count <= DC_MAX_CLUSTERS &&
         csm <= dc_max_smem(FACT))
-        k_diag_cluster<T, FACT><<<count * DC, 256, (size_t)csm, st>>>(s, list, L, U, dinv, fp);
+        launch_k(k_diag_cluster<T, FACT>, count * DC, 256, (size_t)csm, st, s, list, L, U, dinv, fp);
     else if (maxnc <= DG_MAXNC)
-        k_diag_dmma<T, FACT><<<count, 256, (size_t)diag_dmma_smem_bytes(maxnc), st>>>(s, list, L, U, dinv, fp);
+        launch_k(k_diag_dmma<T, FACT>, count, 256, (size_t)diag_dmma_smem_bytes(maxnc), st, s, list, L, U, dinv, fp);
     else
-        k_diag_large<T, FACT><<<count, 256, smem, st>>>(s, list, L, U, dinv, fp);
+        launch_k(k_diag_large<T, FACT>, count, 256, smem, st, s, list, L, U, dinv, fp);
 }
 
 template <typename T, int FACT>
@@ -2857,13 +2892,13 @@ void launch_trsm(const DevStruct &s, const RowTile *tiles, int count, int maxnc,
     if (maxnc <= TD_MAXNC)
         k_trsm_dmma<T, FACT><<<grid, 256, 0, st>>>(s, tiles, L, U, dinv);
     else
-        k_trsm<T, FACT><<<grid, 256, smem, st>>>(s, tiles, L, U, dinv);
+        launch_k(k_trsm<T, FACT>, grid, 256, smem, st, s, tiles, L, U, dinv);
 }
 
 template <typename T, int FACT>
 void launch_update(const DevStruct &s, const UpdTile *tiles, int count, T *L, T *U, cudaStream_t st) {
     if (count <= 0) return;
-    k_update<T, FACT, 64, 64, 16, 4, 4><<<count, 256, 0, st>>>(s, tiles, L, U);
+    launch_k(k_update<T, FACT, 64, 64, 16, 4, 4>, count, 256, 0, st, s, tiles, L, U);
 }
 
 // big tiles (128 x 64): DMMA for FP64, SIMT 8 x 4 per thread for FP32
@@ -2883,7 +2918,7 @@ void launch_update_tc(const DevStruct &s, const UpdTile *tiles, int count, float
                       int *status, cudaStream_t st) {
     if (count <= 0) return;
     const int grid = std::min(count, 2 * sm_count());
-    k_update_tcp<FACT><<<grid, TP_THREADS, TP_SMEM, st>>>(s, tiles, count, L, U, img0, img1, sp_off, queue, status);
+    launch_k(k_update_tcp<FACT>, grid, TP_THREADS, TP_SMEM, st, s, tiles, count, L, U, img0, img1, sp_off, queue, status);
 }
 
 template <int FACT>
@@ -2891,13 +2926,13 @@ void launch_trinv(const DevStruct &s, const int *list, int count, int maxnzb, co
                   const float *dinv, const int64_t *ti_off, float *tinv, cudaStream_t st) {
     if (count <= 0 || maxnzb <= 0) return;
     dim3 grid(count, maxnzb, FACT == FACT_GETRF ? 2 : 1);
-    k_trinv<float, FACT><<<grid, 256, (size_t)trinv_smem_bytes(maxnzb), st>>>(s, list, L, U, dinv, ti_off, tinv,
-                                                                               maxnzb);
+    launch_k(k_trinv<float, FACT>, grid, 256, (size_t)trinv_smem_bytes(maxnzb), st, s, list, L, U, dinv, ti_off, tinv,
+             maxnzb);
 }
 
 void launch_split_dense(const DenseSlab *slabs, int count, const float *src, unsigned char *img, cudaStream_t st) {
     if (count <= 0) return;
-    k_split_dense<<<dim3(count, SPLIT_CTAS), 256, 0, st>>>(slabs, src, img);
+    launch_k(k_split_dense, dim3(count, SPLIT_CTAS), 256, 0, st, slabs, src, img);
 }
 
 template <int FACT>
@@ -2906,14 +2941,14 @@ void launch_trsm_tc(const DevStruct &s, const UpdTile *tiles, int count, float *
                     const unsigned char *timg, const int64_t *ti_img, int *queue, int *status, cudaStream_t st) {
     if (count <= 0) return;
     const int grid = std::min(count, 2 * sm_count());
-    k_trsm_tcp<FACT><<<grid, TP_THREADS, TP_SMEM, st>>>(s, tiles, count, L, U, img0, img1, sp_off, timg, ti_img,
-                                                         queue, status);
+    launch_k(k_trsm_tcp<FACT>, grid, TP_THREADS, TP_SMEM, st, s, tiles, count, L, U, img0, img1, sp_off, timg, ti_img,
+             queue, status);
 }
 
 void launch_split(const DevStruct &s, const SplitSlab *slabs, int count, const float *P, const float *D,
                   const int64_t *sp_off, unsigned char *img, int scale, cudaStream_t st) {
     if (count <= 0) return;
-    k_split<<<dim3(count, SPLIT_CTAS), 256, 0, st>>>(s, slabs, P, D, sp_off, img, scale);
+    launch_k(k_split, dim3(count, SPLIT_CTAS), 256, 0, st, s, slabs, P, D, sp_off, img, scale);
 }
 
 long long split_image_bytes(int nc, int st) { return split_bytes(nc, st); }

@@ -2154,7 +2154,7 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
 // memory epilogue) is the persistent engine tc_persistent below.  Every wait
 // is bounded; on expiry the kernel records PGPU_STATUS_TIMEOUT and returns.
 // ---------------------------------------------------------------------------
-constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 16;
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32;
 constexpr int TC_CH = TC_BK / 8;                    // 8-column chunks per K block
 constexpr int TC_GROUP = 128 * TC_CH;               // bytes of 8 rows x TC_BK columns of one term
 constexpr int TC_PIECE = (TC_BM / 8) * TC_GROUP;    // one term of a 128-row operand block
@@ -2506,7 +2506,7 @@ __global__ void __launch_bounds__(256) k_split_dense(const DenseSlab *__restrict
 //   colinfo(t, op, col)     per-column value shared through shared memory
 //   epi(t, op, rinfo, ct, row, c0, v)  accumulator columns c0 .. c0 + 15 of a row
 // ---------------------------------------------------------------------------
-constexpr int TP_STAGES = 4;
+constexpr int TP_STAGES = 2;
 constexpr size_t TP_SMEM = (size_t)TP_STAGES * TC_STAGE;
 constexpr int TP_THREADS = 192;
 

@@ -82,6 +82,31 @@ struct DevStruct {
 // Without such a launch it returns at once.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Launches of the FP32 factorization's level chains may overlap the launch of
+// each kernel with the end of the one ahead of it in its stream (every kernel
+// launched this way waits in pdl_wait first); switched on per host thread by
+// set_pdl.
+void set_pdl(bool on);
+bool pdl_enabled();
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args) {
+    if (!pdl_enabled()) {
+        kernel<<<grid, block, smem, st>>>(args...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 struct FactParams {
     const double *criterion;    // static pivoting threshold (eps * ||A||_F), in device memory so that
                                 // a captured launch sequence stays valid when the values change

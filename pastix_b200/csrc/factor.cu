@@ -2832,29 +2832,9 @@ void launch_fill_coef(int64_t nnz, const double *vals, const int64_t *lmap, cons
     k_fill_coef<T><<<blocks, 256, 0, st>>>(nnz, vals, lmap, umap, L, U);
 }
 
-// Launches of the FP32 factorization's level chain may overlap the launch of
-// each kernel with the end of the one ahead of it in its stream (every kernel
-// below waits in pdl_wait first); switched on per host thread by set_pdl.
 static thread_local bool t_pdl = false;
 void set_pdl(bool on) { t_pdl = on; }
-template <typename... KArgs, typename... Args>
-static void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args) {
-    if (!t_pdl) {
-        kernel<<<grid, block, smem, st>>>(args...);
-        return;
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
-}
+bool pdl_enabled() { return t_pdl; }
 
 template <typename T, int FACT>
 void launch_panel_small(const DevStruct &s, const int *list, int count, size_t smem, T *L, T *U,

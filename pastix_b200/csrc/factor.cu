@@ -1793,6 +1793,7 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
     T *A = L + s.cb_coef[k];
     T *gZ = dinv + s.cb_dinv[k];
     double *X = fp.dscr + (size_t)(blockIdx.x / DC) * DC_SCR_DOUBLES;  // this cblk's finished panels (POTRF / SYTRF)
+    const double crit = __ldg(fp.criterion);  // read once, off the panel steps' chain
     if (tid == 0) {
         npiv = 0;
         fpart = 0;
@@ -1858,7 +1859,7 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         if (tid == 0) prog = 0;
         __syncthreads();
         if (warp == 0) {
-            const int n = dg_factor32<FACT>(Tb, nb, __ldg(fp.criterion), &Sx[0][0], &prog);
+            const int n = dg_factor32<FACT>(Tb, nb, crit, &Sx[0][0], &prog);
             if (lane == 0 && n) npiv += n;
         } else if (warp == 1) {
             dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 0, &prog, Zs0, gZ + (size_t)p * 1024, fp.status);
@@ -2025,7 +2026,7 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         __syncthreads();
         double *Xq = X + 32 * q + (size_t)(32 * q) * nc;  // the panel's mirror from its top row
         if (warp == 0) {
-            const int n = dg_factor32<FACT>(W, nb, __ldg(fp.criterion), &Sx[0][0], &prog, bar_n, Xq, nc);
+            const int n = dg_factor32<FACT>(W, nb, crit, &Sx[0][0], &prog, bar_n, Xq, nc);
             if (lane == 0 && n) npiv += n;
         } else if (warp == 1) {
             dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 0, &prog, Zs0, gZ + (size_t)q * 1024, fp.status, bar_n);

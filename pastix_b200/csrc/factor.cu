@@ -1309,6 +1309,7 @@ __device__ __noinline__ int dg_factor32_sym(double *W, int nb, double crit, doub
 //   x_c = (w_c - sum_{k<c} x_k P(k, c)) / d_c      (L(i, jb + c), written in place
 //                                                   and to gX, column-major, ld ldx)
 //   w_j -= sum_c x_c P(c, j)                        (the row's later columns)
+// bar_n = 0: the factorization has published every block already (no waits).
 template <int FACT>
 __device__ __noinline__ void dg_follow_rows(double *W, int nrows, int nb, const double *Pub, int bar_n, double *gX,
                                             int ldx) {
@@ -1319,7 +1320,7 @@ __device__ __noinline__ void dg_follow_rows(double *W, int nrows, int nb, const 
     for (int j = 0; j < 32; j++) r[j] = (own && j < nb) ? W[lane * DG_LD + j] : 0.0;
 #pragma unroll 1
     for (int jb = 0; jb < nb; jb += 8) {
-        asm volatile("bar.sync %0, %1;" ::"r"(1 + jb / 8), "r"(bar_n) : "memory");
+        if (bar_n) asm volatile("bar.sync %0, %1;" ::"r"(1 + jb / 8), "r"(bar_n) : "memory");
         const double *P = Pub + jb * DG_BLD + jb;
         double x[8];
 #pragma unroll
@@ -2005,8 +2006,9 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
     // (dg_follow_rows), so the panel is final one block step after its top
     // block and is announced then (fdone = q + 1), while the inverse (kept for
     // the later TRSM kernels and the solve) is still being written.  Rows beyond
-    // the followers' 192 (blocks wider than 224 columns, first panels) take the
-    // update and the TRSM by the inverse before the announcement.
+    // the followers' 192 (blocks wider than 224 columns, first panels) are
+    // taken 32 at a time by the same warps once their first rows are done,
+    // against the then complete factorization.
     // panel p (final) from shared memory to the factor in global memory
     auto write_panel = [&](int p) {
         const int lop = dc_lo(p, FACT), nb = min(32, nc - 32 * p);
@@ -2020,9 +2022,9 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         const int nb = min(32, nc - 32 * q);
         double *W = Wl + poff(q);  // lo = 32 q: the top block is the panel's first nb rows
         const int nr = nc - 32 * q - nb;
-        const int F = min(DC_FOLLOW, (nr + 31) / 32);
+        const int nch = (nr + 31) / 32;  // 32-row chunks below the top block
+        const int F = min(DC_FOLLOW, nch);
         const int bar_n = 64 + 32 * F;
-        const bool rest = nr > 32 * DC_FOLLOW;
         __syncthreads();
         double *Xq = X + 32 * q + (size_t)(32 * q) * nc;  // the panel's mirror from its top row
         if (warp == 0) {
@@ -2031,13 +2033,14 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
         } else if (warp == 1) {
             dg_inverse_pipe<T, FACT>(&Sx[0][0], nb, 0, &prog, Zs0, gZ + (size_t)q * 1024, fp.status, bar_n);
         } else if (warp - 2 < F) {
-            const int f = warp - 2;
-            double *Wf = W + (nb + 32 * f) * DG_LD;
-            const int nrows = min(32, nr - 32 * f);
-            if (pu >= 0) dg_rows_update(Wf, nrows, X + 32 * q + nb + 32 * f + (size_t)(32 * pu) * nc, nc, Bs);
-            dg_follow_rows<FACT>(Wf, nrows, nb, &Sx[0][0], bar_n, Xq + nb + 32 * f, nc);
+            for (int f = warp - 2; f < nch; f += DC_FOLLOW) {
+                double *Wf = W + (nb + 32 * f) * DG_LD;
+                const int nrows = min(32, nr - 32 * f);
+                if (pu >= 0) dg_rows_update(Wf, nrows, X + 32 * q + nb + 32 * f + (size_t)(32 * pu) * nc, nc, Bs);
+                dg_follow_rows<FACT>(Wf, nrows, nb, &Sx[0][0], f < DC_FOLLOW ? bar_n : 0, Xq + nb + 32 * f, nc);
+            }
         }
-        if (!rest && warp != 1 && warp < 2 + F) {
+        if (warp != 1 && warp < 2 + F) {
             asm volatile("bar.sync 5, %0;" ::"r"(32 * (1 + F)) : "memory");
             if (tid == 0) {
                 asm volatile("fence.acq_rel.cluster;" ::: "memory");
@@ -2045,11 +2048,6 @@ __global__ void __cluster_dims__(DC, 1, 1) __launch_bounds__(256, 1)
             }
         }
         __syncthreads();
-        if (rest) {
-            if (pu >= 0) update_rows(pu, q, 32 * q + nb + 32 * DC_FOLLOW, nc);
-            trsm_rows(q, 32 * q + nb + 32 * DC_FOLLOW, nc);
-            publish(&fdone, q);
-        }
     };
 
     if (FACT != FACT_GETRF) {

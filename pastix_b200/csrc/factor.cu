@@ -2398,14 +2398,24 @@ __global__ void __launch_bounds__(256, 1) k_trinv(DevStruct s, const int *__rest
         const float *ts = Ts + b * 32 * tld;
         const float *zs = Zf + b * 32 * TI_ZLD;
         const int k0 = 32 * (i + 1), K = 32 * (j - i);
-        // S = T_{i, i+1..j} Y_{i+1..j}
-        double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
-        for (int ks = 0; ks < K / 4; ks++) {
-            const double a = (double)ts[(8 * orf + g) * tld + 4 * ks + t4];
+        // S = T_{i, i+1..j} Y_{i+1..j}, K (a multiple of 32) split over four
+        // accumulator chains: with the loads staged ahead, the DMMA latency of
+        // one long chain set the pace
+        double acc4[4][2][2] = {};
+        for (int ks = 0; ks < K / 4; ks += 4) {
 #pragma unroll
-            for (int c = 0; c < 2; c++)
-                dmma884(acc[c][0], acc[c][1], a, Yb[(k0 + 4 * ks + t4) * DG_LD + 8 * (ocf + c) + g]);
+            for (int h = 0; h < 4; h++) {
+                const double a = (double)ts[(8 * orf + g) * tld + 4 * (ks + h) + t4];
+#pragma unroll
+                for (int c = 0; c < 2; c++)
+                    dmma884(acc4[h][c][0], acc4[h][c][1], a, Yb[(k0 + 4 * (ks + h) + t4) * DG_LD + 8 * (ocf + c) + g]);
+            }
         }
+        double acc[2][2];
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) acc[c][e] = (acc4[0][c][e] + acc4[1][c][e]) + (acc4[2][c][e] + acc4[3][c][e]);
         double scale = 1.0;
         if (FACT == FACT_SYTRF) {
             const int a = 32 * i + 8 * orf + g;
